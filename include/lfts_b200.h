@@ -1,0 +1,209 @@
+/*
+ * lfts_b200.h -- C ABI of the B200 chain-propagator engine (liblfts_b200.so).
+ *
+ * Plain pointers and sizes only; every call returns 0 on success or a negative
+ * status, with the message available from lfts_last_error().  Device buffers
+ * are allocated by the caller (lfts_malloc or any CUDA allocator) and passed
+ * in; no entry point below allocates except lfts_ctx_create / lfts_malloc.
+ * All work is enqueued on the context's stream; nothing synchronises with the
+ * host except lfts_synchronize and the blocking copies.
+ *
+ * Real-valued device arrays of a context use its precision (8 = double,
+ * 4 = float): propagator slices, exp(-w ds) factor tables, Boltzmann bond
+ * tables and spectra (complex = two reals).  Fields w, concentrations,
+ * partition functions, stress and every reduction are always double.
+ *
+ * Grid layout: a 1D/2D/3D periodic box is handled as n0 x n1 x n2 (z fastest)
+ * with leading extents of 1, M = n0*n1*n2 reals, Mc = n0*n1*(n2/2+1) complex,
+ * exactly the real / conjugate-even layouts of the reference
+ * (src/platforms/cpu/MklFFT3D.cpp:14-19, src/common/Pseudo.cpp:5-15).
+ */
+#ifndef LFTS_B200_H_
+#define LFTS_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lfts_ctx_s *lfts_ctx;
+
+/* ---- context, memory, errors ------------------------------------------ */
+
+/* Replaces CudaSolverPseudo's constructor (cuFFT plans, device tables;
+ * src/platforms/cuda/CudaSolverPseudo.cu:6-147).  dim = 1..3, nx[0..dim-1];
+ * precision = 8 (FP64) or 4 (FP32).  Prime factors of each extent must be
+ * <= 64 and the x-plane must fit in shared memory (checked, error otherwise). */
+int lfts_ctx_create(lfts_ctx *out, int device, int dim, const int *nx, int precision);
+int lfts_ctx_destroy(lfts_ctx ctx);
+/* Use an external CUDA stream (cudaStream_t as void*); NULL = the context's own. */
+int lfts_ctx_set_stream(lfts_ctx ctx, void *stream);
+void *lfts_ctx_stream(lfts_ctx ctx);
+int lfts_ctx_info(lfts_ctx ctx, long long *M, long long *Mc, int *precision);
+/* Message of the last failing call on this thread. */
+const char *lfts_last_error(void);
+
+int lfts_malloc(lfts_ctx ctx, void **ptr, size_t bytes);
+int lfts_free(lfts_ctx ctx, void *ptr);
+int lfts_memset_async(lfts_ctx ctx, void *ptr, int value, size_t bytes);
+/* Blocking copies (used by the host wrapper for numpy inputs/outputs). */
+int lfts_memcpy_h2d(lfts_ctx ctx, void *dst, const void *src, size_t bytes);
+int lfts_memcpy_d2h(lfts_ctx ctx, void *dst, const void *src, size_t bytes);
+int lfts_memcpy_d2d_async(lfts_ctx ctx, void *dst, const void *src, size_t bytes);
+int lfts_synchronize(lfts_ctx ctx);
+
+/* CUDA graph capture of everything enqueued on the context stream between
+ * begin and end (replaces the reference's per-step launches driven by OpenMP
+ * host threads, CudaComputationContinuous.cu:273-505). */
+typedef struct lfts_graph_s *lfts_graph;
+int lfts_graph_begin(lfts_ctx ctx);
+int lfts_graph_end(lfts_ctx ctx, lfts_graph *out);
+int lfts_graph_launch(lfts_ctx ctx, lfts_graph g);
+int lfts_graph_destroy(lfts_graph g);
+
+/* ---- tables ------------------------------------------------------------ */
+
+/* Boltzmann bond factors exp(-b^2 |k|^2 ds / 6) and exp(-b^2 |k|^2 ds / 12),
+ * each pre-divided by M (the inverse-FFT normalisation), precision of ctx.
+ * Replaces Pseudo::get_boltz_bond (src/common/Pseudo.cpp:17-82) +
+ * CudaSolverPseudo::update_laplacian_operator (CudaSolverPseudo.cu:211-253). */
+int lfts_bond_tables(lfts_ctx ctx, double bond_length_sq, double ds, const double *lx,
+                     void *bond_out, void *bond_half_out);
+/* Weighted Fourier basis k_d^2 (x2 for 0 < kz < n2/2), 3 x Mc doubles.
+ * Replaces Pseudo::get_weighted_fourier_basis (src/common/Pseudo.cpp:84-153). */
+int lfts_fourier_basis(lfts_ctx ctx, const double *lx, double *basis_out);
+/* fac[i] = exp(coef * w[i]) with w double (device), fac in ctx precision.
+ * coef = -ds/4 (continuous: exp(-w ds/4), its square is exp(-w ds/2)) or
+ * -ds (discrete).  Replaces update_dw (CudaSolverPseudo.cu:254-343). */
+int lfts_field_factors(lfts_ctx ctx, const double *w, double coef, void *fac_out);
+
+/* ---- contour steps ------------------------------------------------------ */
+
+/* One propagation job.  For step index s of a launch, the input slice is
+ * in + s*in_stride and the output slice out + s*out_stride (elements of the
+ * ctx precision), so one job array covers a whole schedule slot.
+ * spec: scratch for two complex half spectra (2*Mc complex elements). */
+typedef struct {
+    const void *in;
+    long long in_stride;
+    void *out;
+    long long out_stride;
+    const void *fac;        /* exp(-w ds/4) (continuous) or exp(-w ds) (discrete) */
+    const void *bond;       /* bond table (lfts_bond_tables: bond_out) */
+    const void *bond_half;  /* half-bond table */
+    void *spec;
+} lfts_step_job;
+
+/* 4th-order Richardson continuous step, q' = (4 q_{ds/2,ds/2} - q_ds)/3, for
+ * njobs jobs (array in DEVICE memory) at step index s.  Replaces
+ * CudaSolverPseudo::advance_propagator_continuous (CudaSolverPseudo.cu:345-412)
+ * and CpuSolverPseudo::advance_propagator_continuous (CpuSolverPseudo.cpp:120-188). */
+int lfts_step_continuous(lfts_ctx ctx, const lfts_step_job *jobs, int njobs, int s);
+/* Discrete chain: out = [fac *] F^-1[ b * F[in] ] with b = bond (half=0) or
+ * bond_half (half=1), multiplied by fac when with_fac=1.  (half=0, with_fac=1)
+ * replaces advance_propagator_discrete (CudaSolverPseudo.cu:413-450);
+ * (half=1, with_fac=0) replaces advance_propagator_discrete_half_bond_step
+ * (CudaSolverPseudo.cu:451-476); (half=1, with_fac=1) is the junction start of
+ * CpuComputationDiscrete.cpp:402-445 fused into one pass. */
+int lfts_step_discrete(lfts_ctx ctx, const lfts_step_job *jobs, int njobs, int s, int half, int with_fac);
+
+/* ---- junctions and initial slices --------------------------------------- */
+
+/* out[i] = prod_d dep_d[i] (mode 0) or sum_d weight_d * dep_d[i] (mode 1),
+ * optionally times fac[i] (continuous: fac^2 = exp(-w ds/2) is NOT applied;
+ * the factor is used by discrete leaves).  dep pointers/weights in device
+ * arrays.  Replaces the junction code of CudaComputationContinuous.cu:326-392
+ * and CpuComputationDiscrete.cpp:298-445. */
+typedef struct {
+    void *out;
+    const void *fac;      /* NULL or a factor table multiplied into out */
+    int ndeps;            /* 0: out = 1 (times fac) */
+    int mode;             /* 0 product, 1 weighted sum */
+    int dep_offset;       /* first entry in dep_ptrs/dep_weights */
+    int pad;
+} lfts_junction_job;
+int lfts_junctions(lfts_ctx ctx, const lfts_junction_job *jobs, int njobs, const void *const *dep_ptrs,
+                   const double *dep_weights);
+
+/* ---- reductions (FP64 accumulation) ------------------------------------- */
+
+/* out[j] = scale_j * sum_i a_j[i] b_j[i] (/ w_j[i] if w_j != NULL).
+ * Replaces ComputationBox::inner_product / inner_product_inverse_weight
+ * (src/common/ComputationBox.cpp:273-286, CudaComputationBox.cu:56-117).
+ * a, b, w in ctx precision; out (device) double. */
+typedef struct {
+    const void *a;
+    const void *b;
+    const void *w;
+    double scale;
+} lfts_dot_job;
+int lfts_dots(lfts_ctx ctx, const lfts_dot_job *jobs, int njobs, double *out);
+
+/* Block concentrations.  Continuous (model 0):
+ *   phi[i] = norm * sum_{n=0}^{NR} c[coef_offset+n] q_left[(NL-n)*M+i] q_right[n*M+i]
+ * Discrete (model 1):
+ *   phi[i] = norm * sum_{n=1}^{NR} q_left[(NL-n+1)*M+i] q_right[n*M+i] / fac[i]
+ * phi (double).  Replaces calculate_phi_one_block + normalisation
+ * (CpuComputationContinuous.cpp:371-465, CpuComputationDiscrete.cpp:584-679,
+ * CudaComputationContinuous.cu:527-620). */
+typedef struct {
+    const void *q_left;
+    const void *q_right;
+    const void *fac;
+    double *phi;
+    double norm;
+    int n_left;
+    int n_right;
+    int coef_offset;
+    int pad;
+} lfts_phi_job;
+int lfts_phi_blocks(lfts_ctx ctx, int model, const lfts_phi_job *jobs, int njobs, const double *coefs);
+
+/* Stress contributions: out[3*j+d] = weight_j * sum_k Re(F[q1_j](k) conj F[q2_j](k))
+ * * basis_d(k) (* bond_j(k) if bond_j != NULL).  spec: scratch of 2*Mc complex
+ * per job (jobs are processed in chunks of at most max_chunk).  Replaces
+ * compute_single_segment_stress_{continuous,discrete}
+ * (CudaSolverPseudo.cu:477-608, CpuSolverPseudo.cpp:250-356). */
+typedef struct {
+    const void *q1;
+    const void *q2;
+    const void *bond;   /* NULL (continuous) or bond / half-bond table already / M */
+    double weight;
+} lfts_stress_job;
+int lfts_stress(lfts_ctx ctx, const lfts_stress_job *jobs, int njobs, const double *basis, void *spec,
+                int max_chunk, double *out);
+
+/* ---- Anderson mixing (FP64) --------------------------------------------- */
+
+/* History vectors live in a ring of ring_len slots of `stride` doubles; the
+ * i-th newest (i = 0 newest) is slot (head - i) mod ring_len.
+ * dots[i] = sum_k d[k] * hist_i[k] for i < nhist.  Replaces the per-history
+ * dot loop of CudaAndersonMixing.cu:245-250 (CpuAndersonMixing.cpp:100-108). */
+int lfts_am_dots(lfts_ctx ctx, const double *d, const double *hist, long long stride, int nhist, long long n,
+                 double *dots, int head, int ring_len);
+/* w_new = w_0 + d_0 + sum_{i<nh} a[i] (w_{i+1} + d_{i+1} - w_0 - d_0), ring
+ * indexing as above; a in DEVICE memory.  Replaces CudaAndersonMixing.cu:292-304
+ * (CpuAndersonMixing.cpp:143-158). */
+int lfts_am_update(lfts_ctx ctx, double *w_new, const double *w_hist, const double *d_hist, long long stride,
+                   int nh, const double *a, long long n, int head, int ring_len);
+/* w_new = w + mix * d (simple mixing, CpuAndersonMixing.cpp:110-121). */
+int lfts_am_simple(lfts_ctx ctx, double *w_new, const double *w, const double *d, double mix, long long n);
+
+/* ---- small helpers ------------------------------------------------------ */
+
+/* out[i] = sum_k coefs[k] * srcs[k][i] (doubles; srcs/coefs are HOST arrays of
+ * device pointers / values, any count).  Sums block concentrations into the
+ * per-monomer totals (get_total_concentration, CpuComputationContinuous.cpp:466-520). */
+int lfts_lincomb(lfts_ctx ctx, double *out, int nsrc, const double *const *srcs, const double *coefs, long long n);
+/* Solvent: Q = dv_over_V * sum_i fac[i]^power (written to Q_out, device), then
+ * phi[i] = vf * fac[i]^power / Q.  power 4 with fac = exp(-w ds/4) gives the
+ * continuous solvent exp(-w ds)^... of CpuComputationContinuous.cpp:425-436;
+ * power 1 with fac = exp(-w ds) the discrete one (CpuComputationDiscrete.cpp:441-452). */
+int lfts_solvent(lfts_ctx ctx, const void *fac, int power, double vf, double dv_over_V, double *phi_out, double *Q_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

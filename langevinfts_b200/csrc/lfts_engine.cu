@@ -1,0 +1,780 @@
+// liblfts_b200: C-ABI implementation of the B200 chain-propagator engine.
+// Declarations and the reference interfaces each entry replaces are in
+// include/lfts_b200.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "lfts_step_kernels.cuh"
+
+using namespace lfts;
+
+// ---------------------------------------------------------------- errors
+static thread_local std::string g_err;
+
+static int fail(const std::string &msg) {
+    g_err = msg;
+    return -1;
+}
+#define CK(call)                                                                                        \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return fail(std::string(#call) + ": " + cudaGetErrorString(e_) + " (" __FILE__ ":" +        \
+                        std::to_string(__LINE__) + ")");                                                \
+    } while (0)
+#define CKLAUNCH(name) CK(cudaPeekAtLastError())
+
+// ---------------------------------------------------------------- context
+struct lfts_ctx_s {
+    int device = 0, dim = 3, prec = 8;
+    int nx[3] = {1, 1, 1};
+    cudaStream_t stream = nullptr, own_stream = nullptr;
+    GridPlan g;
+    void *tables = nullptr;
+    bool gen = false, nbr2 = true;
+    int TJ = 16, ntiles = 1;
+    size_t sm_pf1 = 0, sm_pf2 = 0, sm_mid = 0, sm_inv1 = 0, sm_inv2 = 0, sm_x1 = 0, sm_x2 = 0;
+    double *partials = nullptr;
+    size_t partials_cap = 0;
+    lfts_step_job *sjobs = nullptr;
+    int sjobs_cap = 0;
+    lfts_step_job *sjobs_host = nullptr;
+};
+
+struct lfts_graph_s {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+static void make_axis(int n, AxisPlan &ap, std::vector<short> &perm, bool &gen, std::string &err) {
+    ap.n = n;
+    ap.nf = 0;
+    int m = n;
+    auto push = [&](int r) {
+        if (ap.nf >= LFTS_MAX_FACTORS) { err = "too many FFT factors"; return; }
+        ap.radix[ap.nf++] = r;
+    };
+    while (m % 8 == 0) { push(8); m /= 8; }
+    while (m % 4 == 0) { push(4); m /= 4; }
+    while (m % 2 == 0) { push(2); m /= 2; }
+    while (m % 3 == 0) { push(3); m /= 3; }
+    while (m % 5 == 0) { push(5); m /= 5; }
+    for (int p = 7; m > 1; p += 2) {
+        while (m % p == 0) {
+            if (p > LFTS_MAX_RADIX) { err = "grid extent " + std::to_string(n) + " has a prime factor > 64"; return; }
+            gen = true;
+            push(p);
+            m /= p;
+        }
+    }
+    // digit-reversal permutation, outermost radix first
+    perm.assign(n, 0);
+    for (int t = 0; t < n; t++) {
+        int pos = 0, len = n, rem = t;
+        for (int f = 0; f < ap.nf; f++) {
+            const int r = ap.radix[f];
+            len /= r;
+            pos += (rem % r) * len;
+            rem /= r;
+        }
+        perm[t] = (short)pos;
+    }
+}
+
+template <typename T, bool GEN>
+__global__ void k_xstress(GridPlan g, const lfts_step_job *__restrict__ sj, const lfts_stress_job *__restrict__ jobs,
+                          const double *__restrict__ basis, int TJ, double *partials);
+
+template <typename T, bool GEN> static void set_attrs_t(lfts_ctx c) {
+    cudaFuncSetAttribute(k_plane_forward<T, 1, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_pf1);
+    cudaFuncSetAttribute(k_plane_mid<T, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_mid);
+    cudaFuncSetAttribute(k_plane_inverse<T, 1, EPI_SCALE, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_inv1);
+    cudaFuncSetAttribute(k_plane_inverse<T, 1, EPI_RICH_ACC, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_inv1);
+    cudaFuncSetAttribute(k_xpass<T, 1, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_x1);
+    {
+        const size_t smx = sizeof(typename CT<T>::type) * (2 * (size_t)c->g.n0 * c->TJ + c->g.n0) + sizeof(short) * c->g.n0;
+        cudaFuncSetAttribute(k_xstress<T, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
+    }
+    if (c->nbr2) {
+        cudaFuncSetAttribute(k_plane_forward<T, 2, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_pf2);
+        cudaFuncSetAttribute(k_plane_inverse<T, 2, EPI_RICH, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_inv2);
+        cudaFuncSetAttribute(k_xpass<T, 2, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_x2);
+    }
+}
+
+template <typename T> static int setup_plan(lfts_ctx c) {
+    using C = typename CT<T>::type;
+    GridPlan &g = c->g;
+    const int n[3] = {g.n0, g.n1, g.n2};
+    std::vector<short> perm[3];
+    std::string err;
+    for (int a = 0; a < 3; a++) {
+        if (n[a] > LFTS_MAX_AXIS) return fail("grid extent " + std::to_string(n[a]) + " exceeds 1024");
+        make_axis(n[a], g.ax[a], perm[a], c->gen, err);
+        if (!err.empty()) return fail(err);
+    }
+    size_t bytes = 0;
+    for (int a = 0; a < 3; a++) bytes += sizeof(C) * n[a] + 16 + sizeof(short) * n[a] + 16;
+    CK(cudaMalloc(&c->tables, bytes));
+    std::vector<unsigned char> host(bytes, 0);
+    size_t off = 0;
+    for (int a = 0; a < 3; a++) {
+        C *tw = (C *)(host.data() + off);
+        for (int j = 0; j < n[a]; j++) {
+            const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)j / (long double)n[a];
+            tw[j].x = (T)std::cos(ang);
+            tw[j].y = (T)std::sin(ang);
+        }
+        g.tw[a] = (const char *)c->tables + off;
+        off += (sizeof(C) * n[a] + 15) / 16 * 16;
+        std::memcpy(host.data() + off, perm[a].data(), sizeof(short) * n[a]);
+        g.perm[a] = (const short *)((const char *)c->tables + off);
+        off += (sizeof(short) * n[a] + 15) / 16 * 16;
+    }
+    CK(cudaMemcpy(c->tables, host.data(), bytes, cudaMemcpyHostToDevice));
+
+    int max_smem = 0;
+    CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    c->TJ = (sizeof(T) == 8) ? 16 : 32;
+    c->ntiles = (int)((g.n1 * (long long)g.nzc + c->TJ - 1) / c->TJ);
+    c->sm_pf1 = PlaneSmem<C>::bytes(1, g.n1, g.n2, g.nzc, false);
+    c->sm_pf2 = PlaneSmem<C>::bytes(2, g.n1, g.n2, g.nzc, false);
+    c->sm_mid = PlaneSmem<C>::bytes(1, g.n1, g.n2, g.nzc, true);
+    c->sm_inv1 = c->sm_pf1;
+    c->sm_inv2 = c->sm_pf2;
+    c->sm_x1 = sizeof(C) * (1 * (size_t)g.n0 * c->TJ + g.n0) + sizeof(short) * g.n0;
+    c->sm_x2 = sizeof(C) * (2 * (size_t)g.n0 * c->TJ + g.n0) + sizeof(short) * g.n0;
+    if ((int)c->sm_mid > max_smem || (int)c->sm_x1 > max_smem)
+        return fail("grid plane " + std::to_string(g.n1) + "x" + std::to_string(g.n2) +
+                    " does not fit in shared memory (" + std::to_string(c->sm_mid) + " > " + std::to_string(max_smem) + " bytes)");
+    c->nbr2 = (int)c->sm_pf2 <= max_smem && (int)c->sm_x2 <= max_smem;
+    if (c->gen) set_attrs_t<T, true>(c); else set_attrs_t<T, false>(c);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+extern "C" const char *lfts_last_error(void) { return g_err.c_str(); }
+
+extern "C" int lfts_ctx_create(lfts_ctx *out, int device, int dim, const int *nx, int precision) {
+    if (!out || !nx) return fail("null argument");
+    if (dim < 1 || dim > 3) return fail("dim must be 1, 2 or 3");
+    if (precision != 8 && precision != 4) return fail("precision must be 8 (double) or 4 (float)");
+    for (int d = 0; d < dim; d++)
+        if (nx[d] < 1) return fail("grid extents must be positive");
+    auto *c = new lfts_ctx_s();
+    c->device = device;
+    c->dim = dim;
+    c->prec = precision;
+    int t[3] = {1, 1, 1};
+    for (int d = 0; d < dim; d++) t[3 - dim + d] = nx[d];
+    for (int d = 0; d < 3; d++) c->nx[d] = t[d];
+    GridPlan &g = c->g;
+    g.n0 = t[0];
+    g.n1 = t[1];
+    g.n2 = t[2];
+    g.nzc = g.n2 / 2 + 1;
+    g.M = (long long)g.n0 * g.n1 * g.n2;
+    g.Mc = (long long)g.n0 * g.n1 * g.nzc;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { delete c; return fail(std::string("cudaSetDevice: ") + cudaGetErrorString(e)); }
+    e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete c; return fail(std::string("cudaStreamCreate: ") + cudaGetErrorString(e)); }
+    c->stream = c->own_stream;
+    int rc = (precision == 8) ? setup_plan<double>(c) : setup_plan<float>(c);
+    if (rc != 0) { lfts_ctx_destroy(c); return rc; }
+    c->partials_cap = 1 << 20;
+    c->sjobs_cap = 2048;
+    if (cudaMalloc(&c->partials, sizeof(double) * c->partials_cap) != cudaSuccess ||
+        cudaMalloc(&c->sjobs, sizeof(lfts_step_job) * c->sjobs_cap) != cudaSuccess ||
+        cudaMallocHost(&c->sjobs_host, sizeof(lfts_step_job) * c->sjobs_cap) != cudaSuccess) {
+        lfts_ctx_destroy(c);
+        return fail("workspace allocation failed");
+    }
+    *out = c;
+    return 0;
+}
+
+extern "C" int lfts_ctx_destroy(lfts_ctx c) {
+    if (!c) return 0;
+    cudaSetDevice(c->device);
+    if (c->tables) cudaFree(c->tables);
+    if (c->partials) cudaFree(c->partials);
+    if (c->sjobs) cudaFree(c->sjobs);
+    if (c->sjobs_host) cudaFreeHost(c->sjobs_host);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return 0;
+}
+
+extern "C" int lfts_ctx_set_stream(lfts_ctx c, void *stream) {
+    if (!c) return fail("null context");
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return 0;
+}
+extern "C" void *lfts_ctx_stream(lfts_ctx c) { return c ? (void *)c->stream : nullptr; }
+extern "C" int lfts_ctx_info(lfts_ctx c, long long *M, long long *Mc, int *prec) {
+    if (!c) return fail("null context");
+    if (M) *M = c->g.M;
+    if (Mc) *Mc = c->g.Mc;
+    if (prec) *prec = c->prec;
+    return 0;
+}
+
+extern "C" int lfts_malloc(lfts_ctx c, void **ptr, size_t bytes) {
+    if (!c || !ptr) return fail("null argument");
+    CK(cudaSetDevice(c->device));
+    CK(cudaMalloc(ptr, bytes ? bytes : 16));
+    return 0;
+}
+extern "C" int lfts_free(lfts_ctx c, void *ptr) {
+    if (!c) return fail("null context");
+    if (ptr) CK(cudaFree(ptr));
+    return 0;
+}
+extern "C" int lfts_memset_async(lfts_ctx c, void *ptr, int v, size_t bytes) {
+    CK(cudaMemsetAsync(ptr, v, bytes, c->stream));
+    return 0;
+}
+extern "C" int lfts_memcpy_h2d(lfts_ctx c, void *dst, const void *src, size_t bytes) {
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+extern "C" int lfts_memcpy_d2h(lfts_ctx c, void *dst, const void *src, size_t bytes) {
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+extern "C" int lfts_memcpy_d2d_async(lfts_ctx c, void *dst, const void *src, size_t bytes) {
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    return 0;
+}
+extern "C" int lfts_synchronize(lfts_ctx c) {
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int lfts_graph_begin(lfts_ctx c) {
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    return 0;
+}
+extern "C" int lfts_graph_end(lfts_ctx c, lfts_graph *out) {
+    auto *gr = new lfts_graph_s();
+    cudaError_t e = cudaStreamEndCapture(c->stream, &gr->graph);
+    if (e != cudaSuccess) { delete gr; return fail(std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e)); }
+    e = cudaGraphInstantiate(&gr->exec, gr->graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(gr->graph);
+        delete gr;
+        return fail(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    *out = gr;
+    return 0;
+}
+extern "C" int lfts_graph_launch(lfts_ctx c, lfts_graph g) {
+    CK(cudaGraphLaunch(g->exec, c->stream));
+    return 0;
+}
+extern "C" int lfts_graph_destroy(lfts_graph g) {
+    if (!g) return 0;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return 0;
+}
+
+// ---------------------------------------------------------------- tables
+// Boltzmann bond factor, same arithmetic as the reference's Pseudo.cpp:17-82
+// (xfactor from nx*dx, integer wave numbers folded at n/2), then / M.
+template <typename T>
+static int bond_tables_t(lfts_ctx c, double b2, double ds, const double *lx, void *b_out, void *bh_out) {
+    const GridPlan &g = c->g;
+    const int tn[3] = {g.n0, g.n1, g.n2};
+    double tdx[3] = {1.0, 1.0, 1.0};
+    for (int d = 0; d < c->dim; d++) tdx[3 - c->dim + d] = lx[d] / c->nx[3 - c->dim + d];
+    const double PI = 3.14159265358979323846;
+    std::vector<T> hb(g.Mc), hh(g.Mc);
+    double xf[3], xh[3];
+    for (int d = 0; d < 3; d++) {
+        xf[d] = -b2 * std::pow(2 * PI / (tn[d] * tdx[d]), 2) * ds / 6.0;
+        xh[d] = -(b2 / 2) * std::pow(2 * PI / (tn[d] * tdx[d]), 2) * ds / 6.0;
+    }
+    const double invM = 1.0 / (double)g.M;
+    for (int i = 0; i < tn[0]; i++) {
+        const int it = i > tn[0] / 2 ? tn[0] - i : i;
+        for (int j = 0; j < tn[1]; j++) {
+            const int jt = j > tn[1] / 2 ? tn[1] - j : j;
+            for (int k = 0; k < g.nzc; k++) {
+                const long long idx = ((long long)i * tn[1] + j) * g.nzc + k;
+                hb[idx] = (T)(std::exp(it * it * xf[0] + jt * jt * xf[1] + k * k * xf[2]) * invM);
+                hh[idx] = (T)(std::exp(it * it * xh[0] + jt * jt * xh[1] + k * k * xh[2]) * invM);
+            }
+        }
+    }
+    CK(cudaMemcpyAsync(b_out, hb.data(), sizeof(T) * g.Mc, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(bh_out, hh.data(), sizeof(T) * g.Mc, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+extern "C" int lfts_bond_tables(lfts_ctx c, double b2, double ds, const double *lx, void *b_out, void *bh_out) {
+    if (!c || !lx || !b_out || !bh_out) return fail("null argument");
+    return c->prec == 8 ? bond_tables_t<double>(c, b2, ds, lx, b_out, bh_out)
+                        : bond_tables_t<float>(c, b2, ds, lx, b_out, bh_out);
+}
+
+// Pseudo.cpp:84-153: k_d^2 (2 pi / L_d)^2, doubled for 0 < kz < n2/2
+extern "C" int lfts_fourier_basis(lfts_ctx c, const double *lx, double *basis_out) {
+    if (!c || !lx || !basis_out) return fail("null argument");
+    const GridPlan &g = c->g;
+    const int tn[3] = {g.n0, g.n1, g.n2};
+    double tdx[3] = {1.0, 1.0, 1.0};
+    for (int d = 0; d < c->dim; d++) tdx[3 - c->dim + d] = lx[d] / c->nx[3 - c->dim + d];
+    const double PI = 3.14159265358979323846;
+    double xf[3];
+    for (int d = 0; d < 3; d++) xf[d] = std::pow(2 * PI / (tn[d] * tdx[d]), 2);
+    std::vector<double> h(3 * g.Mc);
+    for (int i = 0; i < tn[0]; i++) {
+        const int it = i > tn[0] / 2 ? tn[0] - i : i;
+        for (int j = 0; j < tn[1]; j++) {
+            const int jt = j > tn[1] / 2 ? tn[1] - j : j;
+            for (int k = 0; k < g.nzc; k++) {
+                const long long idx = ((long long)i * tn[1] + j) * g.nzc + k;
+                double bx = it * it * xf[0], by = jt * jt * xf[1], bz = k * k * xf[2];
+                if (k != 0 && 2 * k != tn[2]) { bx *= 2; by *= 2; bz *= 2; }
+                h[idx] = bx;
+                h[g.Mc + idx] = by;
+                h[2 * g.Mc + idx] = bz;
+            }
+        }
+    }
+    CK(cudaMemcpyAsync(basis_out, h.data(), sizeof(double) * 3 * g.Mc, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+template <typename T>
+__global__ void k_field_factors(const double *__restrict__ w, double coef, T *__restrict__ fac, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        fac[i] = (T)exp(coef * w[i]);
+}
+static int grid_for(long long n) {
+    long long b = (n + NTHR - 1) / NTHR;
+    if (b > 148 * 16) b = 148 * 16;
+    return (int)(b < 1 ? 1 : b);
+}
+extern "C" int lfts_field_factors(lfts_ctx c, const double *w, double coef, void *fac_out) {
+    if (!c || !w || !fac_out) return fail("null argument");
+    if (c->prec == 8)
+        k_field_factors<double><<<grid_for(c->g.M), NTHR, 0, c->stream>>>(w, coef, (double *)fac_out, c->g.M);
+    else
+        k_field_factors<float><<<grid_for(c->g.M), NTHR, 0, c->stream>>>(w, coef, (float *)fac_out, c->g.M);
+    CKLAUNCH();
+    return 0;
+}
+
+// ---------------------------------------------------------------- steps
+template <typename T, bool GEN>
+static int step_cont_t(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) {
+    const GridPlan &g = c->g;
+    cudaStream_t st = c->stream;
+    const dim3 gp(g.n0, nj), gx(c->ntiles, nj);
+    if (c->nbr2) {
+        k_plane_forward<T, 2, GEN><<<gp, NTHR, c->sm_pf2, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0);
+        k_xpass<T, 2, GEN><<<gx, NTHR, c->sm_x2, st>>>(g, jobs, 0, 0, 1, c->TJ);
+    } else {
+        k_plane_forward<T, 1, GEN><<<gp, NTHR, c->sm_pf1, st>>>(g, jobs, s, FM_FAC_SQ, 0, 0);
+        k_plane_forward<T, 1, GEN><<<gp, NTHR, c->sm_pf1, st>>>(g, jobs, s, FM_FAC, 0, 1);
+        k_xpass<T, 1, GEN><<<gx, NTHR, c->sm_x1, st>>>(g, jobs, 0, 0, 0, c->TJ);
+        k_xpass<T, 1, GEN><<<gx, NTHR, c->sm_x1, st>>>(g, jobs, 1, 1, 1, c->TJ);
+    }
+    k_plane_mid<T, GEN><<<gp, NTHR, c->sm_mid, st>>>(g, jobs, 1);
+    k_xpass<T, 1, GEN><<<gx, NTHR, c->sm_x1, st>>>(g, jobs, 1, 1, 1, c->TJ);
+    if (c->nbr2) {
+        k_plane_inverse<T, 2, EPI_RICH, GEN><<<gp, NTHR, c->sm_inv2, st>>>(g, jobs, s, 0, 0);
+    } else {
+        k_plane_inverse<T, 1, EPI_SCALE, GEN><<<gp, NTHR, c->sm_inv1, st>>>(g, jobs, s, 0, FM_FAC_SQ);
+        k_plane_inverse<T, 1, EPI_RICH_ACC, GEN><<<gp, NTHR, c->sm_inv1, st>>>(g, jobs, s, 1, 0);
+    }
+    CKLAUNCH();
+    return 0;
+}
+extern "C" int lfts_step_continuous(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) {
+    if (!c || !jobs) return fail("null argument");
+    if (nj <= 0) return 0;
+    if (nj > 65535) return fail("too many jobs in one launch (max 65535)");
+    if (c->prec == 8) return c->gen ? step_cont_t<double, true>(c, jobs, nj, s) : step_cont_t<double, false>(c, jobs, nj, s);
+    return c->gen ? step_cont_t<float, true>(c, jobs, nj, s) : step_cont_t<float, false>(c, jobs, nj, s);
+}
+
+template <typename T, bool GEN>
+static int step_disc_t(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, int half, int with_fac) {
+    const GridPlan &g = c->g;
+    cudaStream_t st = c->stream;
+    const dim3 gp(g.n0, nj), gx(c->ntiles, nj);
+    k_plane_forward<T, 1, GEN><<<gp, NTHR, c->sm_pf1, st>>>(g, jobs, s, FM_NONE, 0, 0);
+    k_xpass<T, 1, GEN><<<gx, NTHR, c->sm_x1, st>>>(g, jobs, 0, half, half, c->TJ);
+    k_plane_inverse<T, 1, EPI_SCALE, GEN><<<gp, NTHR, c->sm_inv1, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
+    CKLAUNCH();
+    return 0;
+}
+extern "C" int lfts_step_discrete(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, int half, int with_fac) {
+    if (!c || !jobs) return fail("null argument");
+    if (nj <= 0) return 0;
+    if (nj > 65535) return fail("too many jobs in one launch (max 65535)");
+    half = half ? 1 : 0;
+    if (c->prec == 8)
+        return c->gen ? step_disc_t<double, true>(c, jobs, nj, s, half, with_fac) : step_disc_t<double, false>(c, jobs, nj, s, half, with_fac);
+    return c->gen ? step_disc_t<float, true>(c, jobs, nj, s, half, with_fac) : step_disc_t<float, false>(c, jobs, nj, s, half, with_fac);
+}
+
+// ---------------------------------------------------------------- junctions
+template <typename T>
+__global__ void k_junctions(const lfts_junction_job *__restrict__ jobs, const void *const *__restrict__ deps,
+                            const double *__restrict__ wts, long long M) {
+    const lfts_junction_job jb = jobs[blockIdx.y];
+    T *out = (T *)jb.out;
+    const T *fac = (const T *)jb.fac;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M; i += (long long)gridDim.x * blockDim.x) {
+        T v;
+        if (jb.ndeps == 0) {
+            v = (T)1;
+        } else if (jb.mode == 0) {
+            v = (T)1;
+            for (int d = 0; d < jb.ndeps; d++) v *= ((const T *)deps[jb.dep_offset + d])[i];
+        } else {
+            v = (T)0;
+            for (int d = 0; d < jb.ndeps; d++) v += ((const T *)deps[jb.dep_offset + d])[i] * (T)wts[jb.dep_offset + d];
+        }
+        if (fac) v *= fac[i];
+        out[i] = v;
+    }
+}
+extern "C" int lfts_junctions(lfts_ctx c, const lfts_junction_job *jobs, int nj, const void *const *dep_ptrs,
+                              const double *dep_weights) {
+    if (!c || !jobs) return fail("null argument");
+    if (nj <= 0) return 0;
+    long long b = (c->g.M + NTHR - 1) / NTHR;
+    if (b > 1024) b = 1024;
+    const dim3 grid((unsigned)b, nj);
+    if (c->prec == 8) k_junctions<double><<<grid, NTHR, 0, c->stream>>>(jobs, dep_ptrs, dep_weights, c->g.M);
+    else k_junctions<float><<<grid, NTHR, 0, c->stream>>>(jobs, dep_ptrs, dep_weights, c->g.M);
+    CKLAUNCH();
+    return 0;
+}
+
+// ---------------------------------------------------------------- reductions
+// warp + block sum of a double (block of NTHR threads); result valid in thread 0
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    v = 0;
+    if (w == 0) {
+        v = lane < NWARP ? sh[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+constexpr int DOT_CHUNKS = 128;
+
+template <typename T>
+__global__ void __launch_bounds__(NTHR) k_dots(const lfts_dot_job *__restrict__ jobs, long long M, double *partials) {
+    __shared__ double sh[NWARP];
+    const lfts_dot_job jb = jobs[blockIdx.y];
+    const T *a = (const T *)jb.a, *b = (const T *)jb.b, *w = (const T *)jb.w;
+    double acc = 0.0;
+    for (long long i = blockIdx.x * (long long)NTHR + threadIdx.x; i < M; i += (long long)gridDim.x * NTHR) {
+        double v = (double)a[i] * (double)b[i];
+        if (w) v /= (double)w[i];
+        acc += v;
+    }
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) partials[(long long)blockIdx.y * gridDim.x + blockIdx.x] = acc;
+}
+__global__ void __launch_bounds__(NTHR) k_finish(const double *__restrict__ partials, int nparts, const double *scale_src,
+                                                 int scale_stride, double mult, double *out, int out_stride, int ncomp) {
+    // job = blockIdx.x; component = blockIdx.y; partials[(job*nparts + p)*ncomp + comp]
+    __shared__ double sh[NWARP];
+    const int j = blockIdx.x, d = blockIdx.y;
+    double acc = 0.0;
+    for (int p = threadIdx.x; p < nparts; p += NTHR) acc += partials[((long long)j * nparts + p) * ncomp + d];
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) {
+        const double sc = scale_src ? *(const double *)((const char *)scale_src + (long long)j * scale_stride) : 1.0;
+        out[(long long)j * out_stride + d] = acc * sc * mult;
+    }
+}
+extern "C" int lfts_dots(lfts_ctx c, const lfts_dot_job *jobs, int nj, double *out) {
+    if (!c || !jobs || !out) return fail("null argument");
+    for (int j0 = 0; j0 < nj; j0 += 4096) {
+        const int n = nj - j0 < 4096 ? nj - j0 : 4096;
+        const dim3 grid(DOT_CHUNKS, n);
+        if (c->prec == 8) k_dots<double><<<grid, NTHR, 0, c->stream>>>(jobs + j0, c->g.M, c->partials);
+        else k_dots<float><<<grid, NTHR, 0, c->stream>>>(jobs + j0, c->g.M, c->partials);
+        k_finish<<<dim3(n, 1), NTHR, 0, c->stream>>>(c->partials, DOT_CHUNKS, (const double *)&jobs[j0].scale,
+                                                    (int)sizeof(lfts_dot_job), 1.0, out + j0, 1, 1);
+    }
+    CKLAUNCH();
+    return 0;
+}
+
+// block concentrations
+template <typename T, int MODEL>
+__global__ void __launch_bounds__(NTHR) k_phi(const lfts_phi_job *__restrict__ jobs, const double *__restrict__ coefs,
+                                              long long M) {
+    const lfts_phi_job jb = jobs[blockIdx.y];
+    const T *ql = (const T *)jb.q_left, *qr = (const T *)jb.q_right;
+    for (long long i = blockIdx.x * (long long)NTHR + threadIdx.x; i < M; i += (long long)gridDim.x * NTHR) {
+        double acc = 0.0;
+        if (MODEL == 0) {
+            for (int n = 0; n <= jb.n_right; n++)
+                acc += coefs[jb.coef_offset + n] * (double)ql[(long long)(jb.n_left - n) * M + i] * (double)qr[(long long)n * M + i];
+        } else {
+            for (int n = 1; n <= jb.n_right; n++)
+                acc += (double)ql[(long long)(jb.n_left - n + 1) * M + i] * (double)qr[(long long)n * M + i];
+            acc /= (double)((const T *)jb.fac)[i];
+        }
+        jb.phi[i] = acc * jb.norm;
+    }
+}
+extern "C" int lfts_phi_blocks(lfts_ctx c, int model, const lfts_phi_job *jobs, int nj, const double *coefs) {
+    if (!c || !jobs) return fail("null argument");
+    if (nj <= 0) return 0;
+    long long b = (c->g.M + NTHR - 1) / NTHR;
+    if (b > 2048) b = 2048;
+    const dim3 grid((unsigned)b, nj);
+    if (c->prec == 8) {
+        if (model == 0) k_phi<double, 0><<<grid, NTHR, 0, c->stream>>>(jobs, coefs, c->g.M);
+        else k_phi<double, 1><<<grid, NTHR, 0, c->stream>>>(jobs, coefs, c->g.M);
+    } else {
+        if (model == 0) k_phi<float, 0><<<grid, NTHR, 0, c->stream>>>(jobs, coefs, c->g.M);
+        else k_phi<float, 1><<<grid, NTHR, 0, c->stream>>>(jobs, coefs, c->g.M);
+    }
+    CKLAUNCH();
+    return 0;
+}
+
+// stress: x-transform of both zy spectra of a job, then the weighted k-sum
+template <typename T, bool GEN>
+__global__ void __launch_bounds__(NTHR) k_xstress(GridPlan g, const lfts_step_job *__restrict__ sj,
+                                                  const lfts_stress_job *__restrict__ jobs, const double *__restrict__ basis,
+                                                  int TJ, double *partials) {
+    using C = typename CT<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double sh[NWARP];
+    const int n0 = g.n0;
+    C *tile = (C *)smem_raw;
+    C *twx = tile + 2 * n0 * TJ;
+    short *px = (short *)(twx + n0);
+    const int job = blockIdx.y;
+    const lfts_step_job jb = sj[2 * job];
+    const T *bond = (const T *)jobs[job].bond;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < n0; i += NTHR) { twx[i] = ((const C *)g.tw[0])[i]; px[i] = g.perm[0][i]; }
+    __syncthreads();
+    const long long plane = (long long)g.n1 * g.nzc;
+    const long long j0 = (long long)blockIdx.x * TJ;
+    const int tot = 2 * n0 * TJ;
+    const C *spec = (const C *)jb.spec;  // two consecutive Mc slots: F_zy[q1], F_zy[q2]
+    for (int i = tid; i < tot; i += NTHR) {
+        const int jj = i % TJ, x = (i / TJ) % n0, b = i / (TJ * n0);
+        C v = cmk<C>(0, 0);
+        if (j0 + jj < plane) v = spec[(size_t)b * g.Mc + x * plane + j0 + jj];
+        tile[(b * n0 + px[x]) * TJ + jj] = v;
+    }
+    __syncthreads();
+    const LineMap lmx = {2 * TJ, TJ, n0 * TJ, TJ};
+    dit_lines<C, true, GEN>(tile, lmx, g.ax[0], twx, -1, tid, NTHR);
+    double acc[3] = {0, 0, 0};
+    for (int i = tid; i < n0 * TJ; i += NTHR) {
+        const int jj = i % TJ, x = i / TJ;
+        if (j0 + jj < plane) {
+            const long long k = x * plane + j0 + jj;
+            const C A = tile[x * TJ + jj], B = tile[(n0 + x) * TJ + jj];
+            double co = (double)A.x * (double)B.x + (double)A.y * (double)B.y;
+            if (bond) co *= (double)bond[k] * (double)g.M;  // tables carry 1/M
+            acc[0] += co * basis[k];
+            acc[1] += co * basis[g.Mc + k];
+            acc[2] += co * basis[2 * g.Mc + k];
+        }
+    }
+    for (int d = 0; d < 3; d++) {
+        const double v = block_sum(acc[d], sh);
+        if (tid == 0) partials[((long long)job * gridDim.x + blockIdx.x) * 3 + d] = v;
+    }
+}
+
+template <typename T>
+__global__ void k_stress_prep(const lfts_stress_job *__restrict__ jobs, int nj, void *spec, long long Mc,
+                              lfts_step_job *sj) {
+    using C = typename CT<T>::type;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nj; j += gridDim.x * blockDim.x) {
+        C *sp = (C *)spec + (size_t)2 * j * Mc;
+        lfts_step_job a = {jobs[j].q1, 0, nullptr, 0, nullptr, nullptr, nullptr, sp};
+        lfts_step_job b = {jobs[j].q2, 0, nullptr, 0, nullptr, nullptr, nullptr, sp + Mc};
+        sj[2 * j] = a;
+        sj[2 * j + 1] = b;
+    }
+}
+
+template <typename T, bool GEN>
+static int stress_t(lfts_ctx c, const lfts_stress_job *jobs, int nj, const double *basis, void *spec, int max_chunk,
+                    double *out) {
+    const GridPlan &g = c->g;
+    cudaStream_t st = c->stream;
+    const size_t smx = sizeof(typename CT<T>::type) * (2 * (size_t)g.n0 * c->TJ + g.n0) + sizeof(short) * g.n0;
+    for (int j0 = 0; j0 < nj; j0 += max_chunk) {
+        const int n = nj - j0 < max_chunk ? nj - j0 : max_chunk;
+        if (2 * n > c->sjobs_cap) return fail("stress chunk too large");
+        if ((size_t)n * c->ntiles * 3 > c->partials_cap) return fail("stress chunk exceeds the partial-sum workspace");
+        k_stress_prep<T><<<(n + 127) / 128, 128, 0, st>>>(jobs + j0, n, spec, g.Mc, c->sjobs);
+        k_plane_forward<T, 1, GEN><<<dim3(g.n0, 2 * n), NTHR, c->sm_pf1, st>>>(g, c->sjobs, 0, FM_NONE, 0, 0);
+        k_xstress<T, GEN><<<dim3(c->ntiles, n), NTHR, smx, st>>>(g, c->sjobs, jobs + j0, basis, c->TJ, c->partials);
+        k_finish<<<dim3(n, 3), NTHR, 0, st>>>(c->partials, c->ntiles, (const double *)&jobs[j0].weight,
+                                             (int)sizeof(lfts_stress_job), 1.0, out + 3 * (long long)j0, 3, 3);
+    }
+    CKLAUNCH();
+    return 0;
+}
+extern "C" int lfts_stress(lfts_ctx c, const lfts_stress_job *jobs, int nj, const double *basis, void *spec,
+                           int max_chunk, double *out) {
+    if (!c || !jobs || !basis || !spec || !out) return fail("null argument");
+    if (nj <= 0) return 0;
+    if (max_chunk <= 0) return fail("max_chunk must be positive");
+    if (c->prec == 8) return c->gen ? stress_t<double, true>(c, jobs, nj, basis, spec, max_chunk, out)
+                                    : stress_t<double, false>(c, jobs, nj, basis, spec, max_chunk, out);
+    return c->gen ? stress_t<float, true>(c, jobs, nj, basis, spec, max_chunk, out)
+                  : stress_t<float, false>(c, jobs, nj, basis, spec, max_chunk, out);
+}
+
+// ---------------------------------------------------------------- Anderson mixing
+__device__ __forceinline__ long long ring_slot(int i, int head, int len) { return (long long)(((head - i) % len + len) % len); }
+
+__global__ void __launch_bounds__(NTHR) k_am_dots(const double *__restrict__ d, const double *__restrict__ hist,
+                                                  long long stride, long long n, double *partials, int head, int len) {
+    __shared__ double sh[NWARP];
+    const double *h = hist + ring_slot(blockIdx.y, head, len) * stride;
+    double acc = 0.0;
+    for (long long i = blockIdx.x * (long long)NTHR + threadIdx.x; i < n; i += (long long)gridDim.x * NTHR) acc += d[i] * h[i];
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) partials[(long long)blockIdx.y * gridDim.x + blockIdx.x] = acc;
+}
+extern "C" int lfts_am_dots(lfts_ctx c, const double *d, const double *hist, long long stride, int nhist, long long n,
+                            double *dots, int head, int ring_len) {
+    if (!c || !d || !hist || !dots) return fail("null argument");
+    if (nhist <= 0) return 0;
+    if (ring_len <= 0 || nhist > ring_len) return fail("invalid history ring");
+    if ((size_t)nhist * DOT_CHUNKS > c->partials_cap) return fail("too many history vectors");
+    k_am_dots<<<dim3(DOT_CHUNKS, nhist), NTHR, 0, c->stream>>>(d, hist, stride, n, c->partials, head, ring_len);
+    k_finish<<<dim3(nhist, 1), NTHR, 0, c->stream>>>(c->partials, DOT_CHUNKS, nullptr, 0, 1.0, dots, 1, 1);
+    CKLAUNCH();
+    return 0;
+}
+__global__ void k_am_update(double *__restrict__ wn, const double *__restrict__ wh, const double *__restrict__ dh,
+                            long long stride, int nh, const double *__restrict__ a, long long n, int head, int len) {
+    const long long s0 = ring_slot(0, head, len) * stride;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double w1 = wh[s0 + i], d1 = dh[s0 + i];
+        double acc = w1 + d1;
+        for (int h = 0; h < nh; h++) {
+            const long long sh = ring_slot(h + 1, head, len) * stride;
+            acc += a[h] * (wh[sh + i] + dh[sh + i] - w1 - d1);
+        }
+        wn[i] = acc;
+    }
+}
+extern "C" int lfts_am_update(lfts_ctx c, double *w_new, const double *w_hist, const double *d_hist, long long stride,
+                              int nh, const double *a, long long n, int head, int ring_len) {
+    if (!c || !w_new || !w_hist || !d_hist) return fail("null argument");
+    if (ring_len <= 0 || nh + 1 > ring_len) return fail("invalid history ring");
+    k_am_update<<<grid_for(n), NTHR, 0, c->stream>>>(w_new, w_hist, d_hist, stride, nh, a, n, head, ring_len);
+    CKLAUNCH();
+    return 0;
+}
+__global__ void k_am_simple(double *__restrict__ wn, const double *__restrict__ w, const double *__restrict__ d,
+                            double mix, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        wn[i] = w[i] + mix * d[i];
+}
+extern "C" int lfts_am_simple(lfts_ctx c, double *w_new, const double *w, const double *d, double mix, long long n) {
+    if (!c || !w_new || !w || !d) return fail("null argument");
+    k_am_simple<<<grid_for(n), NTHR, 0, c->stream>>>(w_new, w, d, mix, n);
+    CKLAUNCH();
+    return 0;
+}
+
+// ---------------------------------------------------------------- helpers
+constexpr int LINCOMB_MAX = 16;
+struct LincombArgs {
+    const double *src[LINCOMB_MAX];
+    double coef[LINCOMB_MAX];
+    int n;
+    int accumulate;
+};
+__global__ void k_lincomb(double *__restrict__ out, LincombArgs a, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double v = a.accumulate ? out[i] : 0.0;
+        for (int k = 0; k < a.n; k++) v += a.coef[k] * a.src[k][i];
+        out[i] = v;
+    }
+}
+extern "C" int lfts_lincomb(lfts_ctx c, double *out, int nsrc, const double *const *srcs, const double *coefs, long long n) {
+    if (!c || !out) return fail("null argument");
+    if (nsrc < 0) return fail("negative source count");
+    int k0 = 0;
+    do {
+        LincombArgs a;
+        a.n = nsrc - k0 < LINCOMB_MAX ? nsrc - k0 : LINCOMB_MAX;
+        a.accumulate = k0 > 0;
+        for (int k = 0; k < a.n; k++) { a.src[k] = srcs[k0 + k]; a.coef[k] = coefs ? coefs[k0 + k] : 1.0; }
+        k_lincomb<<<grid_for(n), NTHR, 0, c->stream>>>(out, a, n);
+        k0 += a.n;
+    } while (k0 < nsrc);
+    CKLAUNCH();
+    return 0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NTHR) k_pow_sum(const T *__restrict__ fac, int power, long long M, double *partials) {
+    __shared__ double sh[NWARP];
+    double acc = 0.0;
+    for (long long i = blockIdx.x * (long long)NTHR + threadIdx.x; i < M; i += (long long)gridDim.x * NTHR) {
+        double f = (double)fac[i], v = f;
+        for (int p = 1; p < power; p++) v *= f;
+        acc += v;
+    }
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+template <typename T>
+__global__ void k_solvent_phi(const T *__restrict__ fac, int power, double vf, const double *__restrict__ Q,
+                              double *__restrict__ phi, long long M) {
+    const double q = *Q;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M; i += (long long)gridDim.x * blockDim.x) {
+        double f = (double)fac[i], v = f;
+        for (int p = 1; p < power; p++) v *= f;
+        phi[i] = vf * v / q;
+    }
+}
+extern "C" int lfts_solvent(lfts_ctx c, const void *fac, int power, double vf, double dv_over_V, double *phi_out,
+                            double *Q_out) {
+    if (!c || !fac || !phi_out || !Q_out) return fail("null argument");
+    if (power < 1) return fail("power must be >= 1");
+    const long long M = c->g.M;
+    if (c->prec == 8) k_pow_sum<double><<<DOT_CHUNKS, NTHR, 0, c->stream>>>((const double *)fac, power, M, c->partials);
+    else k_pow_sum<float><<<DOT_CHUNKS, NTHR, 0, c->stream>>>((const float *)fac, power, M, c->partials);
+    k_finish<<<dim3(1, 1), NTHR, 0, c->stream>>>(c->partials, DOT_CHUNKS, nullptr, 0, dv_over_V, Q_out, 1, 1);
+    if (c->prec == 8) k_solvent_phi<double><<<grid_for(M), NTHR, 0, c->stream>>>((const double *)fac, power, vf, Q_out, phi_out, M);
+    else k_solvent_phi<float><<<grid_for(M), NTHR, 0, c->stream>>>((const float *)fac, power, vf, Q_out, phi_out, M);
+    CKLAUNCH();
+    return 0;
+}
