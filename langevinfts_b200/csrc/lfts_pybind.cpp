@@ -1,0 +1,312 @@
+// pybind11 module `langevinfts`: the reference's Python-facing API
+// (src/pybind11/langevinfts.cpp:24-463) over the B200 engine.
+// Same class and method names, argument meaning, size checks and errors; the
+// platform is "cuda" (FP64) or "cuda-fp32" (FP32 propagators and FFTs, FP64
+// reductions).
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include <iostream>
+
+#include "lfts_computation.h"
+#include "lfts_host.h"
+
+namespace py = pybind11;
+using namespace lfts;
+
+namespace {
+
+struct Factory {
+    int precision = 8;
+    bool reduce_memory = false;
+    int device = 0;
+    std::string name = "cuda";
+};
+
+struct PlatformSelector {
+    static std::vector<std::string> avail_platforms() { return {"cuda", "cuda-fp32"}; }
+    static Factory *create_factory(const std::string &platform, bool reduce_memory) {
+        Factory *f = new Factory();
+        if (platform == "cuda") {
+            f->precision = 8;
+        } else if (platform == "cuda-fp32") {
+            f->precision = 4;
+        } else {
+            delete f;
+            LFTS_THROW("Could not find platform '" + platform + "'");
+        }
+        f->name = platform;
+        f->reduce_memory = reduce_memory;
+        if (reduce_memory)
+            std::cout << "(warning) every propagator is kept in GPU memory; the reduce_memory_usage option is ignored."
+                      << std::endl;
+        return f;
+    }
+};
+
+void size_check(const py::buffer_info &b, long long n, const std::string &what, const std::string &against) {
+    if (b.size != n)
+        throw std::runtime_error("Size of input " + what + "(" + std::to_string(b.size) + ") and '" + against + "' (" +
+                                 std::to_string(n) + ") must match");
+}
+
+std::map<std::string, const double *> field_map(std::map<std::string, py::array_t<double, py::array::c_style | py::array::forcecast>> &in,
+                                                long long M, const char *tag) {
+    std::map<std::string, const double *> out;
+    for (auto &kv : in) {
+        py::buffer_info b = kv.second.request();
+        size_check(b, M, std::string(tag) + "[" + kv.first + "] ", "n_grid");
+        out[kv.first] = (const double *)b.ptr;
+    }
+    return out;
+}
+
+using Arr = py::array_t<double, py::array::c_style | py::array::forcecast>;
+
+}  // namespace
+
+PYBIND11_MODULE(langevinfts, m) {
+    m.doc() = "langevinfts chain-propagator solver on NVIDIA B200 (sm_100a)";
+
+    py::class_<ComputationBox>(m, "ComputationBox")
+        .def("get_dim", &ComputationBox::get_dim)
+        .def("get_nx", py::overload_cast<>(&ComputationBox::get_nx, py::const_))
+        .def("get_nx", py::overload_cast<int>(&ComputationBox::get_nx, py::const_))
+        .def("get_lx", py::overload_cast<>(&ComputationBox::get_lx, py::const_))
+        .def("get_lx", py::overload_cast<int>(&ComputationBox::get_lx, py::const_))
+        .def("get_dx", py::overload_cast<>(&ComputationBox::get_dx, py::const_))
+        .def("get_dx", py::overload_cast<int>(&ComputationBox::get_dx, py::const_))
+        .def("get_dv", &ComputationBox::get_dv)
+        .def("get_n_grid", &ComputationBox::get_n_grid)
+        .def("get_volume", &ComputationBox::get_volume)
+        .def("set_lx", &ComputationBox::set_lx)
+        .def("integral", [](ComputationBox &cb, Arr g) {
+            py::buffer_info b = g.request();
+            size_check(b, cb.get_n_grid(), "", "n_grid");
+            return cb.integral((const double *)b.ptr);
+        })
+        .def("inner_product", [](ComputationBox &cb, Arr g, Arr h) {
+            py::buffer_info bg = g.request(), bh = h.request();
+            size_check(bg, cb.get_n_grid(), "", "n_grid");
+            size_check(bh, cb.get_n_grid(), "", "n_grid");
+            return cb.inner_product((const double *)bg.ptr, (const double *)bh.ptr);
+        });
+
+    py::class_<Block>(m, "Block")
+        .def_readonly("monomer_type", &Block::monomer_type)
+        .def_readonly("n_segment", &Block::n_segment)
+        .def_readonly("contour_length", &Block::contour_length)
+        .def_readonly("v", &Block::v)
+        .def_readonly("u", &Block::u);
+
+    py::class_<Polymer>(m, "Polymer")
+        .def("get_alpha", &Polymer::get_alpha)
+        .def("get_volume_fraction", &Polymer::get_volume_fraction)
+        .def("get_n_blocks", &Polymer::get_n_blocks)
+        .def("get_blocks", &Polymer::get_blocks, py::return_value_policy::reference_internal)
+        .def("get_block", &Polymer::get_block, py::return_value_policy::reference_internal)
+        .def("get_n_segment_total", &Polymer::get_n_segment_total)
+        .def("get_n_segment", &Polymer::get_n_segment)
+        .def("get_block_index_from_edge", &Polymer::get_block_index_from_edge)
+        .def("get_adjacent_nodes", &Polymer::get_adjacent_nodes)
+        .def("get_block_indexes", &Polymer::get_block_indexes)
+        .def("get_propagator_key", &Polymer::get_propagator_key);
+
+    auto blocks_from_py = [](const std::vector<std::vector<py::object>> &list) {
+        std::vector<BlockInput> out;
+        for (const auto &b : list) {
+            if (b.size() < 4) throw std::runtime_error("each block must be [monomer_type, contour_length, v, u]");
+            out.push_back({py::cast<std::string>(b[0]), py::cast<double>(b[1]), py::cast<int>(b[2]), py::cast<int>(b[3])});
+        }
+        return out;
+    };
+    py::class_<Molecules>(m, "Molecules")
+        .def(py::init<std::string, double, std::map<std::string, double>>())
+        .def("get_model_name", &Molecules::get_model_name)
+        .def("get_ds", &Molecules::get_ds)
+        .def("get_bond_lengths", &Molecules::get_bond_lengths)
+        .def("get_n_polymer_types", &Molecules::get_n_polymer_types)
+        .def("add_polymer", [blocks_from_py](Molecules &mol, double vf, std::vector<std::vector<py::object>> blocks) {
+            mol.add_polymer(vf, blocks_from_py(blocks), {});
+        })
+        .def("add_polymer", [blocks_from_py](Molecules &mol, double vf, std::vector<std::vector<py::object>> blocks,
+                                             std::map<int, std::string> q_init) {
+            mol.add_polymer(vf, blocks_from_py(blocks), q_init);
+        })
+        .def("get_polymer", &Molecules::get_polymer, py::return_value_policy::reference_internal)
+        .def("get_n_solvent_types", &Molecules::get_n_solvent_types)
+        .def("add_solvent", &Molecules::add_solvent);
+
+    auto edge_dict = [](const ComputationEdge &e) {
+        py::dict d;
+        d["max_n_segment"] = e.max_n_segment;
+        d["monomer_type"] = e.monomer_type;
+        d["deps"] = e.deps;
+        d["height"] = e.height;
+        d["junction_ends"] = std::vector<int>(e.junction_ends.begin(), e.junction_ends.end());
+        return d;
+    };
+    auto block_dict = [](const ComputationBlock &b) {
+        py::dict d;
+        d["monomer_type"] = b.monomer_type;
+        d["n_segment_left"] = b.n_segment_left;
+        d["n_segment_right"] = b.n_segment_right;
+        d["n_repeated"] = b.n_repeated;
+        d["v_u"] = b.v_u;
+        return d;
+    };
+    py::class_<PropagatorAnalyzer>(m, "PropagatorAnalyzer")
+        .def("get_computation_propagators()", [edge_dict](PropagatorAnalyzer &pa) {
+            py::list out;  // keeps the analyzer's key order
+            for (const auto &it : pa.get_computation_propagators()) out.append(py::make_tuple(it.first, edge_dict(it.second)));
+            return out;
+        })
+        .def("get_computation_propagators", [edge_dict](PropagatorAnalyzer &pa) {
+            py::list out;
+            for (const auto &it : pa.get_computation_propagators()) out.append(py::make_tuple(it.first, edge_dict(it.second)));
+            return out;
+        })
+        .def("get_computation_propagator", [edge_dict](PropagatorAnalyzer &pa, const std::string &key) {
+            return edge_dict(pa.get_computation_propagator(key));
+        })
+        .def("get_computation_blocks", [block_dict](PropagatorAnalyzer &pa) {
+            py::list out;
+            for (const auto &it : pa.get_computation_blocks()) out.append(py::make_tuple(it.first, block_dict(it.second)));
+            return out;
+        })
+        .def("get_computation_block", [block_dict](PropagatorAnalyzer &pa, std::tuple<int, std::string, std::string> key) {
+            return block_dict(pa.get_computation_block(key));
+        })
+        .def("display_propagators", &PropagatorAnalyzer::display_propagators)
+        .def("display_blocks", &PropagatorAnalyzer::display_blocks)
+        .def("get_deps_from_key", [](PropagatorAnalyzer &, const std::string &key) { return code::deps_from_key(key); })
+        .def("get_monomer_type_from_key", [](PropagatorAnalyzer &, const std::string &key) { return code::monomer_type_from_key(key); })
+        .def("get_schedule", [](PropagatorAnalyzer &pa, int n_streams) {
+            Scheduler s(pa.get_computation_propagators(), n_streams);
+            return s.get_schedule();
+        }, py::arg("n_streams") = 4);
+
+    py::class_<GpuComputation>(m, "PropagatorComputation")
+        .def("update_laplacian_operator", &GpuComputation::update_laplacian_operator)
+        .def("compute_propagators", [](GpuComputation &c, std::map<std::string, Arr> w, py::object q_init) {
+            const long long M = c.get_n_grid();
+            auto wm = field_map(w, M, "w");
+            std::map<std::string, Arr> qi;
+            if (!q_init.is_none()) qi = q_init.cast<std::map<std::string, Arr>>();
+            auto qm = field_map(qi, M, "q");
+            py::gil_scoped_release nogil;
+            c.compute_propagators(wm, qm);
+        }, py::arg("w_input"), py::arg("q_init") = py::none())
+        .def("compute_concentrations", [](GpuComputation &c) {
+            py::gil_scoped_release nogil;
+            c.compute_concentrations();
+        })
+        .def("compute_statistics", [](GpuComputation &c, std::map<std::string, Arr> w, py::object q_init) {
+            const long long M = c.get_n_grid();
+            auto wm = field_map(w, M, "w");
+            std::map<std::string, Arr> qi;
+            if (!q_init.is_none()) qi = q_init.cast<std::map<std::string, Arr>>();
+            auto qm = field_map(qi, M, "q");
+            py::gil_scoped_release nogil;
+            c.compute_statistics(wm, qm);
+        }, py::arg("w_input"), py::arg("q_init") = py::none())
+        .def("get_total_concentration", [](GpuComputation &c, const std::string &type) {
+            py::array_t<double> phi(c.get_n_grid());
+            c.get_total_concentration(type, (double *)phi.request().ptr);
+            return phi;
+        })
+        .def("get_total_concentration", [](GpuComputation &c, int p, const std::string &type) {
+            py::array_t<double> phi(c.get_n_grid());
+            c.get_total_concentration(p, type, (double *)phi.request().ptr);
+            return phi;
+        })
+        .def("get_total_concentration_gce", [](GpuComputation &c, double fugacity, int p, const std::string &type) {
+            py::array_t<double> phi(c.get_n_grid());
+            c.get_total_concentration_gce(fugacity, p, type, (double *)phi.request().ptr);
+            return phi;
+        })
+        .def("get_block_concentration", [](GpuComputation &c, int p) {
+            py::array_t<double> phi({(py::ssize_t)c.get_n_blocks(p), (py::ssize_t)c.get_n_grid()});
+            c.get_block_concentration(p, (double *)phi.request().ptr);
+            return phi;
+        })
+        .def("get_total_partition", &GpuComputation::get_total_partition)
+        .def("get_solvent_partition", &GpuComputation::get_solvent_partition)
+        .def("get_solvent_concentration", [](GpuComputation &c, int s) {
+            py::array_t<double> phi(c.get_n_grid());
+            c.get_solvent_concentration(s, (double *)phi.request().ptr);
+            return phi;
+        })
+        .def("get_chain_propagator", [](GpuComputation &c, int p, int v, int u, int n) {
+            py::array_t<double> q(c.get_n_grid());
+            c.get_chain_propagator((double *)q.request().ptr, p, v, u, n);
+            return q;
+        })
+        .def("compute_stress", [](GpuComputation &c) {
+            py::gil_scoped_release nogil;
+            c.compute_stress();
+        })
+        .def("get_stress", &GpuComputation::get_stress)
+        .def("get_stress_gce", &GpuComputation::get_stress_gce)
+        .def("check_total_partition", &GpuComputation::check_total_partition)
+        .def("get_n_grid", &GpuComputation::get_n_grid)
+        .def("get_precision", &GpuComputation::get_precision);
+
+    py::class_<GpuAndersonMixing>(m, "AndersonMixing")
+        .def("reset_count", &GpuAndersonMixing::reset_count)
+        .def("get_n_var", &GpuAndersonMixing::get_n_var)
+        .def("calculate_new_fields", [](GpuAndersonMixing &am, Arr w_current, Arr w_deriv, double old_err, double err) {
+            const long long n = am.get_n_var();
+            py::array_t<double> w_new(n);
+            py::buffer_info bc = w_current.request(), bd = w_deriv.request();
+            size_check(bc, n, "w_current ", "n_var");
+            size_check(bd, n, "w_deriv ", "n_var");
+            double *out = (double *)w_new.request().ptr;
+            {
+                py::gil_scoped_release nogil;
+                am.calculate_new_fields(out, (const double *)bc.ptr, (const double *)bd.ptr, old_err, err);
+            }
+            return w_new;
+        });
+
+    py::class_<Factory>(m, "AbstractFactory")
+        .def("create_array", [](Factory &, unsigned int) -> py::object {
+            throw std::runtime_error("Array is not part of this build (the solver API works on numpy arrays)");
+        })
+        .def("create_computation_box", [](Factory &, std::vector<int> nx, std::vector<double> lx, py::object bc, py::object mask) {
+            std::vector<std::string> bcv;
+            if (!bc.is_none()) bcv = bc.cast<std::vector<std::string>>();
+            if (!mask.is_none()) throw std::runtime_error("mask (impenetrable regions) is not supported by this build");
+            return new ComputationBox(nx, lx, bcv);
+        }, py::arg("nx"), py::arg("lx"), py::arg("bc") = py::none(), py::arg("mask") = py::none())
+        .def("create_molecules_information", [](Factory &, std::string model, double ds, std::map<std::string, double> bonds) {
+            return new Molecules(model, ds, bonds);
+        })
+        .def("create_propagator_analyzer", [](Factory &, Molecules *mol, bool aggregate) {
+            return new PropagatorAnalyzer(mol, aggregate);
+        }, py::keep_alive<0, 2>())
+        .def("create_pseudospectral_solver", [](Factory &f, ComputationBox *cb, Molecules *mol, PropagatorAnalyzer *pa) {
+            if (pa->get_model_name() != mol->get_model_name())
+                throw std::runtime_error("molecules and propagator analyzer use different chain models");
+            return new GpuComputation(cb, mol, pa, f.precision, f.device);
+        }, py::keep_alive<0, 2>(), py::keep_alive<0, 3>(), py::keep_alive<0, 4>())
+        .def("create_realspace_solver", [](Factory &, py::object, py::object, py::object) -> py::object {
+            throw std::runtime_error("The real-space (Crank-Nicolson) solver is not part of this build");
+        })
+        .def("create_anderson_mixing", [](Factory &f, int n_var, int max_hist, double start_error, double mix_min, double mix_init) {
+            return new GpuAndersonMixing(n_var, max_hist, start_error, mix_min, mix_init, f.device);
+        })
+        .def("display_info", [](Factory &f) {
+            std::cout << "==================== B200 engine ====================" << std::endl;
+            std::cout << "Platform: " << f.name << " (" << (f.precision == 8 ? "FP64" : "FP32 propagators, FP64 reductions")
+                      << "), device " << f.device << std::endl;
+        })
+        .def("get_model_name", [](Factory &) { return std::string(""); });
+
+    py::class_<PlatformSelector>(m, "PlatformSelector")
+        .def(py::init<>())
+        .def_static("avail_platforms", &PlatformSelector::avail_platforms)
+        .def_static("create_factory", [](const std::string &p) { return PlatformSelector::create_factory(p, false); })
+        .def_static("create_factory", &PlatformSelector::create_factory);
+}
