@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Benchmark: batched L-FTS Langevin steps/s on B200.
+
+Workload (one "step" = one Langevin step of every replica, each replica doing
+its Leimkuhler-Matthews update and its Anderson-mixing saddle-point search to
+error 1e-4): AB diblock f=0.5, chiN=17, nbar=100, continuous chain N=90
+(ds=1/90), grid 64^3, box 7.3 R0, dt=0.8, 64 replicas per GPU, FP64.  Replica r
+has seed 1000+r (PCG64) for its initial Normal(0,1) fields and its noise.
+Synthetic data; nothing is read from disk.
+
+  value     replica-steps/s with this step's noise already in HBM
+  e2e       the same through the public BatchedLFTS.step API: noise drawn on
+            the host (PCG64, as the reference driver draws it), copied in, the
+            per-replica statistics copied out, every step
+  roofline  the fused continuous contour step (lfts_step_continuous) at the
+            workload's batch shape, timed with CUDA events on its stream
+  cpu_baseline / --impl reference
+            the reference's own CPU platform (oracle/_ref, OpenMP over
+            propagators) through the same driver on this host
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Langevin steps/s @ saddle err 1e-4 (batched L-FTS, plain FP64)"
+UNIT = "replica-steps/s"
+# mean saddle-point iterations per Langevin step of this workload, measured by
+# the GPU arm on B200 (the algorithm and inputs are the reference's, so the
+# reference arm uses it to convert its timed saddle iterations into steps/s)
+ITERS_PER_STEP = 13.9
+
+
+def params(nx=64, lx=7.3):
+    return {
+        "nx": [nx] * 3, "lx": [lx] * 3, "chain_model": "continuous", "ds": 1 / 90,
+        "segment_lengths": {"A": 1.0, "B": 1.0}, "chi_n": {"A,B": 17.0},
+        "distinct_polymers": [{"volume_fraction": 1.0, "blocks": [{"type": "A", "length": 0.5}, {"type": "B", "length": 0.5}]}],
+        "langevin": {"dt": 0.8, "nbar": 100}, "saddle": {"max_iter": 100, "tolerance": 1e-4},
+        "am": {"max_hist": 20, "start_error": 5e-1, "mix_min": 0.01, "mix_init": 0.01},
+    }
+
+
+def initial_fields(seed, M):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return {"A": rng.normal(0.0, 1.0, M), "B": rng.normal(0.0, 1.0, M)}
+
+
+class Clocks:
+    """nvidia-smi clock/throttle samples during a timed region."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            out, _ = self.proc.communicate(timeout=10)
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_reference():
+    """The reference CPU build (oracle/_ref), loaded under a private name."""
+    import glob
+    import importlib.machinery
+    import importlib.util
+    hits = glob.glob(os.path.join(ROOT, "oracle", "_ref", "langevinfts*.so"))
+    if not hits:
+        return None
+    loader = importlib.machinery.ExtensionFileLoader("langevinfts", hits[0])
+    spec = importlib.util.spec_from_file_location("langevinfts", hits[0], loader=loader)
+    mod = importlib.util.module_from_spec(spec)
+    loader.exec_module(mod)
+    return mod
+
+
+def reference_sample(n_iter, threads):
+    """Time n_iter saddle-point iterations of one replica on the reference CPU
+    platform through the same driver; returns (seconds per iteration, threads)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    ref = load_reference()
+    if ref is None:
+        return None
+    from langevinfts_b200.lfts import LFTS
+    p = params()
+    sim = LFTS(p, random_seed=1000, module=ref, platform="cpu-mkl")
+    M = sim.M
+    w = initial_fields(1000, M)
+    S = len(sim.monomer_types)
+    w_aux = sim.mpt.to_aux_fields(np.array([w[t] for t in sim.monomer_types]))
+    sim.am.reset_count()
+    ts = []
+    err = 1e20
+    for _ in range(n_iter + 1):
+        t0 = time.perf_counter()
+        phi = sim.compute_concentrations(w_aux)
+        h = sim.mpt.compute_func_deriv(w_aux, phi, sim.mpt.aux_fields_imag_idx)
+        old, err = err, float(np.max(np.std(h, axis=1)))
+        for c, i in enumerate(sim.mpt.aux_fields_imag_idx):
+            h[c] *= sim.dt_scaling[i]
+        w_aux[sim.mpt.aux_fields_imag_idx] = np.reshape(
+            sim.am.calculate_new_fields(w_aux[sim.mpt.aux_fields_imag_idx], -h, old, err), [len(sim.mpt.aux_fields_imag_idx), M])
+        ts.append(time.perf_counter() - t0)
+    return float(np.mean(ts[1:])), threads
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation on this host."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    ref = load_reference()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) is missing"}))
+        return 0
+    t_all = []
+    for k in range(args.warmup + args.steps):
+        t_iter, _ = reference_sample(1, threads)
+        if k >= args.warmup:
+            t_all.append(t_iter)
+    t_iter = float(np.mean(t_all))
+    v = 1.0 / (t_iter * ITERS_PER_STEP)
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "batched L-FTS AB diblock 64^3 N=90 (reference CPU: one replica)", "grid": [64, 64, 64],
+                      "N": 90, "replicas": 1},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                            "sample": f"one saddle-point iteration per step (1 replica, 64^3, N=90) x {ITERS_PER_STEP} "
+                                      "iterations per Langevin step; reference CPU platform with the project FFT in place of MKL"},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def roofline_step_kernel(nx, njobs, reps=20):
+    """Time lfts_step_continuous at the batch shape of the workload (njobs =
+    replicas x propagators per schedule slot) with CUDA events on its stream.
+    Inputs (njobs * 2 MB propagator slices) exceed the 126 MB L2."""
+    import torch
+    from langevinfts_b200.capi import Context, StepJob, check
+    ctx = Context([nx] * 3, precision=8)
+    M, Mc = ctx.M, ctx.Mc
+    lx = (C.c_double * 3)(7.3, 7.3, 7.3)
+    bond, bondh = ctx.malloc(Mc * 8), ctx.malloc(Mc * 8)
+    check(ctx.lib.lfts_bond_tables(ctx.h, 1.0, 1 / 90, lx, bond, bondh))
+    w = ctx.upload(np.random.default_rng(0).normal(0, 1, M))
+    fac = ctx.malloc(M * 8)
+    check(ctx.lib.lfts_field_factors(ctx.h, w, -1 / 360, fac))
+    q = ctx.malloc(njobs * 2 * M * 8)
+    check(ctx.lib.lfts_memset_async(ctx.h, q, 0, njobs * 2 * M * 8))
+    ones = np.ones(M)
+    for j in range(njobs):
+        ctx.h2d(q + j * 2 * M * 8, ones)
+    spec = ctx.malloc(njobs * 2 * Mc * 16)
+    jobs = (StepJob * njobs)(*[StepJob(q + j * 2 * M * 8, 0, q + (j * 2 + 1) * M * 8, 0, fac, bond, bondh,
+                                       spec + j * 2 * Mc * 16, None, 0, 0) for j in range(njobs)])
+    jp = ctx.upload(np.frombuffer(jobs, dtype=np.uint8))
+    stream = torch.cuda.ExternalStream(ctx.lib.lfts_ctx_stream(ctx.h))
+    for _ in range(3):
+        check(ctx.lib.lfts_step_continuous(ctx.h, jp, njobs, 0))
+    ctx.sync()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    for _ in range(reps):
+        check(ctx.lib.lfts_step_continuous(ctx.h, jp, njobs, 0))
+    ev[1].record(stream)
+    ev[1].synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / reps
+    ctx.close()
+    return ms, M, Mc
+
+
+def run_ours(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    os.environ.setdefault("CUDA_DEVICE_ORDER", "PCI_BUS_ID")
+    from langevinfts_b200 import langevinfts as L
+    from langevinfts_b200.lfts import BatchedLFTS
+
+    R = args.replicas
+    p = params(args.nx)
+    seeds = [1000 + rank * R + r for r in range(R)]
+    f = L.PlatformSelector.create_factory("cuda", False)
+    sim = BatchedLFTS(p, seeds, module=L)
+    M = sim.M
+    st0 = sim.start([initial_fields(s, M) for s in seeds])
+    for _ in range(args.warmup):
+        sim.step()
+    stream = torch.cuda.ExternalStream(sim.engine.stream_ptr())
+    nreal = sim.mpt.R
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- value: noise for the K steps already on the device
+    noises = [torch.from_numpy(sim.draw_noise()).cuda() for _ in range(args.steps)]
+    barrier()
+    iters, fails = [], 0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    k0 = sim.engine.kernel_launches()
+    with Clocks(local) as clk:
+        ev[0].record(stream)
+        for k in range(args.steps):
+            s = sim.engine.step_device(noises[k].data_ptr())
+            iters += s["iterations"]
+            fails += sum(s["failed"])
+        ev[1].record(stream)
+        ev[1].synchronize()
+    barrier()
+    launches = sim.engine.kernel_launches() - k0
+    t = ev[0].elapsed_time(ev[1]) / 1000.0
+    # ---- e2e: public API with host noise in and statistics out every step
+    pool_noise = sim.draw_noise()
+    barrier()
+    e0 = time.perf_counter()
+    ev2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev2[0].record(stream)
+    from concurrent.futures import ThreadPoolExecutor
+    ex = ThreadPoolExecutor(max_workers=1)
+    nxt = ex.submit(sim.draw_noise)
+    d2h = 0
+    for k in range(args.steps):
+        s = sim.step(pool_noise)
+        d2h += 8 * (len(s["error"]) * 3 + len(s["partitions"])) + 8 * R * (1 + 21) * max(s["iterations"])
+        pool_noise = nxt.result()
+        nxt = ex.submit(sim.draw_noise)
+    ev2[1].record(stream)
+    ev2[1].synchronize()
+    t_e2e = max(time.perf_counter() - e0, ev2[0].elapsed_time(ev2[1]) / 1000.0)
+    ex.shutdown(wait=False)
+    if dist is not None:
+        tt = torch.tensor([t, t_e2e], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t, t_e2e = float(tt[0]), float(tt[1])
+    value = world * R * args.steps / t
+    e2e = world * R * args.steps / t_e2e
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    # ---- roofline of the fused continuous step at the workload batch shape
+    njobs = 2 * R  # two propagators per schedule slot (A and B side) per replica
+    ms, Mg, Mcg = roofline_step_kernel(args.nx, njobs)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    s_bytes = 8
+    unit_bytes = s_bytes * (12 * Mg + 24 * Mcg)  # pass-model bytes per (replica, key, contour step)
+    achieved = njobs * unit_bytes / (ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "step_traffic.json")))
+        traffic = prof["dram_bytes_per_job_step"] * njobs
+    except (OSError, KeyError, ValueError):
+        pass
+    # ---- CPU baseline: the reference CPU platform on a bounded sample
+    cpu = None
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        r = reference_sample(1, threads)
+        if r is not None:
+            mean_iters = float(np.mean(iters)) if iters else ITERS_PER_STEP
+            cpu = {"value": 1.0 / (r[0] * mean_iters), "unit": UNIT, "cores": r[1], "kind": "reference",
+                   "sample": f"2 saddle-point iterations of 1 replica (64^3, N=90) on the reference CPU platform "
+                             f"(first discarded), {r[0]:.2f} s/iteration x {mean_iters:.1f} iterations per step measured above"}
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"batched L-FTS: {R} replicas/GPU of AB diblock f=0.5 chiN=17 nbar=100 N=90, "
+                               f"{args.nx}^3 box 7.3, dt=0.8, saddle tol 1e-4, AM max_hist 20",
+                   "replicas_per_gpu": R, "grid": [args.nx] * 3, "N": 90, "parallelism": f"replicas x{world}",
+                   "l2": "inputs (64 replicas x 4 propagators x 46 slices x 2 MB) far exceed the 126 MB L2",
+                   "mean_saddle_iterations": float(np.mean(iters)) if iters else None, "failed_steps": fails,
+                   "initial_saddle_iterations": max(st0["iterations"])},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": R * nreal * M * 8,
+                "d2h_bytes_per_step": int(d2h / max(args.steps, 1))},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "lfts_step_continuous (5 fused FFT-pass kernels)",
+                     "launch_ms": ms, "jobs_per_launch": njobs,
+                     "bytes_model": "8*(12M+24Mc) per job (pass model), peak = measured hbm_gbs"},
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--replicas", type=int, default=64)
+    ap.add_argument("--nx", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -41,6 +41,9 @@ int lfts_ctx_destroy(lfts_ctx ctx);
 int lfts_ctx_set_stream(lfts_ctx ctx, void *stream);
 void *lfts_ctx_stream(lfts_ctx ctx);
 int lfts_ctx_info(lfts_ctx ctx, long long *M, long long *Mc, int *precision);
+/* Number of kernels enqueued through this context so far (kernels replayed by
+ * lfts_graph_launch are not counted; count them at capture). */
+long long lfts_ctx_launches(lfts_ctx ctx);
 /* Message of the last failing call on this thread. */
 const char *lfts_last_error(void);
 
@@ -77,13 +80,18 @@ int lfts_fourier_basis(lfts_ctx ctx, const double *lx, double *basis_out);
  * coef = -ds/4 (continuous: exp(-w ds/4), its square is exp(-w ds/2)) or
  * -ds (discrete).  Replaces update_dw (CudaSolverPseudo.cu:254-343). */
 int lfts_field_factors(lfts_ctx ctx, const double *w, double coef, void *fac_out);
+/* The same for `count` consecutive fields (count*M points, e.g. all replicas). */
+int lfts_field_factors_batch(lfts_ctx ctx, const double *w, double coef, void *fac_out, int count);
 
 /* ---- contour steps ------------------------------------------------------ */
 
 /* One propagation job.  For step index s of a launch, the input slice is
  * in + s*in_stride and the output slice out + s*out_stride (elements of the
  * ctx precision), so one job array covers a whole schedule slot.
- * spec: scratch for two complex half spectra (2*Mc complex elements). */
+ * spec: scratch for two complex half spectra (2*Mc complex elements).
+ * active/replica: when active != NULL the job is skipped unless
+ * active[replica] != 0 (converged replicas of a batch stop without changing
+ * the launch, so a captured graph stays valid). */
 typedef struct {
     const void *in;
     long long in_stride;
@@ -93,6 +101,9 @@ typedef struct {
     const void *bond;       /* bond table (lfts_bond_tables: bond_out) */
     const void *bond_half;  /* half-bond table */
     void *spec;
+    const int *active;
+    int replica;
+    int pad;
 } lfts_step_job;
 
 /* 4th-order Richardson continuous step, q' = (4 q_{ds/2,ds/2} - q_ds)/3, for
@@ -144,7 +155,8 @@ int lfts_dots(lfts_ctx ctx, const lfts_dot_job *jobs, int njobs, double *out);
  *   phi[i] = norm * sum_{n=0}^{NR} c[coef_offset+n] q_left[(NL-n)*M+i] q_right[n*M+i]
  * Discrete (model 1):
  *   phi[i] = norm * sum_{n=1}^{NR} q_left[(NL-n+1)*M+i] q_right[n*M+i] / fac[i]
- * phi (double).  Replaces calculate_phi_one_block + normalisation
+ * (norm divided by *q_div when q_div != NULL); phi (double).
+ * Replaces calculate_phi_one_block + normalisation
  * (CpuComputationContinuous.cpp:371-465, CpuComputationDiscrete.cpp:584-679,
  * CudaComputationContinuous.cu:527-620). */
 typedef struct {
@@ -153,6 +165,7 @@ typedef struct {
     const void *fac;
     double *phi;
     double norm;
+    const double *q_div;  /* NULL, or a device scalar the norm is divided by (Q_p) */
     int n_left;
     int n_right;
     int coef_offset;
@@ -201,6 +214,56 @@ int lfts_lincomb(lfts_ctx ctx, double *out, int nsrc, const double *const *srcs,
  * continuous solvent exp(-w ds)^... of CpuComputationContinuous.cpp:425-436;
  * power 1 with fac = exp(-w ds) the discrete one (CpuComputationDiscrete.cpp:441-452). */
 int lfts_solvent(lfts_ctx ctx, const void *fac, int power, double vf, double dv_over_V, double *phi_out, double *Q_out);
+
+/* ---- batched Langevin FTS (FP64; replicas r < R, fields w_aux[r][S][M]) --- */
+
+#define LFTS_MAX_MONOMERS 8
+
+/* w_mono[i][r][m] = sum_j A[i*S+j] w_aux[r][j][m]: auxiliary -> monomer fields
+ * (SymmetricPolymerTheory.to_monomer_fields, examples/fts/lfts.py:181-182).
+ * A: host S*S; w_mono: host array of S device pointers (each R x M). */
+int lfts_lfts_monomer_fields(lfts_ctx ctx, int R, int S, long long M, const double *A, const double *w_aux,
+                             double *const *w_mono);
+/* out[r][c][m] = scale[c] * dH/dw_aux[idx[c]] (lfts.py:238-262): for i < S-1
+ * 2 h2[i] w_i + h1[i] + sum_j A[j*S+i] phi_j, for i = S-1 sum_j phi_j - 1.
+ * phi: host array of S device pointers (R x M each).  Replicas with
+ * active[r] == 0 are skipped (active may be NULL). */
+int lfts_lfts_field_deriv(lfts_ctx ctx, int R, int S, long long M, int nf, const int *idx, const double *scale,
+                          const double *A, const double *h1, const double *h2, const double *w_aux,
+                          const double *const *phi, double *out, const int *active);
+/* Leimkuhler-Matthews update of the real fields idx[0..nreal-1]
+ * (lfts.py:697-706): w += -dH/dw dt s + (xi_prev + xi_cur)/2 sqrt(s),
+ * s = dt_scaling[c]; xi_* are [R][nreal][M]. */
+int lfts_lfts_langevin(lfts_ctx ctx, int R, int S, long long M, int nreal, const int *idx, const double *A,
+                       const double *h1, const double *h2, const double *const *phi, double dt,
+                       const double *dt_scaling, double *w_aux, const double *xi_prev, const double *xi_cur,
+                       const int *active);
+/* Row moments: for row = r*rows_per_rep + c, x_row = x + r*rep_stride +
+ * c*row_stride (M doubles): mean[row] = <x - center[row]>, msq[row] =
+ * <(x - center[row])^2> (center may be NULL).  partials: >= 128*R*rows_per_rep
+ * doubles of device scratch.  Gives the saddle-point error max_c std (lfts.py:833)
+ * and the field averages of the Hamiltonian (lfts.py:219-235). */
+int lfts_lfts_row_moments(lfts_ctx ctx, const double *x, int R, int rows_per_rep, long long M, long long row_stride,
+                          long long rep_stride, const double *center, double *partials, double *mean, double *msq);
+/* w_aux[r][field] -= mean[r] (zero-mean pressure field, lfts.py:866). */
+int lfts_lfts_subtract_mean(lfts_ctx ctx, double *w_aux, int R, int S, int field, long long M, const double *mean,
+                            const int *active);
+
+/* Batched Anderson mixing: per replica a ring of L slots of n doubles
+ * (hist + (r*L + slot)*n); i-th newest slot = (head[r] - i) mod L.
+ * insert: where flag[r], copy w_cur/d_cur (replica stride *_stride) into slot head[r].
+ * dots:   dots[r*L + i] = d_0 . d_i for i < ndots[r] (partials: >= 64*R*L doubles).
+ * update: mode[r] 0 skip, 1 simple mixing w_cur + mix[r] d_cur, 2 Anderson
+ *         w_0 + d_0 + sum_{h<nh[r]} a[r*L+h] (w_{h+1} + d_{h+1} - w_0 - d_0).
+ * All control arrays are device arrays.  Replaces CpuAndersonMixing.cpp:76-161
+ * for a batch of independent mixers. */
+int lfts_am_batch_insert(lfts_ctx ctx, int R, long long n, int L, const int *head, const int *flag, const double *w_cur,
+                         long long w_stride, const double *d_cur, long long d_stride, double *w_hist, double *d_hist);
+int lfts_am_batch_dots(lfts_ctx ctx, int R, long long n, int L, const int *head, const int *ndots, const double *d_hist,
+                       double *partials, double *dots);
+int lfts_am_batch_update(lfts_ctx ctx, int R, long long n, int L, const int *head, const int *mode, const int *nh,
+                         const double *mix, const double *a, const double *w_cur, long long w_stride, const double *d_cur,
+                         long long d_stride, const double *w_hist, const double *d_hist, double *w_out, long long out_stride);
 
 #ifdef __cplusplus
 }

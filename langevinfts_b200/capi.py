@@ -13,7 +13,8 @@ LIB_PATH = os.path.join(_HERE, "liblfts_b200.so")
 
 class StepJob(C.Structure):
     _fields_ = [("in_", C.c_void_p), ("in_stride", C.c_longlong), ("out", C.c_void_p), ("out_stride", C.c_longlong),
-                ("fac", C.c_void_p), ("bond", C.c_void_p), ("bond_half", C.c_void_p), ("spec", C.c_void_p)]
+                ("fac", C.c_void_p), ("bond", C.c_void_p), ("bond_half", C.c_void_p), ("spec", C.c_void_p),
+                ("active", C.c_void_p), ("replica", C.c_int), ("pad", C.c_int)]
 
 
 class JunctionJob(C.Structure):
@@ -27,8 +28,8 @@ class DotJob(C.Structure):
 
 class PhiJob(C.Structure):
     _fields_ = [("q_left", C.c_void_p), ("q_right", C.c_void_p), ("fac", C.c_void_p), ("phi", C.c_void_p),
-                ("norm", C.c_double), ("n_left", C.c_int), ("n_right", C.c_int), ("coef_offset", C.c_int),
-                ("pad", C.c_int)]
+                ("norm", C.c_double), ("q_div", C.c_void_p), ("n_left", C.c_int), ("n_right", C.c_int),
+                ("coef_offset", C.c_int), ("pad", C.c_int)]
 
 
 class StressJob(C.Structure):
@@ -54,6 +55,7 @@ _SIGS = {
     "lfts_bond_tables": [C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_double), C.c_void_p, C.c_void_p],
     "lfts_fourier_basis": [C.c_void_p, C.POINTER(C.c_double), C.c_void_p],
     "lfts_field_factors": [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p],
+    "lfts_field_factors_batch": [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int],
     "lfts_step_continuous": [C.c_void_p, C.c_void_p, C.c_int, C.c_int],
     "lfts_step_discrete": [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int],
     "lfts_junctions": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],
@@ -66,6 +68,21 @@ _SIGS = {
     "lfts_am_simple": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_longlong],
     "lfts_lincomb": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_longlong],
     "lfts_solvent": [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p],
+    "lfts_lfts_monomer_fields": [C.c_void_p, C.c_int, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p],
+    "lfts_lfts_field_deriv": [C.c_void_p, C.c_int, C.c_int, C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "lfts_lfts_langevin": [C.c_void_p, C.c_int, C.c_int, C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                           C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "lfts_lfts_row_moments": [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_longlong, C.c_longlong, C.c_longlong,
+                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "lfts_lfts_subtract_mean": [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p],
+    "lfts_am_batch_insert": [C.c_void_p, C.c_int, C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                             C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p],
+    "lfts_am_batch_dots": [C.c_void_p, C.c_int, C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                           C.c_void_p],
+    "lfts_am_batch_update": [C.c_void_p, C.c_int, C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                             C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p,
+                             C.c_void_p, C.c_longlong],
 }
 
 _lib = None
@@ -86,13 +103,15 @@ def lib():
         L.lfts_last_error.argtypes = []
         L.lfts_ctx_stream.restype = C.c_void_p
         L.lfts_ctx_stream.argtypes = [C.c_void_p]
+        L.lfts_ctx_launches.restype = C.c_longlong
+        L.lfts_ctx_launches.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
 
 def declared_symbols():
     """Names of every entry point declared in include/lfts_b200.h."""
-    return list(_SIGS) + ["lfts_last_error", "lfts_ctx_stream"]
+    return list(_SIGS) + ["lfts_last_error", "lfts_ctx_stream", "lfts_ctx_launches"]
 
 
 def check(rc):

@@ -60,9 +60,11 @@ static size_t arena_push(std::vector<unsigned char> &a, const std::vector<T> &v)
     return off;
 }
 
-GpuComputation::GpuComputation(ComputationBox *cb, Molecules *mol, PropagatorAnalyzer *pa, int precision, int device)
-    : cb_(cb), mol_(mol), pa_(pa), prec_(precision), esz_(precision) {
+GpuComputation::GpuComputation(ComputationBox *cb, Molecules *mol, PropagatorAnalyzer *pa, int precision, int device,
+                               int n_replicas)
+    : cb_(cb), mol_(mol), pa_(pa), prec_(precision), R_(n_replicas), esz_(precision) {
     if (!cb || !mol || !pa) LFTS_THROW("null ComputationBox, Molecules or PropagatorAnalyzer");
+    if (n_replicas < 1) LFTS_THROW("n_replicas must be positive");
     if (pa->get_computation_propagators().empty()) LFTS_THROW("There is no propagator code. Add polymers first.");
     if (pa->get_computation_blocks().empty()) LFTS_THROW("There is no block. Add polymers first.");
     continuous_ = mol->get_model_name() == "continuous";
@@ -70,38 +72,46 @@ GpuComputation::GpuComputation(ComputationBox *cb, Molecules *mol, PropagatorAna
     check_rc(lfts_ctx_create(&ctx_, device, (int)nx.size(), nx.data(), precision));
     check_rc(lfts_ctx_info(ctx_, &M_, &Mc_, nullptr));
     if (const char *e = std::getenv("LFTS_NO_GRAPH")) use_graph_ = std::string(e) != "1";
+    const size_t RM = (size_t)R_ * M_;
 
     for (const auto &kv : mol->get_bond_lengths()) {
         TypeStore &t = types_[kv.first];
-        t.w.alloc(ctx_, sizeof(double) * M_);
-        t.fac.alloc(ctx_, esz_ * M_);
+        t.w.alloc(ctx_, sizeof(double) * RM);
+        t.fac.alloc(ctx_, esz_ * RM);
         t.bond.alloc(ctx_, esz_ * Mc_);
         t.bond_half.alloc(ctx_, esz_ * Mc_);
+        phi_type_[kv.first].alloc(ctx_, sizeof(double) * RM);
     }
     for (const auto &it : pa->get_computation_propagators()) {
         KeyStore &ks = keys_[it.first];
-        ks.q.alloc(ctx_, esz_ * M_ * (it.second.max_n_segment + 1));
+        ks.q.alloc(ctx_, esz_ * RM * (it.second.max_n_segment + 1));
         if (!continuous_) {
-            if (!it.second.deps.empty()) ks.half[0].alloc(ctx_, esz_ * M_);
+            if (!it.second.deps.empty()) ks.half[0].alloc(ctx_, esz_ * RM);
             for (int n : it.second.junction_ends)
-                if (n >= 1 && n <= it.second.max_n_segment && !ks.half.count(n)) ks.half[n].alloc(ctx_, esz_ * M_);
+                if (n >= 1 && n <= it.second.max_n_segment && !ks.half.count(n)) ks.half[n].alloc(ctx_, esz_ * RM);
         }
         if (it.first[0] == '{') {
             const std::string name = code::q_input_from_key(it.first);
-            if (!q_init_.count(name)) q_init_[name].alloc(ctx_, esz_ * M_);
+            if (!q_init_.count(name)) q_init_[name].alloc(ctx_, esz_ * RM);
         }
     }
     for (const auto &it : pa->get_computation_blocks()) {
-        phi_block_[it.first].alloc(ctx_, sizeof(double) * M_);
+        phi_block_[it.first].alloc(ctx_, sizeof(double) * RM);
         block_order_.push_back(it.first);
     }
-    for (int s = 0; s < mol->get_n_solvent_types(); s++) phi_solvent_.emplace_back(ctx_, sizeof(double) * M_);
+    for (int s = 0; s < mol->get_n_solvent_types(); s++) phi_solvent_.emplace_back(ctx_, sizeof(double) * RM);
     phi_tmp_.alloc(ctx_, sizeof(double) * M_);
-    q_poly_.assign(mol->get_n_polymer_types(), 0.0);
+    const int P = mol->get_n_polymer_types();
+    q_poly_.assign((size_t)R_ * P, 0.0);
     q_solvent_.assign(mol->get_n_solvent_types(), 0.0);
-    dq_dl_.assign(mol->get_n_polymer_types(), {0.0, 0.0, 0.0});
-    dev_scalars_.alloc(ctx_, sizeof(double) * (64 + mol->get_n_polymer_types() + mol->get_n_solvent_types()));
+    dq_dl_.assign(P, {0.0, 0.0, 0.0});
+    dev_scalars_.alloc(ctx_, sizeof(double) * ((size_t)R_ * P + 64 + mol->get_n_solvent_types()));
     basis_.alloc(ctx_, sizeof(double) * 3 * Mc_);
+    active_.alloc(ctx_, sizeof(int) * R_);
+    {
+        std::vector<int> ones(R_, 1);
+        check_rc(lfts_memcpy_h2d(ctx_, active_.get(), ones.data(), sizeof(int) * R_));
+    }
 
     // the reference's lane count: OMP_NUM_THREADS, default 4
     int n_streams = 4;
@@ -111,6 +121,7 @@ GpuComputation::GpuComputation(ComputationBox *cb, Molecules *mol, PropagatorAna
     sched_ = new Scheduler(pa->get_computation_propagators(), n_streams);
     build_plan();
     build_dot_jobs();
+    build_phi_jobs();
     build_stress_jobs();
     arena_.alloc(ctx_, std::max<size_t>(arena_host_.size(), 64));
     check_rc(lfts_memcpy_h2d(ctx_, arena_.get(), arena_host_.data(), arena_host_.size()));
@@ -119,51 +130,62 @@ GpuComputation::GpuComputation(ComputationBox *cb, Molecules *mol, PropagatorAna
 
 GpuComputation::~GpuComputation() {
     if (graph_) lfts_graph_destroy(graph_);
+    if (stats_graph_) lfts_graph_destroy(stats_graph_);
     delete sched_;
     keys_.clear();
     types_.clear();
     q_init_.clear();
     phi_block_.clear();
+    phi_type_.clear();
     phi_solvent_.clear();
-    phi_tmp_.release(); spec_.release(); arena_.release(); dev_scalars_.release(); basis_.release(); phi_jobs_.release();
-    coefs_.release(); stress_jobs_.release(); stress_out_.release(); stress_spec_.release();
+    active_.release(); phi_tmp_.release(); spec_.release(); arena_.release(); dev_scalars_.release(); basis_.release();
+    phi_jobs_.release(); coefs_.release(); stress_jobs_.release(); stress_out_.release(); stress_spec_.release();
     if (ctx_) lfts_ctx_destroy(ctx_);
 }
 
-void *GpuComputation::slice(const std::string &key, int n) const {
+void *GpuComputation::slice(const std::string &key, int n, int r) const {
     const KeyStore &ks = keys_.at(key);
-    return (char *)ks.q.get() + esz_ * M_ * (size_t)n;
+    const size_t nslices = ks.q.size() / (esz_ * M_ * R_);
+    return (char *)ks.q.get() + esz_ * M_ * ((size_t)r * nslices + (size_t)n);
 }
-void *GpuComputation::half_slice(const std::string &key, int n) const {
+void *GpuComputation::half_slice(const std::string &key, int n, int r) const {
     const KeyStore &ks = keys_.at(key);
     auto it = ks.half.find(n);
     if (it == ks.half.end()) LFTS_THROW("missing half-bond slice " + std::to_string(n) + " of " + key);
-    return it->second.get();
+    return (char *)it->second.get() + esz_ * M_ * (size_t)r;
 }
 
+double *GpuComputation::w_device(const std::string &type) { return types_.at(type).w.as<double>(); }
+double *GpuComputation::phi_type_device(const std::string &type) { return phi_type_.at(type).as<double>(); }
+double *GpuComputation::partition_device() { return dev_scalars_.as<double>(); }
+
 // Translate the schedule into batched launches: every slot's junction starts,
-// then its steps in lock-step (one launch per step index for all jobs).
+// then its steps in lock-step (one launch per step index for all jobs of all
+// replicas).
 void GpuComputation::build_plan() {
     auto &props = pa_->get_computation_propagators();
     int max_jobs = 1;
-    auto step_job = [&](const void *in, long long is, void *out, long long os, const std::string &type, int spec_idx) {
+    const long long Ml = M_;
+    auto step_job = [&](const void *in, long long is, void *out, long long os, const std::string &type, int r) {
         const TypeStore &t = types_.at(type);
         lfts_step_job j;
         j.in = in;
         j.in_stride = is;
         j.out = out;
         j.out_stride = os;
-        j.fac = t.fac.get();
+        j.fac = (const char *)t.fac.get() + esz_ * Ml * r;
         j.bond = t.bond.get();
         j.bond_half = t.bond_half.get();
-        j.spec = (void *)(intptr_t)spec_idx;  // patched to a device address once spec_ exists
+        j.spec = nullptr;  // patched to a device address once spec_ exists
+        j.active = R_ > 1 ? active_.as<int>() : nullptr;
+        j.replica = r;
+        j.pad = 0;
         return j;
     };
     struct PendingSteps {
         int kind, nsteps, half, with_fac;
         std::vector<lfts_step_job> jobs;
     };
-    std::vector<std::vector<PendingSteps>> slot_steps;
     for (const auto &slot : sched_->get_schedule()) {
         std::vector<lfts_junction_job> jj;
         std::vector<const void *> deps;
@@ -181,88 +203,91 @@ void GpuComputation::build_plan() {
             }
             steps[g->second].jobs.push_back(j);
         };
-        // discrete jobs whose first step must follow a junction/copy go first
         std::vector<std::pair<lfts_step_job, std::pair<int, int>>> first_steps;
         std::vector<lfts_step_job> half_jobs;
         for (const auto &job : slot) {
             const std::string &key = std::get<0>(job);
-            int n_from = std::get<1>(job);
+            const int n_from0 = std::get<1>(job);
             const int n_to = std::get<2>(job);
             const ComputationEdge &e = props.at(key);
             const std::string &type = e.monomer_type;
-            void *fac = types_.at(type).fac.get();
-            if (continuous_) {
-                if (n_from == 0) {
-                    lfts_junction_job j{slice(key, 0), nullptr, 0, 0, (int)deps.size(), 0};
-                    if (e.deps.empty()) {
-                        if (key[0] == '{') {
-                            j.ndeps = 1;
-                            deps.push_back(q_init_.at(code::q_input_from_key(key)).get());
-                            wts.push_back(1.0);
-                        }
-                    } else {
-                        j.mode = key[0] == '[' ? 1 : 0;
-                        j.ndeps = (int)e.deps.size();
-                        for (const auto &d : e.deps) {
-                            deps.push_back(slice(std::get<0>(d), std::get<1>(d)));
-                            wts.push_back((double)std::get<2>(d));
-                        }
-                    }
-                    jj.push_back(j);
-                }
-                if (n_to > n_from)
-                    add_step(1, n_to - n_from, 0, 1, step_job(slice(key, n_from), M_, slice(key, n_from + 1), M_, type, 0));
-            } else {
-                if (n_from == 0) {
-                    if (e.deps.empty()) {
-                        // leaf: q(1) = exp(-w ds) [* q_init]
-                        lfts_junction_job j{slice(key, 1), fac, 0, 0, (int)deps.size(), 0};
-                        if (key[0] == '{') {
-                            j.ndeps = 1;
-                            deps.push_back(q_init_.at(code::q_input_from_key(key)).get());
-                            wts.push_back(1.0);
-                        }
-                        jj.push_back(j);
-                    } else if (key[0] == '[') {
-                        lfts_junction_job j{slice(key, 1), nullptr, (int)e.deps.size(), 1, (int)deps.size(), 0};
-                        for (const auto &d : e.deps) {
-                            const int n = std::get<1>(d);
-                            deps.push_back(n == 0 ? half_slice(std::get<0>(d), 0) : slice(std::get<0>(d), n));
-                            wts.push_back((double)std::get<2>(d));
-                        }
-                        jj.push_back(j);
-                        if (std::get<1>(e.deps[0]) == 0) {
-                            Launch cp{};
-                            cp.kind = 3;
-                            cp.dst = half_slice(key, 0);
-                            cp.src = slice(key, 1);
-                            cp.bytes = esz_ * M_;
-                            copies.push_back(cp);
-                            first_steps.push_back({step_job(slice(key, 1), 0, slice(key, 1), 0, type, 0), {1, 1}});
+            for (int r = 0; r < R_; r++) {
+                int n_from = n_from0;
+                void *fac = (char *)types_.at(type).fac.get() + esz_ * Ml * r;
+                if (continuous_) {
+                    if (n_from == 0) {
+                        lfts_junction_job j{slice(key, 0, r), nullptr, 0, 0, (int)deps.size(), 0};
+                        if (e.deps.empty()) {
+                            if (key[0] == '{') {
+                                j.ndeps = 1;
+                                deps.push_back((char *)q_init_.at(code::q_input_from_key(key)).get() + esz_ * Ml * r);
+                                wts.push_back(1.0);
+                            }
                         } else {
-                            first_steps.push_back({step_job(slice(key, 1), 0, slice(key, 1), 0, type, 0), {0, 1}});
-                        }
-                    } else {
-                        lfts_junction_job j{half_slice(key, 0), nullptr, (int)e.deps.size(), 0, (int)deps.size(), 0};
-                        for (const auto &d : e.deps) {
-                            deps.push_back(half_slice(std::get<0>(d), std::get<1>(d)));
-                            wts.push_back(1.0);
+                            j.mode = key[0] == '[' ? 1 : 0;
+                            j.ndeps = (int)e.deps.size();
+                            for (const auto &d : e.deps) {
+                                deps.push_back(slice(std::get<0>(d), std::get<1>(d), r));
+                                wts.push_back((double)std::get<2>(d));
+                            }
                         }
                         jj.push_back(j);
-                        if (n_to > 0)
-                            first_steps.push_back({step_job(half_slice(key, 0), 0, slice(key, 1), 0, type, 0), {1, 1}});
                     }
+                    if (n_to > n_from)
+                        add_step(1, n_to - n_from, 0, 1, step_job(slice(key, n_from, r), Ml, slice(key, n_from + 1, r), Ml, type, r));
+                } else {
+                    if (n_from == 0) {
+                        if (e.deps.empty()) {
+                            // leaf: q(1) = exp(-w ds) [* q_init]
+                            lfts_junction_job j{slice(key, 1, r), fac, 0, 0, (int)deps.size(), 0};
+                            if (key[0] == '{') {
+                                j.ndeps = 1;
+                                deps.push_back((char *)q_init_.at(code::q_input_from_key(key)).get() + esz_ * Ml * r);
+                                wts.push_back(1.0);
+                            }
+                            jj.push_back(j);
+                        } else if (key[0] == '[') {
+                            lfts_junction_job j{slice(key, 1, r), nullptr, (int)e.deps.size(), 1, (int)deps.size(), 0};
+                            for (const auto &d : e.deps) {
+                                const int n = std::get<1>(d);
+                                deps.push_back(n == 0 ? half_slice(std::get<0>(d), 0, r) : slice(std::get<0>(d), n, r));
+                                wts.push_back((double)std::get<2>(d));
+                            }
+                            jj.push_back(j);
+                            if (std::get<1>(e.deps[0]) == 0) {
+                                Launch cp{};
+                                cp.kind = 3;
+                                cp.dst = half_slice(key, 0, r);
+                                cp.src = slice(key, 1, r);
+                                cp.bytes = esz_ * Ml;
+                                copies.push_back(cp);
+                                first_steps.push_back({step_job(slice(key, 1, r), 0, slice(key, 1, r), 0, type, r), {1, 1}});
+                            } else {
+                                first_steps.push_back({step_job(slice(key, 1, r), 0, slice(key, 1, r), 0, type, r), {0, 1}});
+                            }
+                        } else {
+                            lfts_junction_job j{half_slice(key, 0, r), nullptr, (int)e.deps.size(), 0, (int)deps.size(), 0};
+                            for (const auto &d : e.deps) {
+                                deps.push_back(half_slice(std::get<0>(d), std::get<1>(d), r));
+                                wts.push_back(1.0);
+                            }
+                            jj.push_back(j);
+                            if (n_to > 0)
+                                first_steps.push_back({step_job(half_slice(key, 0, r), 0, slice(key, 1, r), 0, type, r), {1, 1}});
+                        }
+                    }
+                    if (n_to == 0) continue;
+                    if (n_from == 0) {
+                        if (keys_.at(key).half.count(1))
+                            half_jobs.push_back(step_job(slice(key, 1, r), 0, half_slice(key, 1, r), 0, type, r));
+                        n_from = 1;
+                    }
+                    if (n_to > n_from)
+                        add_step(2, n_to - n_from, 0, 1, step_job(slice(key, n_from, r), Ml, slice(key, n_from + 1, r), Ml, type, r));
+                    for (int n = n_from; n < n_to; n++)
+                        if (e.junction_ends.count(n + 1) && n + 1 != 1)
+                            half_jobs.push_back(step_job(slice(key, n + 1, r), 0, half_slice(key, n + 1, r), 0, type, r));
                 }
-                if (n_to == 0) continue;
-                if (n_from == 0) {
-                    if (keys_.at(key).half.count(1)) half_jobs.push_back(step_job(slice(key, 1), 0, half_slice(key, 1), 0, type, 0));
-                    n_from = 1;
-                }
-                if (n_to > n_from)
-                    add_step(2, n_to - n_from, 0, 1, step_job(slice(key, n_from), M_, slice(key, n_from + 1), M_, type, 0));
-                for (int n = n_from; n < n_to; n++)
-                    if (e.junction_ends.count(n + 1) && n + 1 != 1)
-                        half_jobs.push_back(step_job(slice(key, n + 1), 0, half_slice(key, n + 1), 0, type, 0));
             }
         }
         if (!jj.empty()) {
@@ -275,23 +300,22 @@ void GpuComputation::build_plan() {
             plan_.push_back(L);
         }
         for (auto &cp : copies) plan_.push_back(cp);
-        // first discrete steps grouped by (half, with_fac)
         std::map<std::pair<int, int>, std::vector<lfts_step_job>> fs;
         for (auto &f : first_steps) fs[f.second].push_back(f.first);
         std::vector<PendingSteps> ordered;
         for (auto &g : fs) ordered.push_back({2, 1, g.first.first, g.first.second, g.second});
-        for (auto &s : steps) ordered.push_back(s);
+        for (auto &st : steps) ordered.push_back(st);
         if (!half_jobs.empty()) ordered.push_back({2, 1, 1, 0, half_jobs});
-        for (auto &s : ordered) {
-            for (size_t i = 0; i < s.jobs.size(); i++) s.jobs[i].spec = (void *)(intptr_t)i;
-            max_jobs = std::max(max_jobs, (int)s.jobs.size());
+        for (auto &st : ordered) {
+            for (size_t i = 0; i < st.jobs.size(); i++) st.jobs[i].spec = (void *)(intptr_t)i;
+            max_jobs = std::max(max_jobs, (int)st.jobs.size());
             Launch L{};
-            L.kind = s.kind;
-            L.njobs = (int)s.jobs.size();
-            L.nsteps = s.nsteps;
-            L.half = s.half;
-            L.with_fac = s.with_fac;
-            L.jobs = arena_push(arena_host_, s.jobs);
+            L.kind = st.kind;
+            L.njobs = (int)st.jobs.size();
+            L.nsteps = st.nsteps;
+            L.half = st.half;
+            L.with_fac = st.with_fac;
+            L.jobs = arena_push(arena_host_, st.jobs);
             plan_.push_back(L);
         }
     }
@@ -307,31 +331,83 @@ void GpuComputation::build_plan() {
 
 // Single-chain partition functions: the first block of each polymer in block
 // order (CpuComputationContinuous.cpp:62-91, CpuComputationDiscrete.cpp:92-122).
+// Jobs are replica-major: Q of (replica r, polymer p) lands at r * P + p.
 void GpuComputation::build_dot_jobs() {
     std::vector<lfts_dot_job> jobs;
+    std::vector<std::pair<BlockKey, int>> chosen;
     int current_p = 0;
     for (const auto &bk : block_order_) {
         const int p = std::get<0>(bk);
         if (p != current_p) continue;
         const ComputationBlock &b = pa_->get_computation_block(bk);
-        const int n_agg = (int)b.v_u.size() / b.n_repeated;
-        const int NL = b.n_segment_left;
-        lfts_dot_job j;
-        if (continuous_) {
-            j = {slice(std::get<1>(bk), NL), slice(std::get<2>(bk), 0), nullptr, (double)n_agg};
-        } else {
-            if (NL == 0) continue;
-            j = {slice(std::get<1>(bk), NL), slice(std::get<2>(bk), 1), types_.at(b.monomer_type).fac.get(), (double)n_agg};
-        }
-        jobs.push_back(j);
-        partition_polymer_.push_back(p);
+        if (!continuous_ && b.n_segment_left == 0) continue;
+        chosen.push_back({bk, p});
         current_p++;
     }
+    const int P = mol_->get_n_polymer_types();
+    if ((int)chosen.size() != P) LFTS_THROW("could not find a block for the partition function of every polymer");
+    for (int r = 0; r < R_; r++) {
+        for (const auto &c : chosen) {
+            const BlockKey &bk = c.first;
+            const ComputationBlock &b = pa_->get_computation_block(bk);
+            const int NL = b.n_segment_left;
+            if (continuous_)
+                jobs.push_back({slice(std::get<1>(bk), NL, r), slice(std::get<2>(bk), 0, r), nullptr, 0.0});
+            else
+                jobs.push_back({slice(std::get<1>(bk), NL, r), slice(std::get<2>(bk), 1, r),
+                                (const char *)types_.at(b.monomer_type).fac.get() + esz_ * M_ * r, 0.0});
+        }
+    }
+    for (const auto &c : chosen) partition_polymer_.push_back(c.second);
     n_dot_jobs_ = (int)jobs.size();
     dot_jobs_ = arena_push(arena_host_, jobs);
 }
 
-// (block, contour point) pairs of the stress sum with their weights
+// Concentration jobs with the normalisation ds phi_p / alpha_p * n_repeated
+// divided on the device by Q_p of the same replica.
+void GpuComputation::build_phi_jobs() {
+    std::vector<lfts_phi_job> cont, disc;
+    std::vector<double> coefs;
+    const int P = mol_->get_n_polymer_types();
+    for (int r = 0; r < R_; r++) {
+        for (const auto &bk : block_order_) {
+            const ComputationBlock &b = pa_->get_computation_block(bk);
+            double *phi = phi_block_.at(bk).as<double>() + (size_t)r * M_;
+            if (b.n_segment_right == 0) {
+                if (r == 0) zero_blocks_.push_back({bk, 0});
+                continue;
+            }
+            const int p = std::get<0>(bk);
+            Polymer &pc = mol_->get_polymer(p);
+            lfts_phi_job j;
+            j.q_left = slice(std::get<1>(bk), 0, r);
+            j.q_right = slice(std::get<2>(bk), 0, r);
+            j.fac = (const char *)types_.at(b.monomer_type).fac.get() + esz_ * M_ * r;
+            j.phi = phi;
+            j.norm = mol_->get_ds() * pc.get_volume_fraction() / pc.get_alpha() * b.n_repeated;
+            j.q_div = dev_scalars_.as<double>() + (size_t)r * P + p;
+            j.n_left = b.n_segment_left;
+            j.n_right = b.n_segment_right;
+            j.coef_offset = 0;
+            j.pad = 0;
+            if (continuous_) {
+                const auto c = simpson(b.n_segment_right);
+                j.coef_offset = (int)coefs.size();
+                coefs.insert(coefs.end(), c.begin(), c.end());
+                cont.push_back(j);
+            } else {
+                disc.push_back(j);
+            }
+        }
+    }
+    n_phi_cont_ = (int)cont.size();
+    n_phi_disc_ = (int)disc.size();
+    phi_jobs_cont_ = arena_push(arena_host_, cont);
+    phi_jobs_disc_ = arena_push(arena_host_, disc);
+    coef_off_ = arena_push(arena_host_, coefs);
+}
+
+// (block, contour point) pairs of the stress sum with their weights, replica 0
 // (CpuComputationContinuous.cpp:643-726, CpuComputationDiscrete.cpp:857-996).
 void GpuComputation::build_stress_jobs() {
     std::vector<lfts_stress_job> jobs;
@@ -385,21 +461,22 @@ void GpuComputation::update_laplacian_operator() {
         check_rc(lfts_bond_tables(ctx_, kv.second * kv.second, mol_->get_ds(), lx.data(), t.bond.get(), t.bond_half.get()));
     }
     check_rc(lfts_fourier_basis(ctx_, lx.data(), basis_.as<double>()));
-    // the partition scale dv / (n_aggregated V) follows the box
+    // partition scale dv / (n_aggregated V): n_aggregated is structural, dv and V follow the box
     const auto *jobs = (const lfts_dot_job *)(arena_host_.data() + dot_jobs_);
-    const double dv = cb_->get_dv(0), V = cb_->get_volume();
     std::vector<lfts_dot_job> dj(jobs, jobs + n_dot_jobs_);
-    // scale = dv / (n_aggregated V): n_aggregated is structural, dv and V follow the box
-    int k = 0, current_p = 0;
+    const double dv = cb_->get_dv(0), V = cb_->get_volume();
+    std::vector<double> scale;
+    int current_p = 0;
     for (const auto &b : block_order_) {
         const int p = std::get<0>(b);
         if (p != current_p) continue;
         const ComputationBlock &cbk = pa_->get_computation_block(b);
         if (!continuous_ && cbk.n_segment_left == 0) continue;
         const int n_agg = (int)cbk.v_u.size() / cbk.n_repeated;
-        dj[k++].scale = dv / n_agg / V;
+        scale.push_back(dv / n_agg / V);
         current_p++;
     }
+    for (int j = 0; j < n_dot_jobs_; j++) dj[j].scale = scale[j % scale.size()];
     if (n_dot_jobs_ > 0)
         check_rc(lfts_memcpy_h2d(ctx_, (char *)arena_.get() + dot_jobs_, dj.data(), sizeof(lfts_dot_job) * n_dot_jobs_));
 }
@@ -407,8 +484,10 @@ void GpuComputation::update_laplacian_operator() {
 void GpuComputation::enqueue_propagation() {
     char *base = (char *)arena_.get();
     const double ds = mol_->get_ds();
-    for (auto &kv : types_)
-        check_rc(lfts_field_factors(ctx_, kv.second.w.as<double>(), continuous_ ? -ds / 4.0 : -ds, kv.second.fac.get()));
+    const size_t RM = (size_t)R_ * M_;
+    (void)RM;
+    for (auto &kv : types_)  // factor tables of all replicas in one pass over R*M points
+        check_rc(lfts_field_factors_batch(ctx_, kv.second.w.as<double>(), continuous_ ? -ds / 4.0 : -ds, kv.second.fac.get(), R_));
     for (const auto &L : plan_) {
         switch (L.kind) {
             case 0:
@@ -432,8 +511,55 @@ void GpuComputation::enqueue_propagation() {
         check_rc(lfts_dots(ctx_, (const lfts_dot_job *)(base + dot_jobs_), n_dot_jobs_, dev_scalars_.as<double>()));
 }
 
+void GpuComputation::enqueue_concentrations() {
+    char *base = (char *)arena_.get();
+    for (const auto &z : zero_blocks_)
+        check_rc(lfts_memset_async(ctx_, phi_block_.at(z.first).get(), 0, sizeof(double) * M_ * R_));
+    if (n_phi_cont_ > 0)
+        check_rc(lfts_phi_blocks(ctx_, 0, (const lfts_phi_job *)(base + phi_jobs_cont_), n_phi_cont_, (const double *)(base + coef_off_)));
+    if (n_phi_disc_ > 0)
+        check_rc(lfts_phi_blocks(ctx_, 1, (const lfts_phi_job *)(base + phi_jobs_disc_), n_phi_disc_, (const double *)(base + coef_off_)));
+    // per-type totals over all replicas at once (blocks are [R][M])
+    for (auto &kv : phi_type_) {
+        std::vector<const double *> srcs;
+        for (const auto &bk : block_order_) {
+            const ComputationBlock &b = pa_->get_computation_block(bk);
+            if (code::monomer_type_from_key(std::get<1>(bk)) == kv.first && b.n_segment_right != 0)
+                srcs.push_back(phi_block_.at(bk).as<double>());
+        }
+        check_rc(lfts_lincomb(ctx_, kv.second.as<double>(), (int)srcs.size(), srcs.data(), nullptr, (long long)M_ * R_));
+    }
+}
+
+void GpuComputation::enqueue_statistics() {
+    if (mol_->get_n_solvent_types() > 0) LFTS_THROW("batched statistics do not support solvents");
+    if (use_graph_) {
+        if (!stats_graph_) {
+            const long long before = lfts_ctx_launches(ctx_);
+            check_rc(lfts_graph_begin(ctx_));
+            enqueue_propagation();
+            enqueue_concentrations();
+            check_rc(lfts_graph_end(ctx_, &stats_graph_));
+            stats_graph_kernels_ = lfts_ctx_launches(ctx_) - before;
+        }
+        check_rc(lfts_graph_launch(ctx_, stats_graph_));
+        graph_kernels_replayed_ += stats_graph_kernels_;
+    } else {
+        enqueue_propagation();
+        enqueue_concentrations();
+    }
+    have_propagators_ = true;
+}
+
+std::vector<double> GpuComputation::partitions_host() {
+    std::vector<double> q((size_t)R_ * mol_->get_n_polymer_types());
+    check_rc(lfts_memcpy_d2h(ctx_, q.data(), dev_scalars_.get(), sizeof(double) * q.size()));
+    return q;
+}
+
 void GpuComputation::compute_propagators(const std::map<std::string, const double *> &w,
                                          const std::map<std::string, const double *> &q_init) {
+    if (R_ != 1) LFTS_THROW("compute_propagators works on single systems; use the batched interface");
     for (const auto &it : pa_->get_computation_propagators())
         if (!w.count(it.second.monomer_type))
             LFTS_THROW("monomer_type \"" + it.second.monomer_type + "\" is not in w_input.");
@@ -469,53 +595,15 @@ void GpuComputation::compute_propagators(const std::map<std::string, const doubl
 void GpuComputation::sync_partitions() {
     std::vector<double> q(std::max(n_dot_jobs_, 1));
     check_rc(lfts_memcpy_d2h(ctx_, q.data(), dev_scalars_.get(), sizeof(double) * n_dot_jobs_));
-    for (int j = 0; j < n_dot_jobs_; j++) q_poly_[partition_polymer_[j]] = q[j];
+    for (int j = 0; j < n_dot_jobs_; j++) q_poly_[j] = q[j];
 }
 
 void GpuComputation::compute_concentrations() {
     if (!have_propagators_) LFTS_THROW("compute_propagators must be called before compute_concentrations");
-    std::vector<lfts_phi_job> cont, disc;
-    std::vector<double> coefs;
-    for (const auto &bk : block_order_) {
-        const ComputationBlock &b = pa_->get_computation_block(bk);
-        double *phi = phi_block_.at(bk).as<double>();
-        if (b.n_segment_right == 0) {
-            check_rc(lfts_memset_async(ctx_, phi, 0, sizeof(double) * M_));
-            continue;
-        }
-        Polymer &pc = mol_->get_polymer(std::get<0>(bk));
-        const double norm = mol_->get_ds() * pc.get_volume_fraction() / pc.get_alpha() / q_poly_[std::get<0>(bk)] * b.n_repeated;
-        lfts_phi_job j;
-        j.q_left = slice(std::get<1>(bk), 0);
-        j.q_right = slice(std::get<2>(bk), 0);
-        j.fac = types_.at(b.monomer_type).fac.get();
-        j.phi = phi;
-        j.norm = norm;
-        j.n_left = b.n_segment_left;
-        j.n_right = b.n_segment_right;
-        j.coef_offset = (int)coefs.size();
-        j.pad = 0;
-        if (continuous_) {
-            const auto c = simpson(b.n_segment_right);
-            coefs.insert(coefs.end(), c.begin(), c.end());
-            cont.push_back(j);
-        } else {
-            disc.push_back(j);
-        }
-    }
-    const size_t need_jobs = sizeof(lfts_phi_job) * (cont.size() + disc.size() + 1);
-    if (phi_jobs_.size() < need_jobs) phi_jobs_.alloc(ctx_, need_jobs);
-    if (coefs_.size() < sizeof(double) * (coefs.size() + 1)) coefs_.alloc(ctx_, sizeof(double) * (coefs.size() + 1));
-    if (!coefs.empty()) check_rc(lfts_memcpy_h2d(ctx_, coefs_.get(), coefs.data(), sizeof(double) * coefs.size()));
-    std::vector<lfts_phi_job> all(cont);
-    all.insert(all.end(), disc.begin(), disc.end());
-    if (!all.empty()) check_rc(lfts_memcpy_h2d(ctx_, phi_jobs_.get(), all.data(), sizeof(lfts_phi_job) * all.size()));
-    if (!cont.empty()) check_rc(lfts_phi_blocks(ctx_, 0, phi_jobs_.as<lfts_phi_job>(), (int)cont.size(), coefs_.as<double>()));
-    if (!disc.empty())
-        check_rc(lfts_phi_blocks(ctx_, 1, phi_jobs_.as<lfts_phi_job>() + cont.size(), (int)disc.size(), coefs_.as<double>()));
+    enqueue_concentrations();
     // solvents (CpuComputationContinuous.cpp:425-436, CpuComputationDiscrete.cpp:441-452)
     const double dv_over_V = cb_->get_dv(0) / cb_->get_volume();
-    double *qs = dev_scalars_.as<double>() + std::max(n_dot_jobs_, mol_->get_n_polymer_types());
+    double *qs = dev_scalars_.as<double>() + (size_t)R_ * mol_->get_n_polymer_types();
     for (int s = 0; s < mol_->get_n_solvent_types(); s++) {
         const auto sol = mol_->get_solvent(s);
         const TypeStore &t = types_.at(std::get<1>(sol));
@@ -534,7 +622,7 @@ void GpuComputation::compute_statistics(const std::map<std::string, const double
 }
 
 double GpuComputation::get_total_partition(int p) {
-    if (p < 0 || p >= (int)q_poly_.size()) LFTS_THROW("Index (" + std::to_string(p) + ") is out of range.");
+    if (p < 0 || p >= mol_->get_n_polymer_types()) LFTS_THROW("Index (" + std::to_string(p) + ") is out of range.");
     return q_poly_[p];
 }
 
@@ -673,7 +761,7 @@ std::vector<double> GpuComputation::get_stress_gce(const std::vector<double> &fu
 // (CpuComputationContinuous.cpp:755-816, CpuComputationDiscrete.cpp:1036-1089).
 bool GpuComputation::check_total_partition() {
     std::vector<lfts_dot_job> jobs;
-    std::vector<std::pair<int, int>> owner;  // (polymer, n_propagators)
+    std::vector<int> owner;
     const double dv = cb_->get_dv(0), V = cb_->get_volume();
     for (const auto &bk : block_order_) {
         const ComputationBlock &b = pa_->get_computation_block(bk);
@@ -687,7 +775,7 @@ bool GpuComputation::check_total_partition() {
                 jobs.push_back({slice(std::get<1>(bk), NL - n + 1), slice(std::get<2>(bk), n),
                                 types_.at(b.monomer_type).fac.get(), sc});
         }
-        owner.resize(jobs.size(), {p, 0});
+        owner.resize(jobs.size(), p);
     }
     if (jobs.empty()) return true;
     DevBuf dj(ctx_, sizeof(lfts_dot_job) * jobs.size()), dout(ctx_, sizeof(double) * jobs.size());
@@ -698,8 +786,8 @@ bool GpuComputation::check_total_partition() {
     const int P = mol_->get_n_polymer_types();
     std::vector<double> mx(P, -1e20), mn(P, 1e20);
     for (size_t j = 0; j < q.size(); j++) {
-        mx[owner[j].first] = std::max(mx[owner[j].first], q[j]);
-        mn[owner[j].first] = std::min(mn[owner[j].first], q[j]);
+        mx[owner[j]] = std::max(mx[owner[j]], q[j]);
+        mn[owner[j]] = std::min(mn[owner[j]], q[j]);
     }
     std::cout << "Polymer id: maximum,  minimum, and difference of total partitions" << std::endl;
     for (int p = 0; p < P; p++) {

@@ -42,7 +42,10 @@ class DevBuf {
 
 class GpuComputation {
    public:
-    GpuComputation(ComputationBox *cb, Molecules *molecules, PropagatorAnalyzer *analyzer, int precision, int device);
+    // n_replicas independent systems of the same molecules and box advance in
+    // the same launches (replica r of every device array at offset r * size).
+    GpuComputation(ComputationBox *cb, Molecules *molecules, PropagatorAnalyzer *analyzer, int precision, int device,
+                   int n_replicas = 1);
     ~GpuComputation();
 
     int get_n_grid() const { return cb_->get_n_grid(); }
@@ -70,6 +73,25 @@ class GpuComputation {
     lfts_ctx context() const { return ctx_; }
     const Scheduler &scheduler() const { return *sched_; }
 
+    // ---- batched (device-resident) interface, all replicas at once
+    int n_replicas() const { return R_; }
+    long long n_grid() const { return M_; }
+    // fields w of a monomer type, R x M doubles on the device (filled by the caller)
+    double *w_device(const std::string &type);
+    // total concentration of a monomer type, R x M doubles on the device
+    double *phi_type_device(const std::string &type);
+    // single-chain partition functions, R x P doubles on the device
+    double *partition_device();
+    // per-replica flags: replicas with 0 are skipped by the step kernels
+    int *active_device() { return active_.as<int>(); }
+    // Enqueue field factors, propagators, partition functions, block and
+    // per-type concentrations for every active replica (graph-capturable).
+    void enqueue_statistics();
+    // Copy the partition functions of every replica to the host.
+    std::vector<double> partitions_host();
+    // kernels launched so far: direct launches + kernels replayed in graphs
+    long long kernel_launches() const { return lfts_ctx_launches(ctx_) + graph_kernels_replayed_; }
+
    private:
     struct KeyStore {
         DevBuf q;                      // slices 0..max_n_segment
@@ -90,18 +112,21 @@ class GpuComputation {
         size_t bytes;
     };
 
-    void *slice(const std::string &key, int n) const;
-    void *half_slice(const std::string &key, int n) const;
+    void *slice(const std::string &key, int n, int r = 0) const;
+    void *half_slice(const std::string &key, int n, int r = 0) const;
     void build_plan();
     void build_stress_jobs();
     void build_dot_jobs();
+    void build_phi_jobs();
     void enqueue_propagation();
+    void enqueue_concentrations();
     void sync_partitions();
 
     ComputationBox *cb_;
     Molecules *mol_;
     PropagatorAnalyzer *pa_;
     int prec_ = 8;
+    int R_ = 1;
     size_t esz_ = 8;
     bool continuous_ = true;
     lfts_ctx ctx_ = nullptr;
@@ -112,12 +137,17 @@ class GpuComputation {
     std::map<std::string, TypeStore> types_;
     std::map<std::string, DevBuf> q_init_;
     std::map<BlockKey, DevBuf> phi_block_;
+    std::map<std::string, DevBuf> phi_type_;
     std::vector<DevBuf> phi_solvent_;
-    DevBuf phi_tmp_, spec_, arena_, dev_scalars_, basis_, phi_jobs_, coefs_, stress_jobs_, stress_out_, stress_spec_;
+    DevBuf active_, phi_tmp_, spec_, arena_, dev_scalars_, basis_, phi_jobs_, coefs_, stress_jobs_, stress_out_, stress_spec_;
     std::vector<Launch> plan_;
+    size_t phi_jobs_cont_ = 0, phi_jobs_disc_ = 0, coef_off_ = 0;
+    int n_phi_cont_ = 0, n_phi_disc_ = 0;
+    std::vector<std::pair<BlockKey, int>> zero_blocks_;
     std::vector<unsigned char> arena_host_;
-    lfts_graph graph_ = nullptr;
+    lfts_graph graph_ = nullptr, stats_graph_ = nullptr;
     bool use_graph_ = true;
+    long long stats_graph_kernels_ = 0, graph_kernels_replayed_ = 0;
 
     // single-chain partition: (polymer, dot job index)
     std::vector<int> partition_polymer_;

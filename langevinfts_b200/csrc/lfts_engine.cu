@@ -20,6 +20,8 @@ static int fail(const std::string &msg) {
     g_err = msg;
     return -1;
 }
+int lfts_internal_fail(const std::string &msg) { return fail(msg); }
+void lfts_internal_count(lfts_ctx c, int n);
 #define CK(call)                                                                                        \
     do {                                                                                                \
         cudaError_t e_ = (call);                                                                        \
@@ -44,6 +46,7 @@ struct lfts_ctx_s {
     lfts_step_job *sjobs = nullptr;
     int sjobs_cap = 0;
     lfts_step_job *sjobs_host = nullptr;
+    long long launches = 0;  // kernels enqueued through this context (graph replays excluded)
 };
 
 struct lfts_graph_s {
@@ -90,21 +93,21 @@ template <typename T, bool GEN>
 __global__ void k_xstress(GridPlan g, const lfts_step_job *__restrict__ sj, const lfts_stress_job *__restrict__ jobs,
                           const double *__restrict__ basis, int TJ, double *partials);
 
-template <typename T, bool GEN> static void set_attrs_t(lfts_ctx c) {
-    cudaFuncSetAttribute(k_plane_forward<T, 1, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_pf1);
-    cudaFuncSetAttribute(k_plane_mid<T, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_mid);
-    cudaFuncSetAttribute(k_plane_inverse<T, 1, EPI_SCALE, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_inv1);
-    cudaFuncSetAttribute(k_plane_inverse<T, 1, EPI_RICH_ACC, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_inv1);
-    cudaFuncSetAttribute(k_xpass<T, 1, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_x1);
-    {
-        const size_t smx = sizeof(typename CT<T>::type) * (2 * (size_t)c->g.n0 * c->TJ + c->g.n0) + sizeof(short) * c->g.n0;
-        cudaFuncSetAttribute(k_xstress<T, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
-    }
-    if (c->nbr2) {
-        cudaFuncSetAttribute(k_plane_forward<T, 2, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_pf2);
-        cudaFuncSetAttribute(k_plane_inverse<T, 2, EPI_RICH, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_inv2);
-        cudaFuncSetAttribute(k_xpass<T, 2, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->sm_x2);
-    }
+// The dynamic shared-memory limit is a per-kernel, process-wide attribute:
+// contexts with different grids share the kernels, so every kernel gets the
+// device's opt-in maximum once instead of a per-grid value (a smaller grid's
+// context would otherwise lower the limit another context relies on).
+template <typename T, bool GEN> static void set_attrs_t(int max_smem) {
+    const int a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaFuncSetAttribute(k_plane_forward<T, 1, GEN>, (cudaFuncAttribute)a, max_smem);
+    cudaFuncSetAttribute(k_plane_forward<T, 2, GEN>, (cudaFuncAttribute)a, max_smem);
+    cudaFuncSetAttribute(k_plane_mid<T, GEN>, (cudaFuncAttribute)a, max_smem);
+    cudaFuncSetAttribute(k_plane_inverse<T, 1, EPI_SCALE, GEN>, (cudaFuncAttribute)a, max_smem);
+    cudaFuncSetAttribute(k_plane_inverse<T, 1, EPI_RICH_ACC, GEN>, (cudaFuncAttribute)a, max_smem);
+    cudaFuncSetAttribute(k_plane_inverse<T, 2, EPI_RICH, GEN>, (cudaFuncAttribute)a, max_smem);
+    cudaFuncSetAttribute(k_xpass<T, 1, GEN>, (cudaFuncAttribute)a, max_smem);
+    cudaFuncSetAttribute(k_xpass<T, 2, GEN>, (cudaFuncAttribute)a, max_smem);
+    cudaFuncSetAttribute(k_xstress<T, GEN>, (cudaFuncAttribute)a, max_smem);
 }
 
 template <typename T> static int setup_plan(lfts_ctx c) {
@@ -153,7 +156,7 @@ template <typename T> static int setup_plan(lfts_ctx c) {
         return fail("grid plane " + std::to_string(g.n1) + "x" + std::to_string(g.n2) +
                     " does not fit in shared memory (" + std::to_string(c->sm_mid) + " > " + std::to_string(max_smem) + " bytes)");
     c->nbr2 = (int)c->sm_pf2 <= max_smem && (int)c->sm_x2 <= max_smem;
-    if (c->gen) set_attrs_t<T, true>(c); else set_attrs_t<T, false>(c);
+    if (c->gen) set_attrs_t<T, true>(max_smem); else set_attrs_t<T, false>(max_smem);
     CK(cudaGetLastError());
     return 0;
 }
@@ -374,6 +377,7 @@ extern "C" int lfts_field_factors(lfts_ctx c, const double *w, double coef, void
         k_field_factors<double><<<grid_for(c->g.M), NTHR, 0, c->stream>>>(w, coef, (double *)fac_out, c->g.M);
     else
         k_field_factors<float><<<grid_for(c->g.M), NTHR, 0, c->stream>>>(w, coef, (float *)fac_out, c->g.M);
+    c->launches += 1;
     CKLAUNCH();
     return 0;
 }
@@ -408,6 +412,7 @@ extern "C" int lfts_step_continuous(lfts_ctx c, const lfts_step_job *jobs, int n
     if (!c || !jobs) return fail("null argument");
     if (nj <= 0) return 0;
     if (nj > 65535) return fail("too many jobs in one launch (max 65535)");
+    c->launches += c->nbr2 ? 5 : 8;
     if (c->prec == 8) return c->gen ? step_cont_t<double, true>(c, jobs, nj, s) : step_cont_t<double, false>(c, jobs, nj, s);
     return c->gen ? step_cont_t<float, true>(c, jobs, nj, s) : step_cont_t<float, false>(c, jobs, nj, s);
 }
@@ -428,6 +433,7 @@ extern "C" int lfts_step_discrete(lfts_ctx c, const lfts_step_job *jobs, int nj,
     if (nj <= 0) return 0;
     if (nj > 65535) return fail("too many jobs in one launch (max 65535)");
     half = half ? 1 : 0;
+    c->launches += 3;
     if (c->prec == 8)
         return c->gen ? step_disc_t<double, true>(c, jobs, nj, s, half, with_fac) : step_disc_t<double, false>(c, jobs, nj, s, half, with_fac);
     return c->gen ? step_disc_t<float, true>(c, jobs, nj, s, half, with_fac) : step_disc_t<float, false>(c, jobs, nj, s, half, with_fac);
@@ -464,6 +470,7 @@ extern "C" int lfts_junctions(lfts_ctx c, const lfts_junction_job *jobs, int nj,
     const dim3 grid((unsigned)b, nj);
     if (c->prec == 8) k_junctions<double><<<grid, NTHR, 0, c->stream>>>(jobs, dep_ptrs, dep_weights, c->g.M);
     else k_junctions<float><<<grid, NTHR, 0, c->stream>>>(jobs, dep_ptrs, dep_weights, c->g.M);
+    c->launches += 1;
     CKLAUNCH();
     return 0;
 }
@@ -522,6 +529,7 @@ extern "C" int lfts_dots(lfts_ctx c, const lfts_dot_job *jobs, int nj, double *o
         else k_dots<float><<<grid, NTHR, 0, c->stream>>>(jobs + j0, c->g.M, c->partials);
         k_finish<<<dim3(n, 1), NTHR, 0, c->stream>>>(c->partials, DOT_CHUNKS, (const double *)&jobs[j0].scale,
                                                     (int)sizeof(lfts_dot_job), 1.0, out + j0, 1, 1);
+        c->launches += 2;
     }
     CKLAUNCH();
     return 0;
@@ -533,6 +541,7 @@ __global__ void __launch_bounds__(NTHR) k_phi(const lfts_phi_job *__restrict__ j
                                               long long M) {
     const lfts_phi_job jb = jobs[blockIdx.y];
     const T *ql = (const T *)jb.q_left, *qr = (const T *)jb.q_right;
+    const double norm = jb.q_div ? jb.norm / *jb.q_div : jb.norm;
     for (long long i = blockIdx.x * (long long)NTHR + threadIdx.x; i < M; i += (long long)gridDim.x * NTHR) {
         double acc = 0.0;
         if (MODEL == 0) {
@@ -543,7 +552,7 @@ __global__ void __launch_bounds__(NTHR) k_phi(const lfts_phi_job *__restrict__ j
                 acc += (double)ql[(long long)(jb.n_left - n + 1) * M + i] * (double)qr[(long long)n * M + i];
             acc /= (double)((const T *)jb.fac)[i];
         }
-        jb.phi[i] = acc * jb.norm;
+        jb.phi[i] = acc * norm;
     }
 }
 extern "C" int lfts_phi_blocks(lfts_ctx c, int model, const lfts_phi_job *jobs, int nj, const double *coefs) {
@@ -559,6 +568,7 @@ extern "C" int lfts_phi_blocks(lfts_ctx c, int model, const lfts_phi_job *jobs, 
         if (model == 0) k_phi<float, 0><<<grid, NTHR, 0, c->stream>>>(jobs, coefs, c->g.M);
         else k_phi<float, 1><<<grid, NTHR, 0, c->stream>>>(jobs, coefs, c->g.M);
     }
+    c->launches += 1;
     CKLAUNCH();
     return 0;
 }
@@ -619,8 +629,8 @@ __global__ void k_stress_prep(const lfts_stress_job *__restrict__ jobs, int nj, 
     using C = typename CT<T>::type;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nj; j += gridDim.x * blockDim.x) {
         C *sp = (C *)spec + (size_t)2 * j * Mc;
-        lfts_step_job a = {jobs[j].q1, 0, nullptr, 0, nullptr, nullptr, nullptr, sp};
-        lfts_step_job b = {jobs[j].q2, 0, nullptr, 0, nullptr, nullptr, nullptr, sp + Mc};
+        lfts_step_job a = {jobs[j].q1, 0, nullptr, 0, nullptr, nullptr, nullptr, sp, nullptr, 0, 0};
+        lfts_step_job b = {jobs[j].q2, 0, nullptr, 0, nullptr, nullptr, nullptr, sp + Mc, nullptr, 0, 0};
         sj[2 * j] = a;
         sj[2 * j + 1] = b;
     }
@@ -737,6 +747,7 @@ extern "C" int lfts_lincomb(lfts_ctx c, double *out, int nsrc, const double *con
         a.accumulate = k0 > 0;
         for (int k = 0; k < a.n; k++) { a.src[k] = srcs[k0 + k]; a.coef[k] = coefs ? coefs[k0 + k] : 1.0; }
         k_lincomb<<<grid_for(n), NTHR, 0, c->stream>>>(out, a, n);
+        c->launches += 1;
         k0 += a.n;
     } while (k0 < nsrc);
     CKLAUNCH();
@@ -775,6 +786,23 @@ extern "C" int lfts_solvent(lfts_ctx c, const void *fac, int power, double vf, d
     k_finish<<<dim3(1, 1), NTHR, 0, c->stream>>>(c->partials, DOT_CHUNKS, nullptr, 0, dv_over_V, Q_out, 1, 1);
     if (c->prec == 8) k_solvent_phi<double><<<grid_for(M), NTHR, 0, c->stream>>>((const double *)fac, power, vf, Q_out, phi_out, M);
     else k_solvent_phi<float><<<grid_for(M), NTHR, 0, c->stream>>>((const float *)fac, power, vf, Q_out, phi_out, M);
+    CKLAUNCH();
+    return 0;
+}
+
+void lfts_internal_count(lfts_ctx c, int n) {
+    if (c) c->launches += n;
+}
+extern "C" long long lfts_ctx_launches(lfts_ctx c) { return c ? c->launches : 0; }
+
+extern "C" int lfts_field_factors_batch(lfts_ctx c, const double *w, double coef, void *fac_out, int count) {
+    if (!c || !w || !fac_out) return fail("null argument");
+    const long long n = c->g.M * (long long)count;
+    if (c->prec == 8)
+        k_field_factors<double><<<grid_for(n), NTHR, 0, c->stream>>>(w, coef, (double *)fac_out, n);
+    else
+        k_field_factors<float><<<grid_for(n), NTHR, 0, c->stream>>>(w, coef, (float *)fac_out, n);
+    c->launches += 1;
     CKLAUNCH();
     return 0;
 }

@@ -1,0 +1,351 @@
+// Batched Langevin field-theoretic simulation kernels (FP64), all replicas of
+// a batch per launch.  Field layout: w_aux[r][S][M] (auxiliary fields),
+// per-monomer arrays [r][M].  Restates the driver arithmetic of the reference's
+// examples/fts/lfts.py (func derivatives :238-262, Leimkuhler-Matthews update
+// :697-706, saddle error :833-834, zero-mean pressure :866, Hamiltonian
+// :219-235) and the Anderson mixing of src/platforms/cpu/CpuAndersonMixing.cpp.
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/lfts_b200.h"
+
+namespace {
+
+constexpr int NT = 256;
+constexpr int NW = NT / 32;
+
+}  // namespace
+// error channel shared with the engine (lfts_last_error)
+int lfts_internal_fail(const std::string &msg);
+void lfts_internal_count(lfts_ctx c, int n);
+namespace {
+int lfail(const std::string &m) { return lfts_internal_fail(m); }
+#define LCK(call)                                                                                     \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) return lfail(std::string(#call) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+
+__device__ __forceinline__ double bsum(double v, double *sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    v = 0;
+    if (w == 0) {
+        v = lane < NW ? sh[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+struct DerivArgs {
+    int S, nf;
+    int idx[LFTS_MAX_MONOMERS];
+    double scale[LFTS_MAX_MONOMERS];
+    double A[LFTS_MAX_MONOMERS * LFTS_MAX_MONOMERS];
+    double h1[LFTS_MAX_MONOMERS], h2[LFTS_MAX_MONOMERS];
+    const double *phi[LFTS_MAX_MONOMERS];
+};
+
+// g_i = 2 h2_i w_i + h1_i + sum_j A[j][i] phi_j  (i < S-1);  sum_j phi_j - 1 (i = S-1)
+__device__ __forceinline__ double deriv(const DerivArgs &a, int i, const double *w_r, long long M, long long m,
+                                        long long off) {
+    double g;
+    if (i != a.S - 1) {
+        g = 2.0 * a.h2[i] * w_r[(long long)i * M + m] + a.h1[i];
+        for (int j = 0; j < a.S; j++) g += a.A[j * a.S + i] * a.phi[j][off];
+    } else {
+        g = -1.0;
+        for (int j = 0; j < a.S; j++) g += a.phi[j][off];
+    }
+    return g;
+}
+
+__global__ void k_deriv(DerivArgs a, const double *__restrict__ w_aux, long long M, int R, double *__restrict__ out,
+                        const int *__restrict__ active) {
+    const int r = blockIdx.y;
+    if (active && !active[r]) return;
+    const double *w_r = w_aux + (long long)r * a.S * M;
+    for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < M; m += (long long)gridDim.x * NT) {
+        const long long off = (long long)r * M + m;
+        for (int c = 0; c < a.nf; c++) out[((long long)r * a.nf + c) * M + m] = a.scale[c] * deriv(a, a.idx[c], w_r, M, m, off);
+    }
+}
+
+// Leimkuhler-Matthews: w_i += -g_i dt s_i + (xi_prev + xi_cur)/2 sqrt(s_i) for the real fields
+struct LangevinArgs {
+    DerivArgs d;
+    double dt;
+    double s[LFTS_MAX_MONOMERS];
+    double sqrt_s[LFTS_MAX_MONOMERS];
+};
+__global__ void k_langevin(LangevinArgs a, double *__restrict__ w_aux, long long M, const double *__restrict__ xi_prev,
+                           const double *__restrict__ xi_cur, const int *__restrict__ active) {
+    const int r = blockIdx.y;
+    if (active && !active[r]) return;
+    double *w_r = w_aux + (long long)r * a.d.S * M;
+    for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < M; m += (long long)gridDim.x * NT) {
+        const long long off = (long long)r * M + m;
+        double g[LFTS_MAX_MONOMERS];
+        for (int c = 0; c < a.d.nf; c++) g[c] = deriv(a.d, a.d.idx[c], w_r, M, m, off);
+        for (int c = 0; c < a.d.nf; c++) {
+            const long long n = ((long long)r * a.d.nf + c) * M + m;
+            w_r[(long long)a.d.idx[c] * M + m] += -g[c] * a.dt * a.s[c] + 0.5 * (xi_prev[n] + xi_cur[n]) * a.sqrt_s[c];
+        }
+    }
+}
+
+struct MonoArgs {
+    int S;
+    double A[LFTS_MAX_MONOMERS * LFTS_MAX_MONOMERS];
+    double *w[LFTS_MAX_MONOMERS];
+};
+__global__ void k_monomer_fields(MonoArgs a, const double *__restrict__ w_aux, long long M, int R) {
+    const long long n = (long long)R * M;
+    for (long long t = blockIdx.x * (long long)NT + threadIdx.x; t < n; t += (long long)gridDim.x * NT) {
+        const long long r = t / M, m = t - r * M;
+        const double *w_r = w_aux + r * a.S * M;
+        for (int i = 0; i < a.S; i++) {
+            double v = 0.0;
+            for (int j = 0; j < a.S; j++) v += a.A[i * a.S + j] * w_r[(long long)j * M + m];
+            a.w[i][t] = v;
+        }
+    }
+}
+
+// per (row) sums of x and x^2 -> partials; rows of length M
+__global__ void k_row_sums(const double *__restrict__ x, long long M, long long row_stride, int rows_per_rep,
+                           long long rep_stride, const double *__restrict__ center, double *partials) {
+    __shared__ double sh[NW];
+    const int row = blockIdx.y;
+    const int r = row / rows_per_rep, c = row % rows_per_rep;
+    const double *p = x + (long long)r * rep_stride + (long long)c * row_stride;
+    const double mu = center ? center[row] : 0.0;
+    double s1 = 0.0, s2 = 0.0;
+    for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < M; m += (long long)gridDim.x * NT) {
+        const double v = p[m] - mu;
+        s1 += v;
+        s2 += v * v;
+    }
+    s1 = bsum(s1, sh);
+    s2 = bsum(s2, sh);
+    if (threadIdx.x == 0) {
+        partials[((long long)row * gridDim.x + blockIdx.x) * 2] = s1;
+        partials[((long long)row * gridDim.x + blockIdx.x) * 2 + 1] = s2;
+    }
+}
+__global__ void k_row_finish(const double *__restrict__ partials, int nparts, long long M, double *mean, double *msq) {
+    __shared__ double sh[NW];
+    const int row = blockIdx.x;
+    double s1 = 0.0, s2 = 0.0;
+    for (int p = threadIdx.x; p < nparts; p += NT) {
+        s1 += partials[((long long)row * nparts + p) * 2];
+        s2 += partials[((long long)row * nparts + p) * 2 + 1];
+    }
+    s1 = bsum(s1, sh);
+    s2 = bsum(s2, sh);
+    if (threadIdx.x == 0) {
+        mean[row] = s1 / (double)M;
+        msq[row] = s2 / (double)M;
+    }
+}
+
+__global__ void k_subtract_mean(double *__restrict__ w_aux, int S, int field, long long M, const double *__restrict__ mean,
+                                const int *__restrict__ active) {
+    const int r = blockIdx.y;
+    if (active && !active[r]) return;
+    double *p = w_aux + ((long long)r * S + field) * M;
+    const double mu = mean[r];
+    for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < M; m += (long long)gridDim.x * NT) p[m] -= mu;
+}
+
+// ---- batched Anderson mixing: per replica ring of L slots, vectors of n doubles
+__device__ __forceinline__ long long ring(int i, int head, int L) { return (long long)(((head - i) % L + L) % L); }
+
+__global__ void k_am_insert(int R, long long n, int L, const int *__restrict__ head, const int *__restrict__ flag,
+                            const double *__restrict__ w_cur, long long w_stride, const double *__restrict__ d_cur,
+                            long long d_stride, double *__restrict__ w_hist, double *__restrict__ d_hist) {
+    const int r = blockIdx.y;
+    if (!flag[r]) return;
+    const long long slot = ((long long)r * L + head[r]) * n;
+    for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < n; m += (long long)gridDim.x * NT) {
+        w_hist[slot + m] = w_cur[(long long)r * w_stride + m];
+        d_hist[slot + m] = d_cur[(long long)r * d_stride + m];
+    }
+}
+
+__global__ void k_am_batch_dots(int R, long long n, int L, const int *__restrict__ head, const int *__restrict__ ndots,
+                                const double *__restrict__ d_hist, double *partials) {
+    __shared__ double sh[NW];
+    const int r = blockIdx.y, i = blockIdx.z;
+    if (i >= ndots[r]) return;
+    const double *d0 = d_hist + ((long long)r * L + ring(0, head[r], L)) * n;
+    const double *di = d_hist + ((long long)r * L + ring(i, head[r], L)) * n;
+    double acc = 0.0;
+    for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < n; m += (long long)gridDim.x * NT) acc += d0[m] * di[m];
+    acc = bsum(acc, sh);
+    if (threadIdx.x == 0) partials[(((long long)r * L + i) * gridDim.x) + blockIdx.x] = acc;
+}
+__global__ void k_am_batch_dots_finish(int L, int nparts, const int *__restrict__ ndots, const double *__restrict__ partials,
+                                       double *dots) {
+    __shared__ double sh[NW];
+    const int r = blockIdx.y, i = blockIdx.x;
+    if (i >= ndots[r]) return;
+    double acc = 0.0;
+    for (int p = threadIdx.x; p < nparts; p += NT) acc += partials[(((long long)r * L + i) * nparts) + p];
+    acc = bsum(acc, sh);
+    if (threadIdx.x == 0) dots[(long long)r * L + i] = acc;
+}
+
+// mode 0: skip; 1: simple mixing w = w_cur + mix d_cur; 2: Anderson update from the ring
+__global__ void k_am_batch_update(int R, long long n, int L, const int *__restrict__ head, const int *__restrict__ mode,
+                                  const int *__restrict__ nh, const double *__restrict__ mix, const double *__restrict__ a,
+                                  const double *__restrict__ w_cur, long long w_stride, const double *__restrict__ d_cur,
+                                  long long d_stride, const double *__restrict__ w_hist, const double *__restrict__ d_hist,
+                                  double *__restrict__ w_out, long long out_stride) {
+    const int r = blockIdx.y;
+    const int md = mode[r];
+    if (md == 0) return;
+    double *o = w_out + (long long)r * out_stride;
+    if (md == 1) {
+        const double mx = mix[r];
+        const double *w = w_cur + (long long)r * w_stride, *d = d_cur + (long long)r * d_stride;
+        for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < n; m += (long long)gridDim.x * NT) o[m] = w[m] + mx * d[m];
+        return;
+    }
+    const int hd = head[r], k = nh[r];
+    const double *w1 = w_hist + ((long long)r * L + ring(0, hd, L)) * n;
+    const double *d1 = d_hist + ((long long)r * L + ring(0, hd, L)) * n;
+    for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < n; m += (long long)gridDim.x * NT) {
+        const double b = w1[m] + d1[m];
+        double acc = b;
+        for (int h = 0; h < k; h++) {
+            const long long s = ((long long)r * L + ring(h + 1, hd, L)) * n;
+            acc += a[(long long)r * L + h] * (w_hist[s + m] + d_hist[s + m] - w1[m] - d1[m]);
+        }
+        o[m] = acc;
+    }
+}
+
+int grid1(long long n, int cap) {
+    long long b = (n + NT - 1) / NT;
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+bool fill_deriv(DerivArgs &d, int S, int nf, const int *idx, const double *scale, const double *A, const double *h1,
+                const double *h2, const double *const *phi) {
+    if (S < 1 || S > LFTS_MAX_MONOMERS || nf < 0 || nf > S) return false;
+    d.S = S;
+    d.nf = nf;
+    for (int c = 0; c < nf; c++) {
+        d.idx[c] = idx[c];
+        d.scale[c] = scale ? scale[c] : 1.0;
+        if (idx[c] < 0 || idx[c] >= S) return false;
+    }
+    for (int i = 0; i < S * S; i++) d.A[i] = A[i];
+    for (int i = 0; i < S; i++) {
+        d.h1[i] = (h1 && i < S - 1) ? h1[i] : 0.0;
+        d.h2[i] = (h2 && i < S - 1) ? h2[i] : 0.0;
+        d.phi[i] = phi[i];
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" int lfts_lfts_monomer_fields(lfts_ctx ctx, int R, int S, long long M, const double *A, const double *w_aux,
+                                        double *const *w_mono) {
+    if (S < 1 || S > LFTS_MAX_MONOMERS) return lfail("monomer count out of range");
+    MonoArgs a;
+    a.S = S;
+    for (int i = 0; i < S * S; i++) a.A[i] = A[i];
+    for (int i = 0; i < S; i++) a.w[i] = w_mono[i];
+    k_monomer_fields<<<grid1((long long)R * M, 148 * 16), NT, 0, (cudaStream_t)lfts_ctx_stream(ctx)>>>(a, w_aux, M, R);
+    lfts_internal_count(ctx, 1);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_lfts_field_deriv(lfts_ctx ctx, int R, int S, long long M, int nf, const int *idx, const double *scale,
+                                     const double *A, const double *h1, const double *h2, const double *w_aux,
+                                     const double *const *phi, double *out, const int *active) {
+    DerivArgs d;
+    if (!fill_deriv(d, S, nf, idx, scale, A, h1, h2, phi)) return lfail("invalid field-derivative arguments");
+    k_deriv<<<dim3(grid1(M, 1024), R), NT, 0, (cudaStream_t)lfts_ctx_stream(ctx)>>>(d, w_aux, M, R, out, active);
+    lfts_internal_count(ctx, 1);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_lfts_langevin(lfts_ctx ctx, int R, int S, long long M, int nreal, const int *idx, const double *A,
+                                  const double *h1, const double *h2, const double *const *phi, double dt,
+                                  const double *dt_scaling, double *w_aux, const double *xi_prev, const double *xi_cur,
+                                  const int *active) {
+    LangevinArgs a;
+    if (!fill_deriv(a.d, S, nreal, idx, nullptr, A, h1, h2, phi)) return lfail("invalid Langevin arguments");
+    a.dt = dt;
+    for (int c = 0; c < nreal; c++) {
+        a.s[c] = dt_scaling[c];
+        a.sqrt_s[c] = sqrt(dt_scaling[c]);
+    }
+    k_langevin<<<dim3(grid1(M, 1024), R), NT, 0, (cudaStream_t)lfts_ctx_stream(ctx)>>>(a, w_aux, M, xi_prev, xi_cur, active);
+    lfts_internal_count(ctx, 1);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_lfts_row_moments(lfts_ctx ctx, const double *x, int R, int rows_per_rep, long long M, long long row_stride,
+                                     long long rep_stride, const double *center, double *partials, double *mean, double *msq) {
+    const int rows = R * rows_per_rep;
+    const int chunks = 64;
+    cudaStream_t st = (cudaStream_t)lfts_ctx_stream(ctx);
+    k_row_sums<<<dim3(chunks, rows), NT, 0, st>>>(x, M, row_stride, rows_per_rep, rep_stride, center, partials);
+    k_row_finish<<<rows, NT, 0, st>>>(partials, chunks, M, mean, msq);
+    lfts_internal_count(ctx, 2);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_lfts_subtract_mean(lfts_ctx ctx, double *w_aux, int R, int S, int field, long long M, const double *mean,
+                                       const int *active) {
+    k_subtract_mean<<<dim3(grid1(M, 1024), R), NT, 0, (cudaStream_t)lfts_ctx_stream(ctx)>>>(w_aux, S, field, M, mean, active);
+    lfts_internal_count(ctx, 1);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_am_batch_insert(lfts_ctx ctx, int R, long long n, int L, const int *head, const int *flag,
+                                    const double *w_cur, long long w_stride, const double *d_cur, long long d_stride,
+                                    double *w_hist, double *d_hist) {
+    k_am_insert<<<dim3(grid1(n, 1024), R), NT, 0, (cudaStream_t)lfts_ctx_stream(ctx)>>>(R, n, L, head, flag, w_cur, w_stride,
+                                                                                       d_cur, d_stride, w_hist, d_hist);
+    lfts_internal_count(ctx, 1);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_am_batch_dots(lfts_ctx ctx, int R, long long n, int L, const int *head, const int *ndots,
+                                  const double *d_hist, double *partials, double *dots) {
+    const int chunks = 64;
+    cudaStream_t st = (cudaStream_t)lfts_ctx_stream(ctx);
+    k_am_batch_dots<<<dim3(chunks, R, L), NT, 0, st>>>(R, n, L, head, ndots, d_hist, partials);
+    k_am_batch_dots_finish<<<dim3(L, R), NT, 0, st>>>(L, chunks, ndots, partials, dots);
+    lfts_internal_count(ctx, 2);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_am_batch_update(lfts_ctx ctx, int R, long long n, int L, const int *head, const int *mode,
+                                    const int *nh, const double *mix, const double *a, const double *w_cur, long long w_stride,
+                                    const double *d_cur, long long d_stride, const double *w_hist, const double *d_hist,
+                                    double *w_out, long long out_stride) {
+    k_am_batch_update<<<dim3(grid1(n, 1024), R), NT, 0, (cudaStream_t)lfts_ctx_stream(ctx)>>>(
+        R, n, L, head, mode, nh, mix, a, w_cur, w_stride, d_cur, d_stride, w_hist, d_hist, w_out, out_stride);
+    lfts_internal_count(ctx, 1);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}

@@ -1,0 +1,76 @@
+// Batched Langevin field-theoretic simulation: many independent replicas of
+// one system advance together; the propagators of every replica run in the
+// same launches and each replica's saddle-point search stops on its own
+// (examples/fts/lfts.py:631-868 of the reference, per replica).
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "lfts_computation.h"
+
+namespace lfts {
+
+struct LangevinConfig {
+    std::vector<std::string> monomer_types;  // sorted; order of the auxiliary/monomer field rows
+    std::vector<double> A;                   // S*S, w = A w_aux
+    std::vector<double> h_coef_mu1, h_coef_mu2;  // S-1
+    double h_const = 0.0;
+    std::vector<int> real_idx, imag_idx;     // imaginary fields must be the trailing block
+    std::vector<double> dt_scaling;          // S
+    double dt = 0.0;
+    double tolerance = 1e-4;
+    int max_iter = 100;
+    int am_max_hist = 20;
+    double am_start_error = 0.5, am_mix_min = 0.01, am_mix_init = 0.01;
+};
+
+struct SaddleStats {
+    std::vector<int> iterations;      // per replica
+    std::vector<double> error;        // per replica
+    std::vector<double> hamiltonian;  // per replica
+    std::vector<int> failed;          // per replica: tolerance not met (fields restored)
+    std::vector<double> partitions;   // R x P
+};
+
+class BatchedLangevin {
+   public:
+    BatchedLangevin(ComputationBox *cb, Molecules *mol, PropagatorAnalyzer *pa, int precision, int device, int n_replicas,
+                    const LangevinConfig &cfg);
+    ~BatchedLangevin();
+    int n_replicas() const { return R_; }
+    int n_grid() const { return (int)M_; }
+    int n_real() const { return (int)cfg_.real_idx.size(); }
+    void set_fields(const double *w_aux);  // host [R][S][M]
+    void get_fields(double *w_aux) const;
+    void get_concentrations(double *phi) const;  // host [R][S][M], monomer_types order
+    SaddleStats find_saddle_point(bool restore_on_failure = false);
+    // One Langevin step of every replica; noise host [R][n_real][M] (the draw of this step)
+    SaddleStats step(const double *noise);
+    // Same, with this step's noise already on the device ([R][n_real][M] doubles)
+    SaddleStats step_device(const double *noise_dev);
+    void *stream() const { return lfts_ctx_stream(ctx_); }
+    GpuComputation &computation() { return *comp_; }
+
+   private:
+    void am_reset();
+    double hamiltonian(int r, const std::vector<double> &mean, const std::vector<double> &msq, const std::vector<double> &Q) const;
+
+    LangevinConfig cfg_;
+    int R_, S_, I_, Rr_;
+    long long M_;
+    std::unique_ptr<GpuComputation> comp_;
+    lfts_ctx ctx_;
+    Molecules *mol_;
+    DevBuf w_aux_, w_save_, phi_save_, d_cur_, xi_[2], partials_, stats_, ctl_, am_w_, am_d_, am_dots_, am_a_;
+    int xi_cur_ = 0;
+    std::vector<double *> phi_ptrs_, w_mono_ptrs_;
+    // per replica Anderson-mixing control (CpuAndersonMixing.cpp:76-161)
+    int L_;
+    std::vector<int> n_anderson_, head_;
+    std::vector<double> mix_;
+    std::vector<std::vector<std::vector<double>>> dot_rows_;
+};
+
+}  // namespace lfts

@@ -1,0 +1,287 @@
+// Batched Langevin FTS driver loop (host side of lfts_langevin.cu).
+// Per replica it follows the reference driver examples/fts/lfts.py:
+//   Leimkuhler-Matthews step of the real fields         :697-706
+//   saddle point of the imaginary fields by AM          :807-868
+//   error = max over imaginary fields of std(dH/dw)     :833-834
+//   restore the fields when the tolerance is missed     :713-730
+// and the Anderson mixing control of CpuAndersonMixing.cpp:76-161.
+#include "lfts_langevin.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace lfts {
+
+namespace {
+// Gaussian elimination without pivoting (src/common/AndersonMixing.cpp:19-47)
+void solve_no_pivot(std::vector<std::vector<double>> &u, std::vector<double> &v, std::vector<double> &a, int n) {
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++) {
+            const double f = u[j][i] / u[i][i];
+            v[j] = v[j] - v[i] * f;
+            for (int k = i + 1; k < n; k++) u[j][k] = u[j][k] - u[i][k] * f;
+        }
+    a[n - 1] = v[n - 1] / u[n - 1][n - 1];
+    for (int i = n - 2; i >= 0; i--) {
+        double s = 0.0;
+        for (int j = i + 1; j < n; j++) s = s + u[i][j] * a[j];
+        a[i] = (v[i] - s) / u[i][i];
+    }
+}
+}  // namespace
+
+BatchedLangevin::BatchedLangevin(ComputationBox *cb, Molecules *mol, PropagatorAnalyzer *pa, int precision, int device,
+                                 int n_replicas, const LangevinConfig &cfg)
+    : cfg_(cfg), R_(n_replicas), mol_(mol) {
+    S_ = (int)cfg.monomer_types.size();
+    I_ = (int)cfg.imag_idx.size();
+    Rr_ = (int)cfg.real_idx.size();
+    if (S_ < 1 || S_ > LFTS_MAX_MONOMERS) LFTS_THROW("number of monomer types must be 1.." + std::to_string(LFTS_MAX_MONOMERS));
+    if ((int)cfg.A.size() != S_ * S_) LFTS_THROW("matrix A must be S x S");
+    if (I_ < 1 || Rr_ + I_ != S_) LFTS_THROW("real and imaginary field indices must partition the S fields");
+    for (int c = 0; c < I_; c++)
+        if (cfg.imag_idx[c] != S_ - I_ + c) LFTS_THROW("the imaginary fields must be the trailing auxiliary fields");
+    if ((int)cfg.dt_scaling.size() != S_) LFTS_THROW("dt_scaling must have S entries");
+    for (const auto &t : cfg.monomer_types)
+        if (!mol->get_bond_lengths().count(t)) LFTS_THROW("monomer type " + t + " is not in the molecules");
+    if (mol->get_bond_lengths().size() != (size_t)S_) LFTS_THROW("every monomer type of the molecules needs a field");
+    comp_.reset(new GpuComputation(cb, mol, pa, precision, device, n_replicas));
+    ctx_ = comp_->context();
+    M_ = comp_->n_grid();
+    const size_t RSM = (size_t)R_ * S_ * M_;
+    w_aux_.alloc(ctx_, sizeof(double) * RSM);
+    w_save_.alloc(ctx_, sizeof(double) * RSM);
+    phi_save_.alloc(ctx_, sizeof(double) * RSM);
+    d_cur_.alloc(ctx_, sizeof(double) * (size_t)R_ * I_ * M_);
+    for (auto &x : xi_) {
+        x.alloc(ctx_, sizeof(double) * (size_t)R_ * std::max(Rr_, 1) * M_);
+        check_rc(lfts_memset_async(ctx_, x.get(), 0, x.size()));
+    }
+    L_ = cfg.am_max_hist + 1;
+    partials_.alloc(ctx_, sizeof(double) * std::max<size_t>((size_t)128 * R_ * S_, (size_t)64 * R_ * L_));
+    stats_.alloc(ctx_, sizeof(double) * 4 * (size_t)R_ * S_);
+    ctl_.alloc(ctx_, sizeof(int) * 5 * (size_t)R_);
+    am_w_.alloc(ctx_, sizeof(double) * (size_t)R_ * L_ * I_ * M_);
+    am_d_.alloc(ctx_, sizeof(double) * (size_t)R_ * L_ * I_ * M_);
+    am_dots_.alloc(ctx_, sizeof(double) * (size_t)R_ * L_);
+    am_a_.alloc(ctx_, sizeof(double) * (size_t)R_ * (L_ + 1));
+    for (const auto &t : cfg.monomer_types) {
+        phi_ptrs_.push_back(comp_->phi_type_device(t));
+        w_mono_ptrs_.push_back(comp_->w_device(t));
+    }
+    check_rc(lfts_memset_async(ctx_, w_aux_.get(), 0, w_aux_.size()));
+    for (auto p : phi_ptrs_) check_rc(lfts_memset_async(ctx_, p, 0, sizeof(double) * (size_t)R_ * M_));
+    check_rc(lfts_synchronize(ctx_));
+    am_reset();
+}
+
+BatchedLangevin::~BatchedLangevin() {
+    w_aux_.release(); w_save_.release(); phi_save_.release(); d_cur_.release(); xi_[0].release(); xi_[1].release();
+    partials_.release(); stats_.release(); ctl_.release(); am_w_.release(); am_d_.release(); am_dots_.release(); am_a_.release();
+    comp_.reset();
+}
+
+void BatchedLangevin::set_fields(const double *w) {
+    check_rc(lfts_memcpy_h2d(ctx_, w_aux_.get(), w, w_aux_.size()));
+}
+void BatchedLangevin::get_fields(double *w) const { check_rc(lfts_memcpy_d2h(ctx_, w, w_aux_.get(), w_aux_.size())); }
+void BatchedLangevin::get_concentrations(double *phi) const {
+    for (int r = 0; r < R_; r++)
+        for (int s = 0; s < S_; s++)
+            check_rc(lfts_memcpy_d2h(ctx_, phi + ((size_t)r * S_ + s) * M_, phi_ptrs_[s] + (size_t)r * M_, sizeof(double) * M_));
+}
+
+void BatchedLangevin::am_reset() {
+    n_anderson_.assign(R_, -1);
+    head_.assign(R_, -1);
+    mix_.assign(R_, cfg_.am_mix_init);
+    dot_rows_.assign(R_, {});
+}
+
+double BatchedLangevin::hamiltonian(int r, const std::vector<double> &mean, const std::vector<double> &msq,
+                                    const std::vector<double> &Q) const {
+    // lfts.py:219-235
+    double h = -mean[(size_t)r * S_ + S_ - 1];
+    for (int i = 0; i < S_ - 1; i++) {
+        h += cfg_.h_coef_mu2[i] * msq[(size_t)r * S_ + i];
+        h += cfg_.h_coef_mu1[i] * mean[(size_t)r * S_ + i];
+    }
+    const int P = mol_->get_n_polymer_types();
+    double hp = 0.0;
+    for (int p = 0; p < P; p++) {
+        Polymer &pc = mol_->get_polymer(p);
+        hp -= pc.get_volume_fraction() / pc.get_alpha() * std::log(Q[(size_t)r * P + p]);
+    }
+    return hp + h + cfg_.h_const;
+}
+
+SaddleStats BatchedLangevin::find_saddle_point(bool restore_on_failure) {
+    SaddleStats st;
+    st.iterations.assign(R_, 0);
+    st.error.assign(R_, 1e20);
+    st.failed.assign(R_, 0);
+    am_reset();
+    const long long nI = (long long)I_ * M_;
+    std::vector<int> active(R_, 1), head_flag(R_), ndots(R_), mode(R_), nh(R_);
+    std::vector<double> err_old(R_, 1e20), err(R_, 1e20), a_host((size_t)R_ * L_, 0.0), var((size_t)R_ * I_);
+    int *d_active = comp_->active_device();
+    int *d_head = ctl_.as<int>(), *d_flag = d_head + R_, *d_ndots = d_flag + R_, *d_mode = d_ndots + R_, *d_nh = d_mode + R_;
+    double *d_mix = am_a_.as<double>(), *d_a = d_mix + R_;
+    double *d_mean = stats_.as<double>(), *d_var = d_mean + (size_t)R_ * S_;
+    double *w_imag = w_aux_.as<double>() + (size_t)(S_ - I_) * M_;
+    std::vector<double> scale(I_);
+    for (int c = 0; c < I_; c++) scale[c] = cfg_.dt_scaling[cfg_.imag_idx[c]];
+
+    for (int it = 1; it <= cfg_.max_iter; it++) {
+        bool any = false;
+        for (int r = 0; r < R_; r++) any = any || active[r];
+        if (!any) break;
+        check_rc(lfts_memcpy_h2d(ctx_, d_active, active.data(), sizeof(int) * R_));
+        check_rc(lfts_lfts_monomer_fields(ctx_, R_, S_, M_, cfg_.A.data(), w_aux_.as<double>(), w_mono_ptrs_.data()));
+        comp_->enqueue_statistics();
+        // d = dt_scaling * dH/dw for the imaginary fields (the AM residual of lfts.py:858-863)
+        check_rc(lfts_lfts_field_deriv(ctx_, R_, S_, M_, I_, cfg_.imag_idx.data(), scale.data(), cfg_.A.data(),
+                                       cfg_.h_coef_mu1.data(), cfg_.h_coef_mu2.data(), w_aux_.as<double>(),
+                                       (const double *const *)phi_ptrs_.data(), d_cur_.as<double>(), d_active));
+        check_rc(lfts_lfts_row_moments(ctx_, d_cur_.as<double>(), R_, I_, M_, M_, nI, nullptr, partials_.as<double>(), d_mean,
+                                       d_var));
+        check_rc(lfts_lfts_row_moments(ctx_, d_cur_.as<double>(), R_, I_, M_, M_, nI, d_mean, partials_.as<double>(),
+                                       stats_.as<double>() + 2 * (size_t)R_ * S_, d_var));
+        check_rc(lfts_memcpy_d2h(ctx_, var.data(), d_var, sizeof(double) * R_ * I_));
+        bool need_dots = false;
+        for (int r = 0; r < R_; r++) {
+            head_flag[r] = 0;
+            ndots[r] = 0;
+            mode[r] = 0;
+            nh[r] = 0;
+            if (!active[r]) continue;
+            double e = 0.0;
+            for (int c = 0; c < I_; c++) {
+                const double sd = std::sqrt(std::max(var[(size_t)r * I_ + c], 0.0)) / scale[c];
+                e = (c == 0 || sd > e || std::isnan(sd)) ? sd : e;
+            }
+            err_old[r] = err[r];
+            err[r] = e;
+            st.iterations[r] = it;
+            st.error[r] = e;
+            if (e < cfg_.tolerance) {
+                active[r] = 0;  // converged: this replica's fields and statistics stay as they are
+                continue;
+            }
+            // Anderson-mixing control (CpuAndersonMixing.cpp:86-121)
+            if (e < cfg_.am_start_error || n_anderson_[r] >= 0) n_anderson_[r]++;
+            if (n_anderson_[r] >= 0) {
+                n_anderson_[r] = std::min(cfg_.am_max_hist, n_anderson_[r]);
+                head_[r] = (head_[r] + 1) % L_;
+                head_flag[r] = 1;
+                ndots[r] = n_anderson_[r] + 1;
+                need_dots = true;
+            }
+            if (n_anderson_[r] <= 0) {
+                mix_[r] = (err_old[r] < e) ? std::max(mix_[r] * 0.7, cfg_.am_mix_min) : mix_[r] * 1.01;
+                mode[r] = 1;
+            } else {
+                mode[r] = 2;
+                nh[r] = n_anderson_[r];
+            }
+        }
+        std::vector<int> hd(head_.begin(), head_.end());
+        for (int r = 0; r < R_; r++) hd[r] = std::max(hd[r], 0);
+        check_rc(lfts_memcpy_h2d(ctx_, d_head, hd.data(), sizeof(int) * R_));
+        check_rc(lfts_memcpy_h2d(ctx_, d_flag, head_flag.data(), sizeof(int) * R_));
+        check_rc(lfts_memcpy_h2d(ctx_, d_ndots, ndots.data(), sizeof(int) * R_));
+        if (need_dots) {
+            check_rc(lfts_am_batch_insert(ctx_, R_, nI, L_, d_head, d_flag, w_imag, (long long)S_ * M_, d_cur_.as<double>(), nI,
+                                          am_w_.as<double>(), am_d_.as<double>()));
+            check_rc(lfts_am_batch_dots(ctx_, R_, nI, L_, d_head, d_ndots, am_d_.as<double>(), partials_.as<double>(),
+                                        am_dots_.as<double>()));
+            std::vector<double> dots((size_t)R_ * L_);
+            check_rc(lfts_memcpy_d2h(ctx_, dots.data(), am_dots_.get(), sizeof(double) * dots.size()));
+            for (int r = 0; r < R_; r++) {
+                if (!ndots[r]) continue;
+                auto &rows = dot_rows_[r];
+                rows.insert(rows.begin(), std::vector<double>(dots.begin() + (size_t)r * L_, dots.begin() + (size_t)r * L_ + ndots[r]));
+                if ((int)rows.size() > L_) rows.resize(L_);
+                if (mode[r] == 2) {
+                    const int n = nh[r];
+                    std::vector<std::vector<double>> u(n, std::vector<double>(n));
+                    std::vector<double> v(n), a(n);
+                    for (int i = 0; i < n; i++) {
+                        v[i] = rows[0][0] - rows[0][i + 1];
+                        for (int j = 0; j < n; j++)
+                            u[i][j] = rows[0][0] - rows[0][i + 1] - rows[0][j + 1] + rows[std::min(i + 1, j + 1)][std::abs(i - j)];
+                    }
+                    solve_no_pivot(u, v, a, n);
+                    for (int i = 0; i < n; i++) a_host[(size_t)r * L_ + i] = a[i];
+                }
+            }
+        }
+        check_rc(lfts_memcpy_h2d(ctx_, d_mode, mode.data(), sizeof(int) * R_));
+        check_rc(lfts_memcpy_h2d(ctx_, d_nh, nh.data(), sizeof(int) * R_));
+        check_rc(lfts_memcpy_h2d(ctx_, d_mix, mix_.data(), sizeof(double) * R_));
+        check_rc(lfts_memcpy_h2d(ctx_, d_a, a_host.data(), sizeof(double) * a_host.size()));
+        check_rc(lfts_am_batch_update(ctx_, R_, nI, L_, d_head, d_mode, d_nh, d_mix, d_a, w_imag, (long long)S_ * M_,
+                                      d_cur_.as<double>(), nI, am_w_.as<double>(), am_d_.as<double>(), w_imag,
+                                      (long long)S_ * M_));
+    }
+    // Hamiltonian at the final fields (before the pressure shift, as the reference prints it)
+    check_rc(lfts_lfts_row_moments(ctx_, w_aux_.as<double>(), R_, S_, M_, M_, (long long)S_ * M_, nullptr, partials_.as<double>(),
+                                   d_mean, d_var));
+    std::vector<double> mean((size_t)R_ * S_), msq((size_t)R_ * S_);
+    check_rc(lfts_memcpy_d2h(ctx_, mean.data(), d_mean, sizeof(double) * mean.size()));
+    check_rc(lfts_memcpy_d2h(ctx_, msq.data(), d_var, sizeof(double) * msq.size()));
+    st.partitions = comp_->partitions_host();
+    st.hamiltonian.resize(R_);
+    for (int r = 0; r < R_; r++) st.hamiltonian[r] = hamiltonian(r, mean, msq, st.partitions);
+    // zero-mean pressure field of every replica (lfts.py:866)
+    std::vector<double> pmean(R_);
+    for (int r = 0; r < R_; r++) pmean[r] = mean[(size_t)r * S_ + S_ - 1];
+    check_rc(lfts_memcpy_h2d(ctx_, d_mean, pmean.data(), sizeof(double) * R_));
+    check_rc(lfts_lfts_subtract_mean(ctx_, w_aux_.as<double>(), R_, S_, S_ - 1, M_, d_mean, nullptr));
+    for (int r = 0; r < R_; r++) st.failed[r] = (std::isnan(st.error[r]) || st.error[r] >= cfg_.tolerance) ? 1 : 0;
+    if (restore_on_failure) {
+        const size_t SM = (size_t)S_ * M_;
+        for (int r = 0; r < R_; r++) {
+            if (!st.failed[r]) continue;
+            check_rc(lfts_memcpy_d2d_async(ctx_, w_aux_.as<double>() + r * SM, w_save_.as<double>() + r * SM, sizeof(double) * SM));
+            for (int s = 0; s < S_; s++)
+                check_rc(lfts_memcpy_d2d_async(ctx_, phi_ptrs_[s] + (size_t)r * M_, phi_save_.as<double>() + r * SM + (size_t)s * M_,
+                                               sizeof(double) * M_));
+        }
+    }
+    check_rc(lfts_synchronize(ctx_));
+    return st;
+}
+
+SaddleStats BatchedLangevin::step(const double *noise) {
+    if (Rr_ > 0) {
+        DevBuf &cur = xi_[1 - xi_cur_];
+        check_rc(lfts_memcpy_h2d(ctx_, cur.get(), noise, sizeof(double) * (size_t)R_ * Rr_ * M_));
+    }
+    return step_device(nullptr);
+}
+
+SaddleStats BatchedLangevin::step_device(const double *noise_dev) {
+    const size_t SM = (size_t)S_ * M_;
+    // keep the fields and concentrations to restore replicas whose saddle point fails
+    check_rc(lfts_memcpy_d2d_async(ctx_, w_save_.get(), w_aux_.get(), w_aux_.size()));
+    for (int r = 0; r < R_; r++)
+        for (int s = 0; s < S_; s++)
+            check_rc(lfts_memcpy_d2d_async(ctx_, phi_save_.as<double>() + r * SM + (size_t)s * M_, phi_ptrs_[s] + (size_t)r * M_,
+                                           sizeof(double) * M_));
+    if (Rr_ > 0) {
+        DevBuf &cur = xi_[1 - xi_cur_];
+        if (noise_dev)
+            check_rc(lfts_memcpy_d2d_async(ctx_, cur.get(), noise_dev, sizeof(double) * (size_t)R_ * Rr_ * M_));
+        std::vector<double> s(Rr_);
+        for (int c = 0; c < Rr_; c++) s[c] = cfg_.dt_scaling[cfg_.real_idx[c]];
+        check_rc(lfts_lfts_langevin(ctx_, R_, S_, M_, Rr_, cfg_.real_idx.data(), cfg_.A.data(), cfg_.h_coef_mu1.data(),
+                                    cfg_.h_coef_mu2.data(), (const double *const *)phi_ptrs_.data(), cfg_.dt, s.data(),
+                                    w_aux_.as<double>(), xi_[xi_cur_].as<double>(), cur.as<double>(), nullptr));
+        xi_cur_ = 1 - xi_cur_;  // this step's draw is the next step's "previous" noise (lfts.py:708-709)
+    }
+    return find_saddle_point(true);
+}
+
+}  // namespace lfts

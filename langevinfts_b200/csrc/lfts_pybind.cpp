@@ -11,6 +11,7 @@
 
 #include "lfts_computation.h"
 #include "lfts_host.h"
+#include "lfts_langevin.h"
 
 namespace py = pybind11;
 using namespace lfts;
@@ -303,6 +304,83 @@ PYBIND11_MODULE(langevinfts, m) {
                       << "), device " << f.device << std::endl;
         })
         .def("get_model_name", [](Factory &) { return std::string(""); });
+
+    // Batched L-FTS engine: n_replicas independent systems on the device.
+    py::class_<BatchedLangevin>(m, "BatchedLangevin")
+        .def(py::init([](Factory &f, ComputationBox *cb, Molecules *mol, PropagatorAnalyzer *pa, int n_replicas, py::dict c) {
+            LangevinConfig cfg;
+            cfg.monomer_types = c["monomer_types"].cast<std::vector<std::string>>();
+            cfg.A = c["matrix_a"].cast<std::vector<double>>();
+            cfg.h_coef_mu1 = c["h_coef_mu1"].cast<std::vector<double>>();
+            cfg.h_coef_mu2 = c["h_coef_mu2"].cast<std::vector<double>>();
+            cfg.h_const = c["h_const"].cast<double>();
+            cfg.real_idx = c["real_idx"].cast<std::vector<int>>();
+            cfg.imag_idx = c["imag_idx"].cast<std::vector<int>>();
+            cfg.dt_scaling = c["dt_scaling"].cast<std::vector<double>>();
+            cfg.dt = c["dt"].cast<double>();
+            cfg.tolerance = c["tolerance"].cast<double>();
+            cfg.max_iter = c["max_iter"].cast<int>();
+            cfg.am_max_hist = c["am_max_hist"].cast<int>();
+            cfg.am_start_error = c["am_start_error"].cast<double>();
+            cfg.am_mix_min = c["am_mix_min"].cast<double>();
+            cfg.am_mix_init = c["am_mix_init"].cast<double>();
+            return new BatchedLangevin(cb, mol, pa, f.precision, f.device, n_replicas, cfg);
+        }), py::keep_alive<1, 3>(), py::keep_alive<1, 4>(), py::keep_alive<1, 5>())
+        .def("n_replicas", &BatchedLangevin::n_replicas)
+        .def("stream_ptr", [](BatchedLangevin &b) { return (std::uintptr_t)b.stream(); })
+        .def("kernel_launches", [](BatchedLangevin &b) { return b.computation().kernel_launches(); })
+        .def("context_ptr", [](BatchedLangevin &b) { return (std::uintptr_t)b.computation().context(); })
+        .def("step_device", [](BatchedLangevin &b, std::uintptr_t noise_dev) {
+            SaddleStats s;
+            {
+                py::gil_scoped_release nogil;
+                s = b.step_device((const double *)noise_dev);
+            }
+            py::dict d;
+            d["iterations"] = s.iterations; d["error"] = s.error; d["hamiltonian"] = s.hamiltonian;
+            d["failed"] = s.failed; d["partitions"] = s.partitions;
+            return d;
+        })
+        .def("set_fields", [](BatchedLangevin &b, Arr w) {
+            py::buffer_info bi = w.request();
+            size_check(bi, (long long)b.n_replicas() * b.n_grid() * (long long)(bi.size / ((long long)b.n_replicas() * b.n_grid())),
+                       "w_aux ", "n_replicas*S*n_grid");
+            b.set_fields((const double *)bi.ptr);
+        })
+        .def("get_fields", [](BatchedLangevin &b, int S) {
+            py::array_t<double> w({(py::ssize_t)b.n_replicas(), (py::ssize_t)S, (py::ssize_t)b.n_grid()});
+            b.get_fields((double *)w.request().ptr);
+            return w;
+        })
+        .def("get_concentrations", [](BatchedLangevin &b, int S) {
+            py::array_t<double> phi({(py::ssize_t)b.n_replicas(), (py::ssize_t)S, (py::ssize_t)b.n_grid()});
+            b.get_concentrations((double *)phi.request().ptr);
+            return phi;
+        })
+        .def("find_saddle_point", [](BatchedLangevin &b) {
+            SaddleStats s;
+            {
+                py::gil_scoped_release nogil;
+                s = b.find_saddle_point(false);
+            }
+            py::dict d;
+            d["iterations"] = s.iterations; d["error"] = s.error; d["hamiltonian"] = s.hamiltonian;
+            d["failed"] = s.failed; d["partitions"] = s.partitions;
+            return d;
+        })
+        .def("step", [](BatchedLangevin &b, Arr noise) {
+            py::buffer_info bi = noise.request();
+            size_check(bi, (long long)b.n_replicas() * b.n_real() * b.n_grid(), "noise ", "n_replicas*n_real*n_grid");
+            SaddleStats s;
+            {
+                py::gil_scoped_release nogil;
+                s = b.step((const double *)bi.ptr);
+            }
+            py::dict d;
+            d["iterations"] = s.iterations; d["error"] = s.error; d["hamiltonian"] = s.hamiltonian;
+            d["failed"] = s.failed; d["partitions"] = s.partitions;
+            return d;
+        });
 
     py::class_<PlatformSelector>(m, "PlatformSelector")
         .def(py::init<>())

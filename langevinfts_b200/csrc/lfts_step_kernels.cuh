@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(NTHR) k_plane_forward(GridPlan g, const lfts_s
     const int n1 = g.n1, n2 = g.n2, nzc = g.nzc;
     PlaneSmem<C> sm(smem_raw, NBR, n1, n2, nzc, false);
     const lfts_step_job jb = jobs[blockIdx.y];
+    if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     load_plane_tables(g, sm);
@@ -162,6 +163,7 @@ __global__ void __launch_bounds__(NTHR) k_xpass(GridPlan g, const lfts_step_job 
     C *twx = tile + NBR * n0 * TJ;
     short *px = (short *)(twx + n0);
     const lfts_step_job jb = jobs[blockIdx.y];
+    if (jb.active && !jb.active[jb.replica]) return;
     const int tid = threadIdx.x;
     for (int i = tid; i < n0; i += NTHR) { twx[i] = ((const C *)g.tw[0])[i]; px[i] = g.perm[0][i]; }
     __syncthreads();
@@ -224,6 +226,7 @@ __global__ void __launch_bounds__(NTHR) k_plane_mid(GridPlan g, const lfts_step_
     const int n1 = g.n1, n2 = g.n2, nzc = g.nzc;
     PlaneSmem<C> sm(smem_raw, 1, n1, n2, nzc, true);
     const lfts_step_job jb = jobs[blockIdx.y];
+    if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     load_plane_tables(g, sm);
@@ -284,6 +287,7 @@ __global__ void __launch_bounds__(NTHR) k_plane_inverse(GridPlan g, const lfts_s
     const int n1 = g.n1, n2 = g.n2, nzc = g.nzc;
     PlaneSmem<C> sm(smem_raw, NBR, n1, n2, nzc, false);
     const lfts_step_job jb = jobs[blockIdx.y];
+    if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     load_plane_tables(g, sm);

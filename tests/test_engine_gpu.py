@@ -134,11 +134,11 @@ def test_dots_phi_am():
     coef = orc.simpson_coeff(NR)
     pc = ctx.upload(coef)
     phi = ctx.malloc(2 * M * 8)
-    pj = (PhiJob * 1)(PhiJob(pql, pqr, None, phi, 1.7, NL, NR, 0, 0))
+    pj = (PhiJob * 1)(PhiJob(pql, pqr, None, phi, 1.7, None, NL, NR, 0, 0))
     check(ctx.lib.lfts_phi_blocks(ctx.h, 0, ctx.upload(np.frombuffer(pj, dtype=np.uint8)), 1, pc))
     ref = 1.7 * sum(coef[n] * ql[NL - n] * qr[n] for n in range(NR + 1))
     assert np.max(np.abs(ctx.d2h(phi, (M,), np.float64) - ref)) < 1e-12 * np.max(ref)
-    pj = (PhiJob * 1)(PhiJob(pql, pqr, pw, phi + M * 8, 0.3, NL, NR, 0, 0))
+    pj = (PhiJob * 1)(PhiJob(pql, pqr, pw, phi + M * 8, 0.3, None, NL, NR, 0, 0))
     check(ctx.lib.lfts_phi_blocks(ctx.h, 1, ctx.upload(np.frombuffer(pj, dtype=np.uint8)), 1, pc))
     ref = 0.3 * sum(ql[NL - n + 1] * qr[n] for n in range(1, NR + 1)) / w
     assert np.max(np.abs(ctx.d2h(phi + M * 8, (M,), np.float64) - ref)) < 1e-12 * np.max(ref)
