@@ -114,10 +114,27 @@ def load_reference():
     return mod
 
 
-def reference_sample(n_iter, threads):
+def reference_sample(n_iter, threads, timeout=900):
     """Time n_iter saddle-point iterations of one replica on the reference CPU
-    platform through the same driver; returns (seconds per iteration, threads)."""
-    os.environ["OMP_NUM_THREADS"] = str(threads)
+    platform through the same driver; returns (seconds per iteration, threads).
+    Runs in a child process: the reference keeps two grids of reals and two of
+    complex spectra per contour step on the stack (CpuSolverPseudo.cpp:127-128,
+    8.3 MB at 64^3) and needs an unlimited stack and OMP_STACKSIZE, as its
+    README and driver set them."""
+    import resource
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_STACKSIZE="1G")
+
+    def unlimited_stack():
+        resource.setrlimit(resource.RLIMIT_STACK, (resource.RLIM_INFINITY, resource.RLIM_INFINITY))
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-sample", str(n_iter), "--threads", str(threads)],
+                       env=env, preexec_fn=unlimited_stack, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout[-2000:] + r.stderr[-2000:])
+        return None
+    return tuple(json.loads(r.stdout.strip().splitlines()[-1]))
+
+
+def _reference_sample_child(n_iter, threads):
     ref = load_reference()
     if ref is None:
         return None
@@ -141,7 +158,8 @@ def reference_sample(n_iter, threads):
         w_aux[sim.mpt.aux_fields_imag_idx] = np.reshape(
             sim.am.calculate_new_fields(w_aux[sim.mpt.aux_fields_imag_idx], -h, old, err), [len(sim.mpt.aux_fields_imag_idx), M])
         ts.append(time.perf_counter() - t0)
-    return float(np.mean(ts[1:])), threads
+    print(json.dumps([float(np.mean(ts[1:])), threads]))
+    return 0
 
 
 def run_reference(args):
@@ -154,12 +172,11 @@ def run_reference(args):
     if ref is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) is missing"}))
         return 0
-    t_all = []
-    for k in range(args.warmup + args.steps):
-        t_iter, _ = reference_sample(1, threads)
-        if k >= args.warmup:
-            t_all.append(t_iter)
-    t_iter = float(np.mean(t_all))
+    r = reference_sample(args.steps, threads)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference CPU platform failed on this host (see stderr)"}))
+        return 0
+    t_iter = r[0]
     v = 1.0 / (t_iter * ITERS_PER_STEP)
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
@@ -167,8 +184,9 @@ def run_reference(args):
            "config": {"workload": "batched L-FTS AB diblock 64^3 N=90 (reference CPU: one replica)", "grid": [64, 64, 64],
                       "N": 90, "replicas": 1},
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                            "sample": f"one saddle-point iteration per step (1 replica, 64^3, N=90) x {ITERS_PER_STEP} "
-                                      "iterations per Langevin step; reference CPU platform with the project FFT in place of MKL"},
+                            "sample": f"{args.steps} timed saddle-point iterations (after 1 untimed) of 1 replica, 64^3, N=90, "
+                                      f"x {ITERS_PER_STEP} iterations per Langevin step; reference CPU platform, project FFT "
+                                      "in place of MKL"},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
@@ -290,6 +308,8 @@ def run_ours(args):
         if dist is not None:
             dist.destroy_process_group()
         return 0
+    sys.stderr.write(f"[bench] value {value:.3f} {UNIT}, e2e {e2e:.3f}, mean saddle iterations {np.mean(iters):.2f}, "
+                     f"failed {fails}, launches {launches}\n")
     # ---- roofline of the fused continuous step at the workload batch shape
     njobs = 2 * R  # two propagators per schedule slot (A and B side) per replica
     ms, Mg, Mcg = roofline_step_kernel(args.nx, njobs)
@@ -313,6 +333,7 @@ def run_ours(args):
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         r = reference_sample(1, threads)
+        sys.stderr.write(f"[bench] reference CPU sample: {r}\n")
         if r is not None:
             mean_iters = float(np.mean(iters)) if iters else ITERS_PER_STEP
             cpu = {"value": 1.0 / (r[0] * mean_iters), "unit": UNIT, "cores": r[1], "kind": "reference",
@@ -353,9 +374,23 @@ def main():
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--nx", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-sample", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--threads", type=int, default=1, help=argparse.SUPPRESS)
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="only time the fused continuous step at 2*replicas jobs (for profiling)")
     args = ap.parse_args()
+    if args.ref_sample:
+        return _reference_sample_child(args.ref_sample, args.threads)
     if args.warmup < 3:
         args.warmup = 3
+    if args.kernel_only:
+        import torch
+        torch.cuda.init()
+        ms, M, Mc = roofline_step_kernel(args.nx, 2 * args.replicas, reps=args.steps)
+        unit = 8 * (12 * M + 24 * Mc)
+        print(json.dumps({"kernel": "lfts_step_continuous", "jobs": 2 * args.replicas, "nx": args.nx, "launch_ms": ms,
+                          "pass_model_GBps": 2 * args.replicas * unit / (ms * 1e-3) / 1e9}))
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -97,17 +97,25 @@ __global__ void k_xstress(GridPlan g, const lfts_step_job *__restrict__ sj, cons
 // contexts with different grids share the kernels, so every kernel gets the
 // device's opt-in maximum once instead of a per-grid value (a smaller grid's
 // context would otherwise lower the limit another context relies on).
-template <typename T, bool GEN> static void set_attrs_t(int max_smem) {
-    const int a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    cudaFuncSetAttribute(k_plane_forward<T, 1, GEN>, (cudaFuncAttribute)a, max_smem);
-    cudaFuncSetAttribute(k_plane_forward<T, 2, GEN>, (cudaFuncAttribute)a, max_smem);
-    cudaFuncSetAttribute(k_plane_mid<T, GEN>, (cudaFuncAttribute)a, max_smem);
-    cudaFuncSetAttribute(k_plane_inverse<T, 1, EPI_SCALE, GEN>, (cudaFuncAttribute)a, max_smem);
-    cudaFuncSetAttribute(k_plane_inverse<T, 1, EPI_RICH_ACC, GEN>, (cudaFuncAttribute)a, max_smem);
-    cudaFuncSetAttribute(k_plane_inverse<T, 2, EPI_RICH, GEN>, (cudaFuncAttribute)a, max_smem);
-    cudaFuncSetAttribute(k_xpass<T, 1, GEN>, (cudaFuncAttribute)a, max_smem);
-    cudaFuncSetAttribute(k_xpass<T, 2, GEN>, (cudaFuncAttribute)a, max_smem);
-    cudaFuncSetAttribute(k_xstress<T, GEN>, (cudaFuncAttribute)a, max_smem);
+// (the dynamic limit is the opt-in maximum minus the kernel's static shared memory)
+template <typename K> static cudaError_t allow_smem(K kernel, int max_smem) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem - (int)fa.sharedSizeBytes);
+}
+template <typename T, bool GEN> static cudaError_t set_attrs_t(int max_smem) {
+    cudaError_t e = cudaSuccess, r;
+    if ((r = allow_smem(k_plane_forward<T, 1, GEN>, max_smem)) != cudaSuccess) e = r;
+    if ((r = allow_smem(k_plane_forward<T, 2, GEN>, max_smem)) != cudaSuccess) e = r;
+    if ((r = allow_smem(k_plane_mid<T, GEN>, max_smem)) != cudaSuccess) e = r;
+    if ((r = allow_smem(k_plane_inverse<T, 1, EPI_SCALE, GEN>, max_smem)) != cudaSuccess) e = r;
+    if ((r = allow_smem(k_plane_inverse<T, 1, EPI_RICH_ACC, GEN>, max_smem)) != cudaSuccess) e = r;
+    if ((r = allow_smem(k_plane_inverse<T, 2, EPI_RICH, GEN>, max_smem)) != cudaSuccess) e = r;
+    if ((r = allow_smem(k_xpass<T, 1, GEN>, max_smem)) != cudaSuccess) e = r;
+    if ((r = allow_smem(k_xpass<T, 2, GEN>, max_smem)) != cudaSuccess) e = r;
+    if ((r = allow_smem(k_xstress<T, GEN>, max_smem)) != cudaSuccess) e = r;
+    return e;
 }
 
 template <typename T> static int setup_plan(lfts_ctx c) {
@@ -156,8 +164,7 @@ template <typename T> static int setup_plan(lfts_ctx c) {
         return fail("grid plane " + std::to_string(g.n1) + "x" + std::to_string(g.n2) +
                     " does not fit in shared memory (" + std::to_string(c->sm_mid) + " > " + std::to_string(max_smem) + " bytes)");
     c->nbr2 = (int)c->sm_pf2 <= max_smem && (int)c->sm_x2 <= max_smem;
-    if (c->gen) set_attrs_t<T, true>(max_smem); else set_attrs_t<T, false>(max_smem);
-    CK(cudaGetLastError());
+    CK((c->gen ? set_attrs_t<T, true>(max_smem) : set_attrs_t<T, false>(max_smem)));
     return 0;
 }
 

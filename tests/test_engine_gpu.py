@@ -157,7 +157,8 @@ def test_dots_phi_am():
     pwh, pdh, pa2 = ctx.upload(wh), ctx.upload(dh), ctx.upload(av)
     wn = ctx.malloc(M * 8)
     check(ctx.lib.lfts_am_update(ctx.h, wn, pwh, pdh, M, nh - 1, pa2, M, 0, nh))
-    ref = wh[0] + dh[0] + sum(av[i] * (wh[i + 1] + dh[i + 1] - wh[0] - dh[0]) for i in range(nh - 1))
+    # head = 0: the k-th newest history is ring slot (-k) mod nh
+    ref = wh[0] + dh[0] + sum(av[i] * (wh[(-(i + 1)) % nh] + dh[(-(i + 1)) % nh] - wh[0] - dh[0]) for i in range(nh - 1))
     assert np.allclose(ctx.d2h(wn, (M,), np.float64), ref, rtol=1e-13, atol=1e-13)
     ctx.close()
 
