@@ -10,12 +10,13 @@
  *
  * Algorithm (own restatement of textbook methods):
  *   - complex transforms use a mixed-radix Stockham auto-sort decimation in
- *     frequency, radices 4, 2, 3, 5 hand-coded and any other prime by a direct
- *     small DFT.  A strided axis of a row-major array is transformed in place
+ *     frequency, radices 4 and 2 hand-coded and any other prime by a direct
+ *     small DFT, twiddles hoisted out of the inner loop.  A strided axis of a row-major array is transformed in place
  *     of its layout: element i of column q sits at q + B*i, which is exactly
  *     the interleaved form Stockham works on, so no transposes are needed.
  *   - the last (contiguous) axis is real: two real rows a, b are packed into
- *     one complex row a + i b, transformed once, and separated with
+ *     one complex row a + i b (16 such pairs at a time, interleaved, so the
+ *     same Stockham inner loop runs over them), transformed once, and separated with
  *     A[k] = (Z[k] + conj Z[n-k])/2, B[k] = (Z[k] - conj Z[n-k])/(2i).
  *     The inverse rebuilds Z = A + iB from the Hermitian halves (imaginary
  *     parts of the DC and Nyquist bins are dropped, as a c2r transform does).
@@ -23,6 +24,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -67,45 +69,49 @@ struct Plan1D {
 
 // One Stockham DIF pass over B interleaved sequences of length n.
 // x and y have n*B elements; returns the buffer holding the result.
-cpx *stockham(const Plan1D &p, int B, cpx *x, cpx *y, int sign) {
+cpx *stockham(const Plan1D &p, long B, cpx *x, cpx *y, int sign) {
     const int N = p.n;
     long s = B;
     int ncur = N;
-    cpx a[64], b[64];
-    std::vector<cpx> abig, bbig;
     for (int r : p.radices) {
         const int m = ncur / r;
         const long stride_tw = N / ncur;  // w_ncur^e = w_N^(e*stride_tw)
-        cpx *ap = a, *bp = b;
-        if (r > 64) { abig.resize(r); bbig.resize(r); ap = abig.data(); bp = bbig.data(); }
+        // small-DFT matrix w_r^(jk) for generic radices
+        std::vector<cpx> wr((size_t)r * r);
+        for (int j = 0; j < r; j++)
+            for (int k = 0; k < r; k++) wr[(size_t)j * r + k] = p.w((long)(N / r) * ((j * k) % r), sign);
+        std::vector<cpx> twk(r), a(r), b(r);
         for (int pp = 0; pp < m; pp++) {
-            for (long q = 0; q < s; q++) {
-                for (int j = 0; j < r; j++) ap[j] = x[q + s * (pp + (long)j * m)];
-                if (r == 2) {
-                    bp[0] = cadd(ap[0], ap[1]);
-                    bp[1] = csub(ap[0], ap[1]);
-                } else if (r == 4) {
-                    cpx t0 = cadd(ap[0], ap[2]), t1 = csub(ap[0], ap[2]);
-                    cpx t2 = cadd(ap[1], ap[3]), t3 = csub(ap[1], ap[3]);
-                    // multiply t3 by -i (forward) or +i (backward)
-                    cpx t3r = sign < 0 ? cpx{t3.im, -t3.re} : cpx{-t3.im, t3.re};
-                    bp[0] = cadd(t0, t2);
-                    bp[2] = csub(t0, t2);
-                    bp[1] = cadd(t1, t3r);
-                    bp[3] = csub(t1, t3r);
-                } else {
-                    const long step = N / r;  // w_r^1 = w_N^(N/r)
-                    for (int k = 0; k < r; k++) {
-                        cpx acc = ap[0];
-                        for (int j = 1; j < r; j++)
-                            acc = cadd(acc, cmul(ap[j], p.w(step * (long)((j * k) % r), sign)));
-                        bp[k] = acc;
-                    }
+            for (int k = 0; k < r; k++) twk[k] = p.w((long)pp * k * stride_tw, sign);
+            const cpx *xs = x + s * pp;
+            cpx *ys = y + s * (long)r * pp;
+            if (r == 2) {
+                const cpx t1 = twk[1];
+                for (long q = 0; q < s; q++) {
+                    const cpx a0 = xs[q], a1 = xs[q + s * m];
+                    ys[q] = cadd(a0, a1);
+                    ys[q + s] = cmul(csub(a0, a1), t1);
                 }
-                for (int k = 0; k < r; k++) {
-                    cpx v = bp[k];
-                    if (pp != 0 && k != 0) v = cmul(v, p.w((long)pp * k * stride_tw, sign));
-                    y[q + s * ((long)r * pp + k)] = v;
+            } else if (r == 4) {
+                const cpx t1 = twk[1], t2 = twk[2], t3 = twk[3];
+                for (long q = 0; q < s; q++) {
+                    const cpx a0 = xs[q], a1 = xs[q + s * m], a2 = xs[q + 2 * s * m], a3 = xs[q + 3 * s * m];
+                    const cpx u0 = cadd(a0, a2), u1 = csub(a0, a2), u2 = cadd(a1, a3), d = csub(a1, a3);
+                    const cpx u3 = sign < 0 ? cpx{d.im, -d.re} : cpx{-d.im, d.re};
+                    ys[q] = cadd(u0, u2);
+                    ys[q + s] = cmul(cadd(u1, u3), t1);
+                    ys[q + 2 * s] = cmul(csub(u0, u2), t2);
+                    ys[q + 3 * s] = cmul(csub(u1, u3), t3);
+                }
+            } else {
+                for (long q = 0; q < s; q++) {
+                    for (int j = 0; j < r; j++) a[j] = xs[q + s * (long)j * m];
+                    for (int k = 0; k < r; k++) {
+                        cpx acc = a[0];
+                        for (int j = 1; j < r; j++) acc = cadd(acc, cmul(a[j], wr[(size_t)j * r + k]));
+                        b[k] = acc;
+                    }
+                    for (int k = 0; k < r; k++) ys[q + s * k] = k ? cmul(b[k], twk[k]) : b[k];
                 }
             }
         }
@@ -134,10 +140,12 @@ void c2c_axis(const Descriptor &d, const long *cshape, int ax, cpx *data, std::v
     work.resize(block);
     for (long o = 0; o < outer; o++) {
         cpx *x = data + o * block;
-        cpx *res = stockham(d.plans[ax], (int)inner, x, work.data(), sign);
+        cpx *res = stockham(d.plans[ax], inner, x, work.data(), sign);
         if (res != x) std::memcpy(x, res, sizeof(cpx) * block);
     }
 }
+
+constexpr long GROUP = 16;  // row pairs transformed together as interleaved columns
 
 void forward(const Descriptor &d, const double *in, cpx *out) {
     const long nz = d.len[d.dim - 1];
@@ -145,18 +153,25 @@ void forward(const Descriptor &d, const double *in, cpx *out) {
     long rows = 1;
     for (int i = 0; i < d.dim - 1; i++) rows *= d.len[i];
     const Plan1D &pz = d.plans[d.dim - 1];
-    std::vector<cpx> zl(nz), wk(nz);
-    for (long r = 0; r < rows; r += 2) {
-        const double *ra = in + r * nz;
-        const double *rb = (r + 1 < rows) ? in + (r + 1) * nz : nullptr;
-        for (long t = 0; t < nz; t++) zl[t] = {ra[t], rb ? rb[t] : 0.0};
-        cpx *Z = stockham(pz, 1, zl.data(), wk.data(), -1);
-        for (long k = 0; k < nzc; k++) {
-            cpx zk = Z[k], zn = cconj(Z[(nz - k) % nz]);
-            cpx A = {0.5 * (zk.re + zn.re), 0.5 * (zk.im + zn.im)};
-            cpx Bv = {0.5 * (zk.im - zn.im), -0.5 * (zk.re - zn.re)};
-            out[r * nzc + k] = A;
-            if (rb) out[(r + 1) * nzc + k] = Bv;
+    const long pairs = (rows + 1) / 2;
+    std::vector<cpx> zl(nz * GROUP), wk(nz * GROUP);
+    for (long g0 = 0; g0 < pairs; g0 += GROUP) {
+        const long G = std::min(GROUP, pairs - g0);
+        for (long g = 0; g < G; g++) {
+            const long r = 2 * (g0 + g);
+            const double *ra = in + r * nz;
+            const double *rb = (r + 1 < rows) ? in + (r + 1) * nz : nullptr;
+            for (long t = 0; t < nz; t++) zl[t * G + g] = {ra[t], rb ? rb[t] : 0.0};
+        }
+        cpx *Z = stockham(pz, G, zl.data(), wk.data(), -1);
+        for (long g = 0; g < G; g++) {
+            const long r = 2 * (g0 + g);
+            const bool pair = r + 1 < rows;
+            for (long k = 0; k < nzc; k++) {
+                cpx zk = Z[k * G + g], zn = cconj(Z[((nz - k) % nz) * G + g]);
+                out[r * nzc + k] = {0.5 * (zk.re + zn.re), 0.5 * (zk.im + zn.im)};
+                if (pair) out[(r + 1) * nzc + k] = {0.5 * (zk.im - zn.im), -0.5 * (zk.re - zn.re)};
+            }
         }
     }
     long cshape[3];
@@ -178,26 +193,34 @@ void backward(const Descriptor &d, const cpx *in, double *out) {
     std::vector<cpx> work;
     for (int ax = 0; ax <= d.dim - 2; ax++) c2c_axis(d, cshape, ax, buf.data(), work, +1);
     const Plan1D &pz = d.plans[d.dim - 1];
-    std::vector<cpx> zl(nz), wk(nz), A(nz), Bf(nz);
-    for (long r = 0; r < rows; r += 2) {
-        const bool pair = (r + 1 < rows);
-        for (long k = 0; k < nz; k++) {
-            cpx a, b = {0.0, 0.0};
-            if (k < nzc) {
-                a = buf[r * nzc + k];
-                if (pair) b = buf[(r + 1) * nzc + k];
-            } else {
-                a = cconj(buf[r * nzc + (nz - k)]);
-                if (pair) b = cconj(buf[(r + 1) * nzc + (nz - k)]);
+    const long pairs = (rows + 1) / 2;
+    std::vector<cpx> zl(nz * GROUP), wk(nz * GROUP);
+    for (long g0 = 0; g0 < pairs; g0 += GROUP) {
+        const long G = std::min(GROUP, pairs - g0);
+        for (long g = 0; g < G; g++) {
+            const long r = 2 * (g0 + g);
+            const bool pair = (r + 1 < rows);
+            for (long k = 0; k < nz; k++) {
+                cpx a, b = {0.0, 0.0};
+                if (k < nzc) {
+                    a = buf[r * nzc + k];
+                    if (pair) b = buf[(r + 1) * nzc + k];
+                } else {
+                    a = cconj(buf[r * nzc + (nz - k)]);
+                    if (pair) b = cconj(buf[(r + 1) * nzc + (nz - k)]);
+                }
+                if (k == 0 || (nz % 2 == 0 && k == nz / 2)) { a.im = 0.0; b.im = 0.0; }
+                zl[k * G + g] = {a.re - b.im, a.im + b.re};  // Z = a + i b
             }
-            if (k == 0 || (nz % 2 == 0 && k == nz / 2)) { a.im = 0.0; b.im = 0.0; }
-            // Z = a + i b
-            zl[k] = {a.re - b.im, a.im + b.re};
         }
-        cpx *z = stockham(pz, 1, zl.data(), wk.data(), +1);
-        for (long t = 0; t < nz; t++) {
-            out[r * nz + t] = z[t].re;
-            if (pair) out[(r + 1) * nz + t] = z[t].im;
+        cpx *z = stockham(pz, G, zl.data(), wk.data(), +1);
+        for (long g = 0; g < G; g++) {
+            const long r = 2 * (g0 + g);
+            const bool pair = (r + 1 < rows);
+            for (long t = 0; t < nz; t++) {
+                out[r * nz + t] = z[t * G + g].re;
+                if (pair) out[(r + 1) * nz + t] = z[t * G + g].im;
+            }
         }
     }
 }
