@@ -39,7 +39,7 @@ UNIT = "replica-steps/s"
 # mean saddle-point iterations per Langevin step of this workload, measured by
 # the GPU arm on B200 (the algorithm and inputs are the reference's, so the
 # reference arm uses it to convert its timed saddle iterations into steps/s)
-ITERS_PER_STEP = 13.9
+ITERS_PER_STEP = 44.0
 
 
 def params(nx=64, lx=7.3):
@@ -192,6 +192,22 @@ def run_reference(args):
     return 0
 
 
+def step_traffic_per_job(s_bytes):
+    """DRAM bytes (read + write) per (replica, key, contour step) of one
+    continuous step, from the ncu summary committed under profiles/ (the line
+    'dram_bytes_per_job_step f64 <bytes>'), or None when it is absent."""
+    tag = {8: "f64", 4: "f32"}[s_bytes]
+    try:
+        with open(os.path.join(ROOT, "profiles", "step_continuous_64cubed.txt")) as fh:
+            for line in fh:
+                f = line.split()
+                if len(f) == 3 and f[0] == "dram_bytes_per_job_step" and f[1] == tag:
+                    return float(f[2])
+    except OSError:
+        pass
+    return None
+
+
 def roofline_step_kernel(nx, njobs, reps=20):
     """Time lfts_step_continuous at the batch shape of the workload (njobs =
     replicas x propagators per schedule slot) with CUDA events on its stream.
@@ -322,12 +338,9 @@ def run_ours(args):
     s_bytes = 8
     unit_bytes = s_bytes * (12 * Mg + 24 * Mcg)  # pass-model bytes per (replica, key, contour step)
     achieved = njobs * unit_bytes / (ms * 1e-3) / 1e9
-    traffic = None
-    try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "step_traffic.json")))
-        traffic = prof["dram_bytes_per_job_step"] * njobs
-    except (OSError, KeyError, ValueError):
-        pass
+    traffic = step_traffic_per_job(s_bytes) if args.nx == 64 else None
+    if traffic is not None:
+        traffic *= njobs
     # ---- CPU baseline: the reference CPU platform on a bounded sample
     cpu = None
     if not args.no_cpu_baseline:

@@ -1,8 +1,8 @@
 """ctypes binding of the C ABI in include/lfts_b200.h (liblfts_b200.so).
 
-This is the binding a non-C++ host would add; the tests
-use it to call the engine entry points directly.  Loading fails loudly when
-the shared library has not been built: there is no CPU fallback.
+This is the binding a non-C++ host would add; the tests use it to call the
+engine entry points directly.  Loading fails loudly when the shared library
+has not been built: there is no CPU fallback.
 """
 import ctypes as C
 import os

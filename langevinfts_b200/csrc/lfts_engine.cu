@@ -5,11 +5,12 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
-#include "lfts_step_kernels.cuh"
+#include "lfts_step_fast.cuh"
 
 using namespace lfts;
 
@@ -39,7 +40,9 @@ struct lfts_ctx_s {
     GridPlan g;
     void *tables = nullptr;
     bool gen = false, nbr2 = true;
-    int TJ = 16, ntiles = 1;
+    int TJ = 16, ntiles = 1, zb = 1;
+    int fastN = 0;            // cubic grid handled by the compile-time specialised kernels (0: generic)
+    void *stw = nullptr;
     size_t sm_pf1 = 0, sm_pf2 = 0, sm_mid = 0, sm_inv1 = 0, sm_inv2 = 0, sm_x1 = 0, sm_x2 = 0;
     double *partials = nullptr;
     size_t partials_cap = 0;
@@ -118,6 +121,23 @@ template <typename T, bool GEN> static cudaError_t set_attrs_t(int max_smem) {
     return e;
 }
 
+// Attributes of the cubic fast kernels; 0 when their shared memory does not fit.
+template <typename T, int N> static int fast_setup(int max_smem) {
+    using C = typename CT<T>::type;
+    const size_t f2 = fast::FSmem<C, N, 2, 1>::BYTES, f1 = fast::FSmem<C, N, 1, 1>::BYTES;
+    const size_t x2 = sizeof(C) * (2 * (size_t)N * (sizeof(T) == 8 ? 16 : 32) + fast::stw_size(N) + 1);
+    if (f2 > (size_t)max_smem || x2 > (size_t)max_smem) return 0;
+    if (allow_smem(fast::kf_plane_forward<T, 1, N>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(fast::kf_plane_forward<T, 2, N>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(fast::kf_plane_mid<T, N>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(fast::kf_plane_inverse<T, 2, EPI_RICH, N>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(fast::kf_plane_inverse<T, 1, EPI_SCALE, N>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(fast::kf_xpass<T, 1, N>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(fast::kf_xpass<T, 2, N>, max_smem) != cudaSuccess) return 0;
+    (void)f1;
+    return 1;
+}
+
 template <typename T> static int setup_plan(lfts_ctx c) {
     using C = typename CT<T>::type;
     GridPlan &g = c->g;
@@ -151,11 +171,15 @@ template <typename T> static int setup_plan(lfts_ctx c) {
 
     int max_smem = 0;
     CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    max_smem -= 64;  // headroom for static shared memory of the reduction kernels
     c->TJ = (sizeof(T) == 8) ? 16 : 32;
     c->ntiles = (int)((g.n1 * (long long)g.nzc + c->TJ - 1) / c->TJ);
-    c->sm_pf1 = PlaneSmem<C>::bytes(1, g.n1, g.n2, g.nzc, false);
-    c->sm_pf2 = PlaneSmem<C>::bytes(2, g.n1, g.n2, g.nzc, false);
-    c->sm_mid = PlaneSmem<C>::bytes(1, g.n1, g.n2, g.nzc, true);
+    // z-lines per warp: enough lines that a radix-8 stage keeps 32 lanes busy
+    c->zb = g.n2 <= 32 ? 8 : (g.n2 <= 128 ? 4 : 1);
+    while (c->zb > 1 && PlaneSmem<C>::bytes(1, g.n1, g.n2, g.nzc, true, c->zb) > (size_t)max_smem) c->zb /= 2;
+    c->sm_pf1 = PlaneSmem<C>::bytes(1, g.n1, g.n2, g.nzc, false, c->zb);
+    c->sm_pf2 = PlaneSmem<C>::bytes(2, g.n1, g.n2, g.nzc, false, c->zb);
+    c->sm_mid = PlaneSmem<C>::bytes(1, g.n1, g.n2, g.nzc, true, c->zb);
     c->sm_inv1 = c->sm_pf1;
     c->sm_inv2 = c->sm_pf2;
     c->sm_x1 = sizeof(C) * (1 * (size_t)g.n0 * c->TJ + g.n0) + sizeof(short) * g.n0;
@@ -165,6 +189,39 @@ template <typename T> static int setup_plan(lfts_ctx c) {
                     " does not fit in shared memory (" + std::to_string(c->sm_mid) + " > " + std::to_string(max_smem) + " bytes)");
     c->nbr2 = (int)c->sm_pf2 <= max_smem && (int)c->sm_x2 <= max_smem;
     CK((c->gen ? set_attrs_t<T, true>(max_smem) : set_attrs_t<T, false>(max_smem)));
+    g.stw = nullptr;
+    if (g.n0 == g.n1 && g.n1 == g.n2 && !std::getenv("LFTS_NO_FAST")) {
+        const int N = g.n0;
+        int ok = 0;
+        switch (N) {
+            case 16: ok = fast_setup<T, 16>(max_smem); break;
+            case 32: ok = fast_setup<T, 32>(max_smem); break;
+            case 48: ok = fast_setup<T, 48>(max_smem); break;
+            case 64: ok = fast_setup<T, 64>(max_smem); break;
+            case 96: ok = fast_setup<T, 96>(max_smem); break;
+            case 128: ok = fast_setup<T, 128>(max_smem); break;
+            default: ok = 0;
+        }
+        if (ok) {
+            // per-stage twiddles w_L^(j k1), stage s (innermost first) at stw_offset, [j-1][k1]
+            const int nf = fast::nrad(N);
+            std::vector<C> h(fast::stw_size(N) + 1);
+            for (int st = 0; st < nf; st++) {
+                const int R = fast::rad(N, nf - 1 - st), M = fast::span_inner(N, st), L = M * R;
+                const int off = fast::stw_offset(N, st);
+                for (int j = 1; j < R; j++)
+                    for (int k1 = 0; k1 < M; k1++) {
+                        const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)(j * k1) / (long double)L;
+                        h[off + (j - 1) * M + k1].x = (T)std::cos(a);
+                        h[off + (j - 1) * M + k1].y = (T)std::sin(a);
+                    }
+            }
+            CK(cudaMalloc(&c->stw, sizeof(C) * h.size()));
+            CK(cudaMemcpy(c->stw, h.data(), sizeof(C) * h.size(), cudaMemcpyHostToDevice));
+            g.stw = c->stw;
+            c->fastN = N;
+        }
+    }
     return 0;
 }
 
@@ -213,6 +270,7 @@ extern "C" int lfts_ctx_destroy(lfts_ctx c) {
     if (!c) return 0;
     cudaSetDevice(c->device);
     if (c->tables) cudaFree(c->tables);
+    if (c->stw) cudaFree(c->stw);
     if (c->partials) cudaFree(c->partials);
     if (c->sjobs) cudaFree(c->sjobs);
     if (c->sjobs_host) cudaFreeHost(c->sjobs_host);
@@ -390,27 +448,73 @@ extern "C" int lfts_field_factors(lfts_ctx c, const double *w, double coef, void
 }
 
 // ---------------------------------------------------------------- steps
+template <typename T, int N>
+static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) {
+    using C = typename CT<T>::type;
+    const GridPlan &g = c->g;
+    cudaStream_t st = c->stream;
+    constexpr int TJ = sizeof(T) == 8 ? 16 : 32;
+    const dim3 gp(N, nj), gx((unsigned)(((long long)N * (N / 2 + 1) + TJ - 1) / TJ), nj);
+    const size_t f2 = fast::FSmem<C, N, 2, 1>::BYTES, f1 = fast::FSmem<C, N, 1, 1>::BYTES;
+    const size_t x2 = sizeof(C) * (2 * (size_t)N * TJ + fast::stw_size(N) + 1);
+    const size_t x1 = sizeof(C) * ((size_t)N * TJ + fast::stw_size(N) + 1);
+    fast::kf_plane_forward<T, 2, N><<<gp, NTHR, f2, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0);
+    fast::kf_xpass<T, 2, N><<<gx, NTHR, x2, st>>>(g, jobs, 0, 0, 1);
+    fast::kf_plane_mid<T, N><<<gp, NTHR, f1, st>>>(g, jobs, 1);
+    fast::kf_xpass<T, 1, N><<<gx, NTHR, x1, st>>>(g, jobs, 1, 1, 1);
+    fast::kf_plane_inverse<T, 2, EPI_RICH, N><<<gp, NTHR, f2, st>>>(g, jobs, s, 0, 0);
+    CKLAUNCH();
+    return 0;
+}
+template <typename T, int N>
+static int step_disc_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, int half, int with_fac) {
+    using C = typename CT<T>::type;
+    const GridPlan &g = c->g;
+    cudaStream_t st = c->stream;
+    constexpr int TJ = sizeof(T) == 8 ? 16 : 32;
+    const dim3 gp(N, nj), gx((unsigned)(((long long)N * (N / 2 + 1) + TJ - 1) / TJ), nj);
+    const size_t f1 = fast::FSmem<C, N, 1, 1>::BYTES;
+    const size_t x1 = sizeof(C) * ((size_t)N * TJ + fast::stw_size(N) + 1);
+    fast::kf_plane_forward<T, 1, N><<<gp, NTHR, f1, st>>>(g, jobs, s, FM_NONE, 0, 0);
+    fast::kf_xpass<T, 1, N><<<gx, NTHR, x1, st>>>(g, jobs, 0, half, half);
+    fast::kf_plane_inverse<T, 1, EPI_SCALE, N><<<gp, NTHR, f1, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
+    CKLAUNCH();
+    return 0;
+}
+template <typename T>
+static int step_fast_dispatch(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, int disc, int half, int wf) {
+    switch (c->fastN) {
+        case 16: return disc ? step_disc_fast<T, 16>(c, jobs, nj, s, half, wf) : step_cont_fast<T, 16>(c, jobs, nj, s);
+        case 32: return disc ? step_disc_fast<T, 32>(c, jobs, nj, s, half, wf) : step_cont_fast<T, 32>(c, jobs, nj, s);
+        case 48: return disc ? step_disc_fast<T, 48>(c, jobs, nj, s, half, wf) : step_cont_fast<T, 48>(c, jobs, nj, s);
+        case 64: return disc ? step_disc_fast<T, 64>(c, jobs, nj, s, half, wf) : step_cont_fast<T, 64>(c, jobs, nj, s);
+        case 96: return disc ? step_disc_fast<T, 96>(c, jobs, nj, s, half, wf) : step_cont_fast<T, 96>(c, jobs, nj, s);
+        case 128: return disc ? step_disc_fast<T, 128>(c, jobs, nj, s, half, wf) : step_cont_fast<T, 128>(c, jobs, nj, s);
+    }
+    return fail("no specialised kernels for this grid");
+}
+
 template <typename T, bool GEN>
 static int step_cont_t(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) {
     const GridPlan &g = c->g;
     cudaStream_t st = c->stream;
     const dim3 gp(g.n0, nj), gx(c->ntiles, nj);
     if (c->nbr2) {
-        k_plane_forward<T, 2, GEN><<<gp, NTHR, c->sm_pf2, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0);
+        k_plane_forward<T, 2, GEN><<<gp, NTHR, c->sm_pf2, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0, c->zb);
         k_xpass<T, 2, GEN><<<gx, NTHR, c->sm_x2, st>>>(g, jobs, 0, 0, 1, c->TJ);
     } else {
-        k_plane_forward<T, 1, GEN><<<gp, NTHR, c->sm_pf1, st>>>(g, jobs, s, FM_FAC_SQ, 0, 0);
-        k_plane_forward<T, 1, GEN><<<gp, NTHR, c->sm_pf1, st>>>(g, jobs, s, FM_FAC, 0, 1);
+        k_plane_forward<T, 1, GEN><<<gp, NTHR, c->sm_pf1, st>>>(g, jobs, s, FM_FAC_SQ, 0, 0, c->zb);
+        k_plane_forward<T, 1, GEN><<<gp, NTHR, c->sm_pf1, st>>>(g, jobs, s, FM_FAC, 0, 1, c->zb);
         k_xpass<T, 1, GEN><<<gx, NTHR, c->sm_x1, st>>>(g, jobs, 0, 0, 0, c->TJ);
         k_xpass<T, 1, GEN><<<gx, NTHR, c->sm_x1, st>>>(g, jobs, 1, 1, 1, c->TJ);
     }
-    k_plane_mid<T, GEN><<<gp, NTHR, c->sm_mid, st>>>(g, jobs, 1);
+    k_plane_mid<T, GEN><<<gp, NTHR, c->sm_mid, st>>>(g, jobs, 1, c->zb);
     k_xpass<T, 1, GEN><<<gx, NTHR, c->sm_x1, st>>>(g, jobs, 1, 1, 1, c->TJ);
     if (c->nbr2) {
-        k_plane_inverse<T, 2, EPI_RICH, GEN><<<gp, NTHR, c->sm_inv2, st>>>(g, jobs, s, 0, 0);
+        k_plane_inverse<T, 2, EPI_RICH, GEN><<<gp, NTHR, c->sm_inv2, st>>>(g, jobs, s, 0, 0, c->zb);
     } else {
-        k_plane_inverse<T, 1, EPI_SCALE, GEN><<<gp, NTHR, c->sm_inv1, st>>>(g, jobs, s, 0, FM_FAC_SQ);
-        k_plane_inverse<T, 1, EPI_RICH_ACC, GEN><<<gp, NTHR, c->sm_inv1, st>>>(g, jobs, s, 1, 0);
+        k_plane_inverse<T, 1, EPI_SCALE, GEN><<<gp, NTHR, c->sm_inv1, st>>>(g, jobs, s, 0, FM_FAC_SQ, c->zb);
+        k_plane_inverse<T, 1, EPI_RICH_ACC, GEN><<<gp, NTHR, c->sm_inv1, st>>>(g, jobs, s, 1, 0, c->zb);
     }
     CKLAUNCH();
     return 0;
@@ -419,6 +523,10 @@ extern "C" int lfts_step_continuous(lfts_ctx c, const lfts_step_job *jobs, int n
     if (!c || !jobs) return fail("null argument");
     if (nj <= 0) return 0;
     if (nj > 65535) return fail("too many jobs in one launch (max 65535)");
+    if (c->fastN) {
+        c->launches += 5;
+        return c->prec == 8 ? step_fast_dispatch<double>(c, jobs, nj, s, 0, 0, 0) : step_fast_dispatch<float>(c, jobs, nj, s, 0, 0, 0);
+    }
     c->launches += c->nbr2 ? 5 : 8;
     if (c->prec == 8) return c->gen ? step_cont_t<double, true>(c, jobs, nj, s) : step_cont_t<double, false>(c, jobs, nj, s);
     return c->gen ? step_cont_t<float, true>(c, jobs, nj, s) : step_cont_t<float, false>(c, jobs, nj, s);
@@ -429,9 +537,9 @@ static int step_disc_t(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, int
     const GridPlan &g = c->g;
     cudaStream_t st = c->stream;
     const dim3 gp(g.n0, nj), gx(c->ntiles, nj);
-    k_plane_forward<T, 1, GEN><<<gp, NTHR, c->sm_pf1, st>>>(g, jobs, s, FM_NONE, 0, 0);
+    k_plane_forward<T, 1, GEN><<<gp, NTHR, c->sm_pf1, st>>>(g, jobs, s, FM_NONE, 0, 0, c->zb);
     k_xpass<T, 1, GEN><<<gx, NTHR, c->sm_x1, st>>>(g, jobs, 0, half, half, c->TJ);
-    k_plane_inverse<T, 1, EPI_SCALE, GEN><<<gp, NTHR, c->sm_inv1, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
+    k_plane_inverse<T, 1, EPI_SCALE, GEN><<<gp, NTHR, c->sm_inv1, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE, c->zb);
     CKLAUNCH();
     return 0;
 }
@@ -441,6 +549,9 @@ extern "C" int lfts_step_discrete(lfts_ctx c, const lfts_step_job *jobs, int nj,
     if (nj > 65535) return fail("too many jobs in one launch (max 65535)");
     half = half ? 1 : 0;
     c->launches += 3;
+    if (c->fastN)
+        return c->prec == 8 ? step_fast_dispatch<double>(c, jobs, nj, s, 1, half, with_fac)
+                            : step_fast_dispatch<float>(c, jobs, nj, s, 1, half, with_fac);
     if (c->prec == 8)
         return c->gen ? step_disc_t<double, true>(c, jobs, nj, s, half, with_fac) : step_disc_t<double, false>(c, jobs, nj, s, half, with_fac);
     return c->gen ? step_disc_t<float, true>(c, jobs, nj, s, half, with_fac) : step_disc_t<float, false>(c, jobs, nj, s, half, with_fac);
@@ -654,7 +765,7 @@ static int stress_t(lfts_ctx c, const lfts_stress_job *jobs, int nj, const doubl
         if (2 * n > c->sjobs_cap) return fail("stress chunk too large");
         if ((size_t)n * c->ntiles * 3 > c->partials_cap) return fail("stress chunk exceeds the partial-sum workspace");
         k_stress_prep<T><<<(n + 127) / 128, 128, 0, st>>>(jobs + j0, n, spec, g.Mc, c->sjobs);
-        k_plane_forward<T, 1, GEN><<<dim3(g.n0, 2 * n), NTHR, c->sm_pf1, st>>>(g, c->sjobs, 0, FM_NONE, 0, 0);
+        k_plane_forward<T, 1, GEN><<<dim3(g.n0, 2 * n), NTHR, c->sm_pf1, st>>>(g, c->sjobs, 0, FM_NONE, 0, 0, c->zb);
         k_xstress<T, GEN><<<dim3(c->ntiles, n), NTHR, smx, st>>>(g, c->sjobs, jobs + j0, basis, c->TJ, c->partials);
         k_finish<<<dim3(n, 3), NTHR, 0, st>>>(c->partials, c->ntiles, (const double *)&jobs[j0].weight,
                                              (int)sizeof(lfts_stress_job), 1.0, out + 3 * (long long)j0, 3, 3);

@@ -31,21 +31,23 @@ __device__ __forceinline__ T fac_value(int mode, const T *fac, long long idx) {
 }
 
 // shared-memory layout shared by the plane kernels
+// Each warp transforms zb z-lines at a time (zl: zb lines of n2 per warp), so
+// all 32 lanes have butterflies even when one line has only n2/8 of them.
 template <typename C>
 struct PlaneSmem {
     C *P, *zl, *zl2, *twy, *twz;
     short *py, *pz;
-    __device__ PlaneSmem(unsigned char *raw, int nbr, int n1, int n2, int nzc, bool two_lines) {
+    __device__ PlaneSmem(unsigned char *raw, int nbr, int n1, int n2, int nzc, bool two_lines, int zb) {
         P = (C *)raw;
         zl = P + nbr * n1 * nzc;
-        zl2 = zl + NWARP * n2;
-        twy = zl2 + (two_lines ? NWARP * n2 : 0);
+        zl2 = zl + NWARP * zb * n2;
+        twy = zl2 + (two_lines ? NWARP * zb * n2 : 0);
         twz = twy + n1;
         py = (short *)(twz + n2);
         pz = py + n1;
     }
-    static size_t bytes(int nbr, int n1, int n2, int nzc, bool two_lines) {
-        return sizeof(C) * ((size_t)nbr * n1 * nzc + (size_t)NWARP * n2 * (two_lines ? 2 : 1) + n1 + n2) +
+    static size_t bytes(int nbr, int n1, int n2, int nzc, bool two_lines, int zb) {
+        return sizeof(C) * ((size_t)nbr * n1 * nzc + (size_t)NWARP * zb * n2 * (two_lines ? 2 : 1) + n1 + n2) +
                sizeof(short) * (n1 + n2);
     }
 };
@@ -89,11 +91,11 @@ __device__ __forceinline__ C pack_pair(const C *rowA, const C *rowB, int k, int 
 // (factors fm0, fm1), z-work unit = one row.  NBR=1: z-work unit = row pair.
 template <typename T, int NBR, bool GEN>
 __global__ void __launch_bounds__(NTHR) k_plane_forward(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
-                                                        int fm0, int fm1, int spec_out0) {
+                                                        int fm0, int fm1, int spec_out0, int zb) {
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n1 = g.n1, n2 = g.n2, nzc = g.nzc;
-    PlaneSmem<C> sm(smem_raw, NBR, n1, n2, nzc, false);
+    PlaneSmem<C> sm(smem_raw, NBR, n1, n2, nzc, false, zb);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x;
@@ -105,38 +107,49 @@ __global__ void __launch_bounds__(NTHR) k_plane_forward(GridPlan g, const lfts_s
     const T *qin = (const T *)jb.in + s * jb.in_stride + poff;
     const T *fac = (const T *)jb.fac;
     const int nunits = (NBR == 2) ? n1 : (n1 + 1) / 2;
-    C *zw = sm.zl + warp * n2;
-    const LineMap lmz = {1, 1, 0, 1};
-    for (int u = warp; u < nunits; u += NWARP) {
-        const int ya = (NBR == 2) ? u : 2 * u;
-        const int yb = (NBR == 2) ? u : 2 * u + 1;
-        const bool hasb = (NBR == 2) || (yb < n1);
-        for (int t = lane; t < n2; t += 32) {
-            const long long ia = poff + (long long)ya * n2 + t;
-            const T qa = qin[ya * n2 + t];
-            T va, vb;
-            if (NBR == 2) {
-                va = qa * fac_value(fm0, fac, ia);
-                vb = qa * fac_value(fm1, fac, ia);
-            } else {
-                va = qa * fac_value(fm0, fac, ia);
-                vb = hasb ? qin[yb * n2 + t] * fac_value(fm0, fac, ia + n2) : (T)0;
+    C *zw = sm.zl + warp * zb * n2;
+    for (int u0 = warp * zb; u0 < nunits; u0 += NWARP * zb) {
+        const int nb = min(zb, nunits - u0);
+        for (int b = 0; b < nb; b++) {
+            const int u = u0 + b;
+            const int ya = (NBR == 2) ? u : 2 * u;
+            const int yb = (NBR == 2) ? u : 2 * u + 1;
+            const bool hasb = (NBR == 2) || (yb < n1);
+            for (int t = lane; t < n2; t += 32) {
+                const long long ia = poff + (long long)ya * n2 + t;
+                const T qa = qin[ya * n2 + t];
+                T va, vb;
+                if (NBR == 2) {
+                    va = qa * fac_value(fm0, fac, ia);
+                    vb = qa * fac_value(fm1, fac, ia);
+                } else {
+                    va = qa * fac_value(fm0, fac, ia);
+                    vb = hasb ? qin[yb * n2 + t] * fac_value(fm0, fac, ia + n2) : (T)0;
+                }
+                C z;
+                z.x = va;
+                z.y = vb;
+                zw[b * n2 + sm.pz[t]] = z;
             }
-            C z;
-            z.x = va;
-            z.y = vb;
-            zw[sm.pz[t]] = z;
         }
         __syncwarp();
+        const LineMap lmz = {nb, 1, n2, 1};
         dit_lines<C, false, GEN>(zw, lmz, g.ax[2], sm.twz, -1, lane, 32);
-        const int pa = 0, pb = (NBR == 2) ? 1 : 0;
-        C *rowA = sm.P + (size_t)pa * n1 * nzc + (size_t)sm.py[ya] * nzc;
-        C *rowB = sm.P + (size_t)pb * n1 * nzc + (size_t)sm.py[yb < n1 ? yb : ya] * nzc;
-        for (int k = lane; k < nzc; k += 32) {
-            C A, B;
-            split_pair(zw[k], cconj(zw[k == 0 ? 0 : n2 - k]), A, B);
-            rowA[k] = A;
-            if (hasb) rowB[k] = B;
+        for (int b = 0; b < nb; b++) {
+            const int u = u0 + b;
+            const int ya = (NBR == 2) ? u : 2 * u;
+            const int yb = (NBR == 2) ? u : 2 * u + 1;
+            const bool hasb = (NBR == 2) || (yb < n1);
+            const int pb = (NBR == 2) ? 1 : 0;
+            C *rowA = sm.P + (size_t)sm.py[ya] * nzc;
+            C *rowB = sm.P + (size_t)pb * n1 * nzc + (size_t)sm.py[yb < n1 ? yb : ya] * nzc;
+            const C *z = zw + b * n2;
+            for (int k = lane; k < nzc; k += 32) {
+                C A, B;
+                split_pair(z[k], cconj(z[k == 0 ? 0 : n2 - k]), A, B);
+                rowA[k] = A;
+                if (hasb) rowB[k] = B;
+            }
         }
         __syncwarp();
     }
@@ -220,11 +233,12 @@ __device__ __forceinline__ void load_and_inverse_y(const GridPlan &g, const lfts
 // K3: half-step seam of the continuous step: inverse zy, multiply by
 // e = fac^2 (exp(-w ds/4)^2 = exp(-w ds/2)), forward zy, in place on spec slot.
 template <typename T, bool GEN>
-__global__ void __launch_bounds__(NTHR) k_plane_mid(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_idx) {
+__global__ void __launch_bounds__(NTHR) k_plane_mid(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_idx,
+                                                    int zb) {
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n1 = g.n1, n2 = g.n2, nzc = g.nzc;
-    PlaneSmem<C> sm(smem_raw, 1, n1, n2, nzc, true);
+    PlaneSmem<C> sm(smem_raw, 1, n1, n2, nzc, true, zb);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x;
@@ -235,32 +249,45 @@ __global__ void __launch_bounds__(NTHR) k_plane_mid(GridPlan g, const lfts_step_
     __syncthreads();
     const T *fac = (const T *)jb.fac;
     const long long poff = (long long)x * n1 * n2;
-    C *zw = sm.zl + warp * n2;
-    C *zw2 = sm.zl2 + warp * n2;
-    const LineMap lmz = {1, 1, 0, 1};
+    C *zw = sm.zl + warp * zb * n2;
+    C *zw2 = sm.zl2 + warp * zb * n2;
     const int nunits = (n1 + 1) / 2;
-    for (int u = warp; u < nunits; u += NWARP) {
-        const int ya = 2 * u, yb = 2 * u + 1;
-        const bool hasb = yb < n1;
-        C *rowA = sm.P + (size_t)sm.py[ya] * nzc;
-        C *rowB = hasb ? sm.P + (size_t)sm.py[yb] * nzc : nullptr;
-        for (int k = lane; k < n2; k += 32) zw[sm.pz[k]] = pack_pair(rowA, rowB, k, n2, nzc);
+    for (int u0 = warp * zb; u0 < nunits; u0 += NWARP * zb) {
+        const int nb = min(zb, nunits - u0);
+        const LineMap lmz = {nb, 1, n2, 1};
+        for (int b = 0; b < nb; b++) {
+            const int ya = 2 * (u0 + b), yb = ya + 1;
+            const C *rowA = sm.P + (size_t)sm.py[ya] * nzc;
+            const C *rowB = yb < n1 ? sm.P + (size_t)sm.py[yb] * nzc : nullptr;
+            for (int k = lane; k < n2; k += 32) zw[b * n2 + sm.pz[k]] = pack_pair(rowA, rowB, k, n2, nzc);
+        }
         __syncwarp();
         dit_lines<C, false, GEN>(zw, lmz, g.ax[2], sm.twz, +1, lane, 32);
-        for (int t = lane; t < n2; t += 32) {
-            const C z = zw[t];
-            C v;
-            v.x = z.x * fac_value(FM_FAC_SQ, fac, poff + (long long)ya * n2 + t);
-            v.y = hasb ? z.y * fac_value(FM_FAC_SQ, fac, poff + (long long)yb * n2 + t) : (T)0;
-            zw2[sm.pz[t]] = v;
+        for (int b = 0; b < nb; b++) {
+            const int ya = 2 * (u0 + b), yb = ya + 1;
+            const bool hasb = yb < n1;
+            for (int t = lane; t < n2; t += 32) {
+                const C z = zw[b * n2 + t];
+                C v;
+                v.x = z.x * fac_value(FM_FAC_SQ, fac, poff + (long long)ya * n2 + t);
+                v.y = hasb ? z.y * fac_value(FM_FAC_SQ, fac, poff + (long long)yb * n2 + t) : (T)0;
+                zw2[b * n2 + sm.pz[t]] = v;
+            }
         }
         __syncwarp();
         dit_lines<C, false, GEN>(zw2, lmz, g.ax[2], sm.twz, -1, lane, 32);
-        for (int k = lane; k < nzc; k += 32) {
-            C A, B;
-            split_pair(zw2[k], cconj(zw2[k == 0 ? 0 : n2 - k]), A, B);
-            rowA[k] = A;
-            if (hasb) rowB[k] = B;
+        for (int b = 0; b < nb; b++) {
+            const int ya = 2 * (u0 + b), yb = ya + 1;
+            const bool hasb = yb < n1;
+            C *rowA = sm.P + (size_t)sm.py[ya] * nzc;
+            C *rowB = hasb ? sm.P + (size_t)sm.py[yb] * nzc : nullptr;
+            const C *z = zw2 + b * n2;
+            for (int k = lane; k < nzc; k += 32) {
+                C A, B;
+                split_pair(z[k], cconj(z[k == 0 ? 0 : n2 - k]), A, B);
+                rowA[k] = A;
+                if (hasb) rowB[k] = B;
+            }
         }
         __syncwarp();
     }
@@ -281,11 +308,11 @@ enum { EPI_SCALE = 0, EPI_RICH = 1, EPI_RICH_ACC = 2 };
 
 template <typename T, int NBR, int EPI, bool GEN>
 __global__ void __launch_bounds__(NTHR) k_plane_inverse(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
-                                                        int spec_in0, int fm0) {
+                                                        int spec_in0, int fm0, int zb) {
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n1 = g.n1, n2 = g.n2, nzc = g.nzc;
-    PlaneSmem<C> sm(smem_raw, NBR, n1, n2, nzc, false);
+    PlaneSmem<C> sm(smem_raw, NBR, n1, n2, nzc, false, zb);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x;
@@ -297,35 +324,45 @@ __global__ void __launch_bounds__(NTHR) k_plane_inverse(GridPlan g, const lfts_s
     const T *fac = (const T *)jb.fac;
     const long long poff = (long long)x * n1 * n2;
     T *qout = (T *)jb.out + s * jb.out_stride + poff;
-    C *zw = sm.zl + warp * n2;
-    const LineMap lmz = {1, 1, 0, 1};
+    C *zw = sm.zl + warp * zb * n2;
     const int nunits = (NBR == 2) ? n1 : (n1 + 1) / 2;
-    for (int u = warp; u < nunits; u += NWARP) {
-        const int ya = (NBR == 2) ? u : 2 * u;
-        const int yb = (NBR == 2) ? u : 2 * u + 1;
-        const bool hasb = (NBR == 2) || (yb < n1);
-        const C *rowA = sm.P + (size_t)sm.py[ya] * nzc;
-        const C *rowB = (NBR == 2) ? sm.P + (size_t)n1 * nzc + (size_t)sm.py[ya] * nzc
-                                   : (hasb ? sm.P + (size_t)sm.py[yb] * nzc : nullptr);
-        for (int k = lane; k < n2; k += 32) zw[sm.pz[k]] = pack_pair(rowA, rowB, k, n2, nzc);
+    for (int u0 = warp * zb; u0 < nunits; u0 += NWARP * zb) {
+        const int nb = min(zb, nunits - u0);
+        for (int b = 0; b < nb; b++) {
+            const int u = u0 + b;
+            const int ya = (NBR == 2) ? u : 2 * u;
+            const int yb = (NBR == 2) ? u : 2 * u + 1;
+            const bool hasb = (NBR == 2) || (yb < n1);
+            const C *rowA = sm.P + (size_t)sm.py[ya] * nzc;
+            const C *rowB = (NBR == 2) ? sm.P + (size_t)n1 * nzc + (size_t)sm.py[ya] * nzc
+                                       : (hasb ? sm.P + (size_t)sm.py[yb] * nzc : nullptr);
+            for (int k = lane; k < n2; k += 32) zw[b * n2 + sm.pz[k]] = pack_pair(rowA, rowB, k, n2, nzc);
+        }
         __syncwarp();
+        const LineMap lmz = {nb, 1, n2, 1};
         dit_lines<C, false, GEN>(zw, lmz, g.ax[2], sm.twz, +1, lane, 32);
-        for (int t = lane; t < n2; t += 32) {
-            const C z = zw[t];
-            const long long ia = poff + (long long)ya * n2 + t;
-            if (EPI == EPI_RICH) {
-                const T eh = fac[ia];
-                qout[ya * n2 + t] = ((T)4 * eh * z.y - eh * eh * z.x) / (T)3;
-            } else if (EPI == EPI_RICH_ACC) {
-                const T eh = fac[ia];
-                qout[ya * n2 + t] = ((T)4 * eh * z.x - qout[ya * n2 + t]) / (T)3;
-                if (hasb) {
-                    const T ehb = fac[ia + n2];
-                    qout[yb * n2 + t] = ((T)4 * ehb * z.y - qout[yb * n2 + t]) / (T)3;
+        for (int b = 0; b < nb; b++) {
+            const int u = u0 + b;
+            const int ya = (NBR == 2) ? u : 2 * u;
+            const int yb = (NBR == 2) ? u : 2 * u + 1;
+            const bool hasb = (NBR == 2) || (yb < n1);
+            for (int t = lane; t < n2; t += 32) {
+                const C z = zw[b * n2 + t];
+                const long long ia = poff + (long long)ya * n2 + t;
+                if (EPI == EPI_RICH) {
+                    const T eh = fac[ia];
+                    qout[ya * n2 + t] = ((T)4 * eh * z.y - eh * eh * z.x) / (T)3;
+                } else if (EPI == EPI_RICH_ACC) {
+                    const T eh = fac[ia];
+                    qout[ya * n2 + t] = ((T)4 * eh * z.x - qout[ya * n2 + t]) / (T)3;
+                    if (hasb) {
+                        const T ehb = fac[ia + n2];
+                        qout[yb * n2 + t] = ((T)4 * ehb * z.y - qout[yb * n2 + t]) / (T)3;
+                    }
+                } else {
+                    qout[ya * n2 + t] = z.x * fac_value(fm0, fac, ia);
+                    if (hasb) qout[yb * n2 + t] = z.y * fac_value(fm0, fac, ia + n2);
                 }
-            } else {
-                qout[ya * n2 + t] = z.x * fac_value(fm0, fac, ia);
-                if (hasb) qout[yb * n2 + t] = z.y * fac_value(fm0, fac, ia + n2);
             }
         }
         __syncwarp();

@@ -100,7 +100,9 @@ def mixture_molecules():
 
 
 def config_molecules():
-    """The molecules of the benchmark configurations."""
+    """Schedule fixtures: the benchmark diblocks (N 100 and 90, conformationally
+    asymmetric f 0.36), a discrete branched mixture, an ABA triblock blend and
+    a nine-arm star."""
     eps = 1.2
     f2 = 0.36
     bb = [["B", 5 / 60, i, i + 1] for i in range(8)] + [["A", 6 / 60, i, 8 + i] for i in range(1, 9)]

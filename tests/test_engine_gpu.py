@@ -13,7 +13,8 @@ pytestmark = pytest.mark.gpu
 
 GRIDS = [((5, 4, 3), (4.0, 3.0, 2.0)), ((8, 8, 8), (3.0, 3.0, 3.0)), ((32, 32, 32), (4.0, 4.0, 4.0)),
          ((23, 27, 25), (3.2, 3.3, 3.4)), ((64,), (5.0,)), ((16, 12), (3.0, 2.5)), ((48, 48, 48), (5.0, 5.0, 5.0)),
-         ((31, 49, 23), (4.0, 4.5, 3.5))]
+         ((31, 49, 23), (4.0, 4.5, 3.5)), ((16, 16, 16), (3.0, 3.0, 3.0)), ((64, 64, 64), (7.3, 7.3, 7.3)),
+         ((96, 96, 96), (8.0, 8.0, 8.0))]
 
 
 def _ctx(nx, prec=8):
