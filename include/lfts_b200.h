@@ -265,6 +265,29 @@ int lfts_am_batch_update(lfts_ctx ctx, int R, long long n, int L, const int *hea
                          const double *mix, const double *a, const double *w_cur, long long w_stride, const double *d_cur,
                          long long d_stride, const double *w_hist, const double *d_hist, double *w_out, long long out_stride);
 
+/* ---- allocation-free inner products (no reference counterpart) ----------
+ * lfts_dots_static computes what lfts_dots computes,
+ *   out[j] = scale_j * sum_{i<M} a_j[i] b_j[i] (/ w_j[i] if w_j != NULL),
+ * without a context and without allocating any device memory.  The reference
+ * has no such entry point: its inner products run through a computation box
+ * that owns allocated scratch.  It serves hosts that hold no lfts context and
+ * may not let a library allocate, e.g. a runtime that hands out all device
+ * memory from its own fixed pool.
+ * precision: 8 (a, b, w double) or 4 (float).  M > 0.  jobs: device array of
+ * njobs entries; out: device array of njobs doubles; stream: a cudaStream_t
+ * (NULL = the default stream).  Everything is enqueued on that stream.
+ * Scratch: one file-scope device array of LFTS_DOTS_STATIC_MAX_JOBS x 128
+ * doubles (256 KiB) per device.  njobs above LFTS_DOTS_STATIC_MAX_JOBS is
+ * rejected with an error.  Every call on a device shares that array, so calls
+ * that overlap in time (two streams, or two host threads, on one device) race
+ * and must be serialised by the caller.  Each call writes every scratch entry
+ * it reads, so nothing needs clearing between calls.
+ * The first call on each device looks up the array's address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. */
+#define LFTS_DOTS_STATIC_MAX_JOBS 256
+int lfts_dots_static(int precision, long long M, const lfts_dot_job *jobs, int njobs, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

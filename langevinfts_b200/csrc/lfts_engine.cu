@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -921,6 +922,54 @@ extern "C" int lfts_field_factors_batch(lfts_ctx c, const double *w, double coef
     else
         k_field_factors<float><<<grid_for(n), NTHR, 0, c->stream>>>(w, coef, (float *)fac_out, n);
     c->launches += 1;
+    CKLAUNCH();
+    return 0;
+}
+
+// ---------------------------------------------------------------- allocation-free inner products
+// The same two kernels as lfts_dots, with their partial sums in a file-scope
+// device array instead of context-owned memory.  Every call on a device shares
+// the array; k_dots writes all nj * DOT_CHUNKS entries that k_finish reads, so
+// no entry has to start at zero.
+static __device__ __align__(256) double g_dots_static_scratch[LFTS_DOTS_STATIC_MAX_JOBS * DOT_CHUNKS];
+constexpr int DOTS_STATIC_MAX_DEVICES = 64;
+static std::mutex g_dots_static_mu;
+static double *g_dots_static_ptr[DOTS_STATIC_MAX_DEVICES];
+
+// Address of the scratch array on the current device, looked up once per
+// device (with that device current) and cached.
+static int dots_static_scratch(double **out) {
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= DOTS_STATIC_MAX_DEVICES)
+        return fail("lfts_dots_static: device ordinal " + std::to_string(dev) + " out of range");
+    std::lock_guard<std::mutex> lock(g_dots_static_mu);
+    if (!g_dots_static_ptr[dev]) {
+        double *p = nullptr;
+        CK(cudaGetSymbolAddress((void **)&p, g_dots_static_scratch));
+        if (!p) return fail("lfts_dots_static: cudaGetSymbolAddress returned a null address");
+        g_dots_static_ptr[dev] = p;
+    }
+    *out = g_dots_static_ptr[dev];
+    return 0;
+}
+
+extern "C" int lfts_dots_static(int precision, long long M, const lfts_dot_job *jobs, int nj, double *out, void *stream) {
+    if (!jobs || !out) return fail("lfts_dots_static: null argument");
+    if (precision != 4 && precision != 8) return fail("lfts_dots_static: precision must be 4 or 8");
+    if (M <= 0) return fail("lfts_dots_static: M must be positive");
+    if (nj < 0 || nj > LFTS_DOTS_STATIC_MAX_JOBS)
+        return fail("lfts_dots_static: njobs = " + std::to_string(nj) + " is outside [0, " +
+                    std::to_string(LFTS_DOTS_STATIC_MAX_JOBS) + "], the size of the static scratch array");
+    if (nj == 0) return 0;
+    double *scratch = nullptr;
+    if (dots_static_scratch(&scratch)) return -1;
+    cudaStream_t st = (cudaStream_t)stream;
+    const dim3 grid(DOT_CHUNKS, nj);
+    if (precision == 8) k_dots<double><<<grid, NTHR, 0, st>>>(jobs, M, scratch);
+    else k_dots<float><<<grid, NTHR, 0, st>>>(jobs, M, scratch);
+    k_finish<<<dim3(nj, 1), NTHR, 0, st>>>(scratch, DOT_CHUNKS, (const double *)&jobs[0].scale, (int)sizeof(lfts_dot_job),
+                                           1.0, out, 1, 1);
     CKLAUNCH();
     return 0;
 }
