@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "lfts_step_fast.cuh"
+#include "lfts_step_r8.cuh"
 
 using namespace lfts;
 
@@ -43,6 +44,7 @@ struct lfts_ctx_s {
     bool gen = false, nbr2 = true;
     int TJ = 16, ntiles = 1, zb = 1;
     int fastN = 0;            // cubic grid handled by the compile-time specialised kernels (0: generic)
+    int r8 = 0;               // 64^3: register-resident 8x8 line transforms (lfts_step_r8.cuh)
     void *stw = nullptr;
     size_t sm_pf1 = 0, sm_pf2 = 0, sm_mid = 0, sm_inv1 = 0, sm_inv2 = 0, sm_x1 = 0, sm_x2 = 0;
     double *partials = nullptr;
@@ -139,6 +141,19 @@ template <typename T, int N> static int fast_setup(int max_smem) {
     return 1;
 }
 
+template <typename T> static int r8_setup(int max_smem) {
+    using C = typename CT<T>::type;
+    if (r8::plane_smem<C>() > (size_t)max_smem || r8::xpass_smem<C>() > (size_t)max_smem) return 0;
+    if (allow_smem(r8::kr_plane_forward<T, 1>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r8::kr_plane_forward<T, 2>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r8::kr_plane_mid<T>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r8::kr_plane_inverse<T, 2, EPI_RICH>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r8::kr_plane_inverse<T, 1, EPI_SCALE>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r8::kr_xpass<T, 1>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r8::kr_xpass<T, 2>, max_smem) != cudaSuccess) return 0;
+    return 1;
+}
+
 template <typename T> static int setup_plan(lfts_ctx c) {
     using C = typename CT<T>::type;
     GridPlan &g = c->g;
@@ -221,6 +236,7 @@ template <typename T> static int setup_plan(lfts_ctx c) {
             CK(cudaMemcpy(c->stw, h.data(), sizeof(C) * h.size(), cudaMemcpyHostToDevice));
             g.stw = c->stw;
             c->fastN = N;
+            if (N == 64 && !std::getenv("LFTS_NO_R8")) c->r8 = r8_setup<T>(max_smem);
         }
     }
     return 0;
@@ -459,6 +475,19 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
     const size_t f2 = fast::FSmem<C, N, 2, 1>::BYTES, f1 = fast::FSmem<C, N, 1, 1>::BYTES;
     const size_t x2 = sizeof(C) * (2 * (size_t)N * TJ + fast::stw_size(N) + 1);
     const size_t x1 = sizeof(C) * ((size_t)N * TJ + fast::stw_size(N) + 1);
+    if constexpr (N == r8::N) {
+        if (c->r8) {
+            const dim3 rp(N, nj), rx(r8::PLANE / r8::GROUPS, nj);
+            const size_t ps = r8::plane_smem<C>(), xs = r8::xpass_smem<C>();
+            r8::kr_plane_forward<T, 2><<<rp, NTHR, ps, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0);
+            r8::kr_xpass<T, 2><<<rx, NTHR, xs, st>>>(g, jobs, 0, 0, 1);
+            r8::kr_plane_mid<T><<<rp, NTHR, ps, st>>>(g, jobs, 1);
+            r8::kr_xpass<T, 1><<<rx, NTHR, xs, st>>>(g, jobs, 1, 1, 1);
+            r8::kr_plane_inverse<T, 2, EPI_RICH><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, 0);
+            CKLAUNCH();
+            return 0;
+        }
+    }
     fast::kf_plane_forward<T, 2, N><<<gp, NTHR, f2, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0);
     fast::kf_xpass<T, 2, N><<<gx, NTHR, x2, st>>>(g, jobs, 0, 0, 1);
     fast::kf_plane_mid<T, N><<<gp, NTHR, f1, st>>>(g, jobs, 1);
@@ -476,6 +505,17 @@ static int step_disc_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, 
     const dim3 gp(N, nj), gx((unsigned)(((long long)N * (N / 2 + 1) + TJ - 1) / TJ), nj);
     const size_t f1 = fast::FSmem<C, N, 1, 1>::BYTES;
     const size_t x1 = sizeof(C) * ((size_t)N * TJ + fast::stw_size(N) + 1);
+    if constexpr (N == r8::N) {
+        if (c->r8) {
+            const dim3 rp(N, nj), rx(r8::PLANE / r8::GROUPS, nj);
+            const size_t ps = r8::plane_smem<C>(), xs = r8::xpass_smem<C>();
+            r8::kr_plane_forward<T, 1><<<rp, NTHR, ps, st>>>(g, jobs, s, FM_NONE, 0, 0);
+            r8::kr_xpass<T, 1><<<rx, NTHR, xs, st>>>(g, jobs, 0, half, half);
+            r8::kr_plane_inverse<T, 1, EPI_SCALE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
+            CKLAUNCH();
+            return 0;
+        }
+    }
     fast::kf_plane_forward<T, 1, N><<<gp, NTHR, f1, st>>>(g, jobs, s, FM_NONE, 0, 0);
     fast::kf_xpass<T, 1, N><<<gx, NTHR, x1, st>>>(g, jobs, 0, half, half);
     fast::kf_plane_inverse<T, 1, EPI_SCALE, N><<<gp, NTHR, f1, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);

@@ -83,12 +83,13 @@ def test_step_continuous(nx, lx, prec):
     ctx.close()
 
 
-@pytest.mark.parametrize("nx,lx", GRIDS[:4] + GRIDS[5:6])
+@pytest.mark.parametrize("nx,lx,prec", [(n, l, 8) for n, l in GRIDS[:4] + GRIDS[5:6] + GRIDS[9:10]] +
+                         [(n, l, 4) for n, l in GRIDS[2:3] + GRIDS[9:10]])
 @pytest.mark.parametrize("half,with_fac", [(0, 1), (1, 0), (1, 1)])
-def test_step_discrete(nx, lx, half, with_fac):
+def test_step_discrete(nx, lx, prec, half, with_fac):
     from langevinfts_b200.capi import StepJob, check
-    dt = np.dtype(np.float64)
-    ctx = _ctx(nx)
+    dt = np.dtype(np.float64 if prec == 8 else np.float32)
+    ctx = _ctx(nx, prec)
     M = ctx.M
     rng = np.random.default_rng(3)
     ds, b2 = 1 / 20, 0.8
@@ -97,19 +98,19 @@ def test_step_discrete(nx, lx, half, with_fac):
     q0 = 1.0 + 0.3 * rng.random(M)
     bond, bondh = _tables(ctx, nx, lx, b2, ds, dt)
     wd = ctx.upload(w)
-    fac = ctx.malloc(M * 8)
+    fac = ctx.malloc(M * dt.itemsize)
     check(ctx.lib.lfts_field_factors(ctx.h, wd, -ds, fac))
-    q = ctx.upload(q0)
-    out = ctx.malloc(M * 8)
-    spec = ctx.malloc(2 * ctx.Mc * 16)
+    q = ctx.upload(q0.astype(dt))
+    out = ctx.malloc(M * dt.itemsize)
+    spec = ctx.malloc(2 * ctx.Mc * 2 * dt.itemsize)
     jp = _jobs(ctx, [StepJob(q, 0, out, 0, fac, bond, bondh, spec)])
     check(ctx.lib.lfts_step_discrete(ctx.h, jp, 1, 0, half, with_fac))
-    got = ctx.d2h(out, (M,), np.float64)
+    got = ctx.d2h(out, (M,), dt).astype(float)
     b = orc.boltz_bond(nx, lx, b2 / 2 if half else b2, ds)
     ref = orc.half_bond_step(g, q0, b)
     if with_fac:
         ref = ref * np.exp(-w * ds)
-    assert _rel(got, ref) < 1e-12
+    assert _rel(got, ref) < (1e-12 if prec == 8 else 2e-5)
     ctx.close()
 
 
