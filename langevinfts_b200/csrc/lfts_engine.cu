@@ -13,6 +13,7 @@
 
 #include "lfts_step_fast.cuh"
 #include "lfts_step_r8.cuh"
+#include "lfts_step_bulk.cuh"
 
 using namespace lfts;
 
@@ -44,7 +45,8 @@ struct lfts_ctx_s {
     bool gen = false, nbr2 = true;
     int TJ = 16, ntiles = 1, zb = 1;
     int fastN = 0;            // cubic grid handled by the compile-time specialised kernels (0: generic)
-    int r8 = 0;               // 64^3: register-resident 8x8 line transforms (lfts_step_r8.cuh)
+    int r8 = 0;               // 64^3: 1 register-resident 8x8 line transforms, 2 the same with bulk-copy staging
+    int nsm = 0;              // streaming multiprocessors of the device
     void *stw = nullptr;
     size_t sm_pf1 = 0, sm_pf2 = 0, sm_mid = 0, sm_inv1 = 0, sm_inv2 = 0, sm_x1 = 0, sm_x2 = 0;
     double *partials = nullptr;
@@ -151,7 +153,17 @@ template <typename T> static int r8_setup(int max_smem) {
     if (allow_smem(r8::kr_plane_inverse<T, 1, EPI_SCALE>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r8::kr_xpass<T, 1>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r8::kr_xpass<T, 2>, max_smem) != cudaSuccess) return 0;
-    return 1;
+    if (allow_smem(r8::kb_xpass<T, 1>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r8::kb_xpass<T, 2>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r8::kp_xpass<T, 1>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r8::kp_xpass<T, 2>, max_smem) != cudaSuccess) return 0;
+    if (!std::getenv("LFTS_BULK_PLANES") || r8::kb_plane_smem<C>(true) > (size_t)max_smem) return 1;
+    if (allow_smem(r8::kb_plane_forward<T, 1>, max_smem) != cudaSuccess) return 1;
+    if (allow_smem(r8::kb_plane_forward<T, 2>, max_smem) != cudaSuccess) return 1;
+    if (allow_smem(r8::kb_plane_mid<T>, max_smem) != cudaSuccess) return 1;
+    if (allow_smem(r8::kb_plane_inverse<T, 2, EPI_RICH>, max_smem) != cudaSuccess) return 1;
+    if (allow_smem(r8::kb_plane_inverse<T, 1, EPI_SCALE>, max_smem) != cudaSuccess) return 1;
+    return 2;
 }
 
 template <typename T> static int setup_plan(lfts_ctx c) {
@@ -187,6 +199,7 @@ template <typename T> static int setup_plan(lfts_ctx c) {
 
     int max_smem = 0;
     CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device));
     max_smem -= 64;  // headroom for static shared memory of the reduction kernels
     c->TJ = (sizeof(T) == 8) ? 16 : 32;
     c->ntiles = (int)((g.n1 * (long long)g.nzc + c->TJ - 1) / c->TJ);
@@ -330,10 +343,24 @@ extern "C" int lfts_memcpy_h2d(lfts_ctx c, void *dst, const void *src, size_t by
     CK(cudaStreamSynchronize(c->stream));
     return 0;
 }
+// Read and clear the device error word that kernels set instead of spinning
+// forever or touching a misaligned copy (called after a stream synchronisation).
+static int check_kernel_errors() {
+    unsigned int e = 0;
+    CK(cudaMemcpyFromSymbol(&e, g_kerr, sizeof e));
+    if (!e) return 0;
+    const unsigned int z = 0;
+    CK(cudaMemcpyToSymbol(g_kerr, &z, sizeof z));
+    std::string what;
+    if (e & KERR_WAIT_TIMEOUT) what += " a kernel's wait for its bulk copies timed out;";
+    if (e & KERR_MISALIGNED) what += " a spectrum buffer is not 16-byte aligned;";
+    return fail("device error word " + std::to_string(e) + ":" + what + " results of the affected launch are invalid");
+}
+
 extern "C" int lfts_memcpy_d2h(lfts_ctx c, void *dst, const void *src, size_t bytes) {
     CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    return 0;
+    return check_kernel_errors();
 }
 extern "C" int lfts_memcpy_d2d_async(lfts_ctx c, void *dst, const void *src, size_t bytes) {
     CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
@@ -342,7 +369,7 @@ extern "C" int lfts_memcpy_d2d_async(lfts_ctx c, void *dst, const void *src, siz
 extern "C" int lfts_synchronize(lfts_ctx c) {
     CK(cudaStreamSynchronize(c->stream));
     CK(cudaGetLastError());
-    return 0;
+    return check_kernel_errors();
 }
 
 extern "C" int lfts_graph_begin(lfts_ctx c) {
@@ -478,11 +505,24 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
     if constexpr (N == r8::N) {
         if (c->r8) {
             const dim3 rp(N, nj), rx(r8::PLANE / r8::GROUPS, nj);
-            const size_t ps = r8::plane_smem<C>(), xs = r8::xpass_smem<C>();
+            const size_t ps = r8::plane_smem<C>();
+            const dim3 bx(r8::PLANE / r8::XT, nj);
+            if (c->r8 == 2) {
+                const size_t p1 = r8::kb_plane_smem<C>(false), p2 = r8::kb_plane_smem<C>(true);
+                r8::kb_plane_forward<T, 2><<<rp, NTHR, p1, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0);
+                r8::kb_xpass<T, 2><<<bx, NTHR, r8::xbulk_smem<C, 2>(), st>>>(g, jobs, 0, 0, 1);
+                r8::kb_plane_mid<T><<<rp, NTHR, p1, st>>>(g, jobs, 1);
+                r8::kb_xpass<T, 1><<<bx, NTHR, r8::xbulk_smem<C, 1>(), st>>>(g, jobs, 1, 1, 1);
+                r8::kb_plane_inverse<T, 2, EPI_RICH><<<rp, NTHR, p2, st>>>(g, jobs, s, 0, 0);
+                CKLAUNCH();
+                return 0;
+            }
+            const long long it2 = (long long)nj * 2 * r8::XTILES, it1 = (long long)nj * r8::XTILES, cap = 3LL * c->nsm;
+            const dim3 px2((unsigned)(it2 < cap ? it2 : cap)), px1((unsigned)(it1 < cap ? it1 : cap));
             r8::kr_plane_forward<T, 2><<<rp, NTHR, ps, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0);
-            r8::kr_xpass<T, 2><<<rx, NTHR, xs, st>>>(g, jobs, 0, 0, 1);
+            r8::kp_xpass<T, 2><<<px2, NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, 0, 1);
             r8::kr_plane_mid<T><<<rp, NTHR, ps, st>>>(g, jobs, 1);
-            r8::kr_xpass<T, 1><<<rx, NTHR, xs, st>>>(g, jobs, 1, 1, 1);
+            r8::kp_xpass<T, 1><<<px1, NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 1, 1, 1);
             r8::kr_plane_inverse<T, 2, EPI_RICH><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, 0);
             CKLAUNCH();
             return 0;
@@ -510,7 +550,17 @@ static int step_disc_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, 
             const dim3 rp(N, nj), rx(r8::PLANE / r8::GROUPS, nj);
             const size_t ps = r8::plane_smem<C>(), xs = r8::xpass_smem<C>();
             r8::kr_plane_forward<T, 1><<<rp, NTHR, ps, st>>>(g, jobs, s, FM_NONE, 0, 0);
-            r8::kr_xpass<T, 1><<<rx, NTHR, xs, st>>>(g, jobs, 0, half, half);
+            const dim3 bx(r8::PLANE / r8::XT, nj);
+            if (c->r8 == 2) {
+                const size_t p1 = r8::kb_plane_smem<C>(false);
+                r8::kb_plane_forward<T, 1><<<rp, NTHR, p1, st>>>(g, jobs, s, FM_NONE, 0, 0);
+                r8::kb_xpass<T, 1><<<bx, NTHR, r8::xbulk_smem<C, 1>(), st>>>(g, jobs, 0, half, half);
+                r8::kb_plane_inverse<T, 1, EPI_SCALE><<<rp, NTHR, p1, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
+                CKLAUNCH();
+                return 0;
+            }
+            const long long it1 = (long long)nj * r8::XTILES, cap = 3LL * c->nsm;
+            r8::kp_xpass<T, 1><<<(unsigned)(it1 < cap ? it1 : cap), NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, half, half);
             r8::kr_plane_inverse<T, 1, EPI_SCALE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
             CKLAUNCH();
             return 0;

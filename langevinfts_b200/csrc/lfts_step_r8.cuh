@@ -21,6 +21,12 @@
 //     j + 8m, so rows y and y + 32 of the same kz sit in the same lane.
 #pragma once
 #include "lfts_step_kernels.cuh"
+#include "lfts_bulk.cuh"
+
+// resident CTAs per SM the plane kernels are compiled for (register budget)
+#ifndef LFTS_R8_MINB
+#define LFTS_R8_MINB 2
+#endif
 
 namespace lfts {
 namespace r8 {
@@ -53,11 +59,14 @@ template <typename C> struct RowX {
     C *b;
     __device__ __forceinline__ C &ref(int k, int j) const { return b[9 * k + j]; }
 };
-// exchange slots down a plane column (row stride PR), skewed: (k, j) at row 8k + ((j + k) & 7)
-template <typename C> struct ColS {
+// exchange slots down a column of a buffer with row stride S, skewed:
+// (k, j) at row 8k + ((j + k) & 7), so both the writes (fixed k) and the reads
+// (fixed j) of a lane group touch eight different banks
+template <typename C, int S> struct ColX {
     C *b;
-    __device__ __forceinline__ C &ref(int k, int j) const { return b[(8 * k + ((j + k) & 7)) * PR]; }
+    __device__ __forceinline__ C &ref(int k, int j) const { return b[(8 * k + ((j + k) & 7)) * S]; }
 };
+template <typename C> using ColS = ColX<C, PR>;
 
 // One 64-point transform held by the 8 lanes of a group (mask = the group's
 // lanes).  On entry lane j holds x[j + 8m] in a[m]; on exit lane t holds
@@ -86,53 +95,133 @@ __device__ __forceinline__ T fmul_mode(int mode, T f) {
     return mode == FM_NONE ? (T)1 : (mode == FM_FAC_SQ ? f * f : f);
 }
 
-// y-phase, forward, rows paired (y, y + 32): lines u = 0..31 of the plane hold
-// Z_u = F_z[row u] + i F_z[row u + 32]; task kz splits them and transforms
-// column kz over y, then stores it to out (column kz of one spectrum plane).
+// The y-phase has 32 tasks, one per lane group: task kz in 1..31 owns the
+// columns kz and 64 - kz of the z-transformed plane, and task 0 owns the DC
+// and Nyquist columns 0 and 32.  Those two are real sequences in y, so task 0
+// carries them as one complex column c = a + i b.
+
+// Lane t holds c[k] = C[t + 8k] with C = F[a] + i F[b] (a, b real sequences);
+// p[k] = C[-(t + 8k) mod 64], fetched from lane (8 - t) & 7 of the group.
 template <typename C>
-__device__ __forceinline__ void y_forward_paired(C *P, int kz, int j, C wf, unsigned mask, C *out) {
-    const int kc = (N - kz) & (N - 1);
-    C a[8];
+__device__ __forceinline__ void herm_partner(const C (&c)[8], C (&p)[8], int t, int lane, unsigned mask) {
+    const int src = (lane & 24) | ((8 - t) & 7);
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-        const int u = j + 8 * m;
-        split_pair(P[u * PR + xpad(kz)], cconj(P[u * PR + xpad(kc)]), a[m], a[m + 4]);
+    for (int k = 0; k < 8; k++) {
+        C v;
+        v.x = __shfl_sync(mask, c[7 - k].x, src);
+        v.y = __shfl_sync(mask, c[7 - k].y, src);
+        p[k] = t == 0 ? c[(8 - k) & 7] : v;
     }
-    __syncwarp(mask);
-    fft64<-1>(a, ColS<C>{P + xpad(kz)}, j, wf, mask);
-#pragma unroll
-    for (int k = 0; k < 8; k++) out[(j + 8 * k) * NZC] = a[k];
 }
 
-// y-phase, inverse, rows paired (y, y + 32): column kz of one spectrum plane
-// (in) is transformed over ky; lane j then holds rows j + 8k and packs rows
-// u and u + 32 into the z-line u: Z_u[kz] = A_u + i A_{u+32} and, at 64 - kz,
-// the Hermitian extension (imaginary parts of DC and Nyquist dropped).
+// After the forward y-transform: write task kz's column(s) (c[k] at ky = j + 8k)
+// to a spectrum plane st ([ky][kz], row stride NZC; global or shared).  Task 0
+// splits c = F[col0] + i F[col32] into the two columns.
 template <typename C>
-__device__ __forceinline__ void y_inverse_paired(C *P, int kz, int j, C wi, unsigned mask, const C *in) {
-    const int kc = (N - kz) & (N - 1);
-    C a[8];
+__device__ __forceinline__ void put_columns(C *st, int kz, const C (&c)[8], int j, int lane, unsigned mask) {
+    if (kz != 0) {
 #pragma unroll
-    for (int m = 0; m < 8; m++) a[m] = in[(j + 8 * m) * NZC];
-    fft64<+1>(a, ColS<C>{P + xpad(kz)}, j, wi, mask);
-    if (kz == 0 || kz == N / 2) {
+        for (int k = 0; k < 8; k++) st[(j + 8 * k) * NZC + kz] = c[k];
+    } else {
+        C p[8];
+        herm_partner(c, p, j, lane, mask);
 #pragma unroll
-        for (int k = 0; k < 8; k++) a[k].y = 0;
+        for (int k = 0; k < 8; k++) {
+            C a, b;
+            split_pair(c[k], cconj(p[k]), a, b);
+            st[(j + 8 * k) * NZC] = a;
+            st[(j + 8 * k) * NZC + N / 2] = b;
+        }
     }
+}
+
+// Read task kz's column(s) of a spectrum plane st for an inverse y-transform
+// (task 0: c = col0 + i col32).
+template <typename C>
+__device__ __forceinline__ void get_columns(const C *st, int kz, C (&c)[8], int j) {
+    if (kz != 0) {
+#pragma unroll
+        for (int m = 0; m < 8; m++) c[m] = st[(j + 8 * m) * NZC + kz];
+    } else {
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const C a = st[(j + 8 * m) * NZC], b = st[(j + 8 * m) * NZC + N / 2];
+            c[m].x = a.x - b.y;
+            c[m].y = a.y + b.x;
+        }
+    }
+}
+
+// y-phase forward on rows paired (u, u + 32): z-lines u = 0..31 of P (row
+// stride S) hold Z_u = F_z[row u] + i F_z[row u + 32].  Task kz splits them,
+// transforms over y and leaves the column(s) in c (lane j: ky = j + 8k).
+template <typename C, int S>
+__device__ __forceinline__ void yfwd_paired_task(C *P, int kz, int j, C wf, unsigned mask, C (&c)[8]) {
+    if (kz != 0) {
+        const int kc = N - kz;
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const int u = j + 8 * m;
+            split_pair(P[u * S + xpad(kz)], cconj(P[u * S + xpad(kc)]), c[m], c[m + 4]);
+        }
+    } else {
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const int u = j + 8 * m;
+            const C z0 = P[u * S], z32 = P[u * S + xpad(N / 2)];
+            c[m].x = z0.x;  // row u: DC + i Nyquist
+            c[m].y = z32.x;
+            c[m + 4].x = z0.y;  // row u + 32
+            c[m + 4].y = z32.y;
+        }
+    }
+    __syncwarp(mask);
+    fft64<-1>(c, ColX<C, S>{P + xpad(kz)}, j, wf, mask);
+}
+
+// Pack rows u, u + 32 (lane j holds rows j + 8k, k < 8) of the inverse
+// y-transformed column(s) of task kz into the z-lines u of P (imaginary parts
+// of DC and Nyquist dropped, Hermitian extension at 64 - kz).
+template <typename C, int S>
+__device__ __forceinline__ void put_zlines_paired(C *P, int kz, int j, const C (&a)[8]) {
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const int u = j + 8 * k;
         const C a0 = a[k], a1 = a[k + 4];
         C z;
-        z.x = a0.x - a1.y;
-        z.y = a0.y + a1.x;
-        P[u * PR + xpad(kz)] = z;
-        if (kc != kz) {
+        if (kz != 0) {
+            z.x = a0.x - a1.y;
+            z.y = a0.y + a1.x;
+            P[u * S + xpad(kz)] = z;
             z.x = a0.x + a1.y;
             z.y = -a0.y + a1.x;
-            P[u * PR + xpad(kc)] = z;
+            P[u * S + xpad(N - kz)] = z;
+        } else {
+            z.x = a0.x;  // s0(u) + i s0(u + 32)
+            z.y = a1.x;
+            P[u * S] = z;
+            z.x = a0.y;  // s32(u) + i s32(u + 32)
+            z.y = a1.y;
+            P[u * S + xpad(N / 2)] = z;
         }
     }
+}
+
+// y-phase forward, rows paired, column(s) stored to a global spectrum plane
+template <typename C>
+__device__ __forceinline__ void y_forward_paired(C *P, int kz, int j, int lane, C wf, unsigned mask, C *plane) {
+    C a[8];
+    yfwd_paired_task<C, PR>(P, kz, j, wf, mask, a);
+    put_columns(plane, kz, a, j, lane, mask);
+}
+
+// y-phase inverse, rows paired, from a global spectrum plane into z-lines
+template <typename C>
+__device__ __forceinline__ void y_inverse_paired(C *P, int kz, int j, C wi, unsigned mask, const C *plane) {
+    C a[8];
+    get_columns(plane, kz, a, j);
+    fft64<+1>(a, ColS<C>{P + xpad(kz)}, j, wi, mask);
+    put_zlines_paired<C, PR>(P, kz, j, a);
 }
 
 // ------------------------------------------------------------------------
@@ -140,7 +229,7 @@ __device__ __forceinline__ void y_inverse_paired(C *P, int kz, int j, C wi, unsi
 //   NBR = 2: spectra of f0(fac) q and f1(fac) q (slots spec_out0, +1);
 //   NBR = 1: spectrum of f0(fac) q (slot spec_out0).
 template <typename T, int NBR>
-__global__ void __launch_bounds__(NTHR, 2) kr_plane_forward(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
+__global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_forward(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
                                                             int fm0, int fm1, int spec_out0) {
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -177,24 +266,31 @@ __global__ void __launch_bounds__(NTHR, 2) kr_plane_forward(GridPlan g, const lf
         }
         __syncthreads();
         // y-columns: task kz splits the branches and transforms both
-        for (int kz = grp; kz <= N / 2; kz += GROUPS) {
-            const int kc = (N - kz) & (N - 1);
-            C A[8], B[8];
+        const int kz = grp;
+        C A[8], B[8];
+        if (kz != 0) {
+            const int kc = N - kz;
 #pragma unroll
             for (int m = 0; m < 8; m++) {
                 const int y = j + 8 * m;
                 split_pair(P[y * PR + xpad(kz)], cconj(P[y * PR + xpad(kc)]), A[m], B[m]);
             }
-            __syncwarp(mask);
-            fft64<-1>(A, ColS<C>{P + xpad(kz)}, j, wf, mask);
-            fft64<-1>(B, ColS<C>{P + xpad(kc)}, j, wf, mask);
-            C *o0 = out + kz, *o1 = out + g.Mc + kz;
+        } else {
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-                o0[(j + 8 * k) * NZC] = A[k];
-                o1[(j + 8 * k) * NZC] = B[k];
+            for (int m = 0; m < 8; m++) {
+                const int y = j + 8 * m;
+                const C z0 = P[y * PR], z32 = P[y * PR + xpad(N / 2)];
+                A[m].x = z0.x;  // branch 0: DC + i Nyquist
+                A[m].y = z32.x;
+                B[m].x = z0.y;  // branch 1
+                B[m].y = z32.y;
             }
         }
+        __syncwarp(mask);
+        fft64<-1>(A, ColS<C>{P + xpad(kz)}, j, wf, mask);
+        fft64<-1>(B, ColS<C>{P + xpad(kz == 0 ? N / 2 : N - kz)}, j, wf, mask);
+        put_columns(out, kz, A, j, lane, mask);
+        put_columns(out + g.Mc, kz, B, j, lane, mask);
     } else {
         // z-lines: rows u and u + 32 packed as real / imaginary part
         {
@@ -218,7 +314,7 @@ __global__ void __launch_bounds__(NTHR, 2) kr_plane_forward(GridPlan g, const lf
             for (int k = 0; k < 8; k++) P[u * PR + 9 * k + j] = a[k];
         }
         __syncthreads();
-        for (int kz = grp; kz <= N / 2; kz += GROUPS) y_forward_paired(P, kz, j, wf, mask, out + kz);
+        y_forward_paired(P, grp, j, lane, wf, mask, out);
     }
 }
 
@@ -262,9 +358,205 @@ __global__ void __launch_bounds__(NTHR, 2) kr_xpass(GridPlan g, const lfts_step_
 }
 
 // ------------------------------------------------------------------------
+// K2 / K4 with bulk copies: the tile of XT columns x 64 rows of each spectrum
+// arrives in shared memory by cp.async.bulk (one 16-byte-aligned row segment
+// per copy), is transformed there with warp w holding rows w + 8m of column
+// lane, and leaves by bulk stores.  All shared-memory accesses are 32
+// consecutive elements of one row (no bank conflicts).
+constexpr int XT = 32;  // columns per CTA
+static_assert(PLANE % XT == 0, "bulk x-pass tiles cover the plane exactly");
+template <typename C, int NBR> constexpr size_t xbulk_smem() { return sizeof(C) * (size_t)NBR * N * XT + 16; }
+
+// 64-point transform down one tile column: on entry warp w holds x[w + 8m],
+// on exit x -> X with warp t holding X[t + 8k].  Uses the column itself as the
+// exchange space (rows 8k + j), bracketed by block barriers.
+template <int SIGN, typename C>
+__device__ __forceinline__ void fft64_tile(C (&a)[8], C *tb, int w, int l, C w1) {
+    SmallDFT<8, C>::run(a, SIGN, nullptr, 0);
+    C t = w1;
+#pragma unroll
+    for (int k = 1; k < 8; k++) {
+        a[k] = cmul(a[k], t);
+        if (k < 7) t = cmul(t, w1);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 8; k++) tb[(8 * k + w) * XT + l] = a[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = tb[(8 * w + k) * XT + l];
+    SmallDFT<8, C>::run(a, SIGN, nullptr, 0);
+}
+
+template <typename T, int NBR>
+__global__ void __launch_bounds__(NTHR, 3) kb_xpass(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_in0,
+                                                    int bsel0, int bsel1) {
+    using C = typename CT<T>::type;
+    constexpr uint32_t ROWB = XT * sizeof(C);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tile = (C *)smem_raw;
+    uint64_t *bar = (uint64_t *)(tile + NBR * N * XT);
+    const lfts_step_job jb = jobs[blockIdx.y];
+    if (jb.active && !jb.active[jb.replica]) return;
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+    const int col0 = blockIdx.x * XT;
+    C *sb = (C *)jb.spec + (size_t)spec_in0 * g.Mc + col0;
+    if (((uintptr_t)sb | (uintptr_t)g.Mc * sizeof(C)) & 15) {
+        if (tid == 0) kerr_set(KERR_MISALIGNED);
+        return;
+    }
+    if (tid == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (w == 0) {
+        if (l == 0) mbar_arrive_expect_tx(bar, NBR * N * ROWB);
+        __syncwarp();
+        for (int r = l; r < NBR * N; r += 32) {
+            const int b = r / N, x = r - b * N;
+            bulk_load(tile + r * XT, sb + (size_t)b * g.Mc + (size_t)x * PLANE, ROWB, bar);
+        }
+    }
+    const T *bt0 = (const T *)(bsel0 ? jb.bond_half : jb.bond) + col0 + l;
+    const T *bt1 = (const T *)(bsel1 ? jb.bond_half : jb.bond) + col0 + l;
+    if (!mbar_wait(bar, 0)) {
+        mbar_wait(bar, 0);
+        return;
+    }
+    const C wf = tw_base<C>(w, -1), wi = tw_base<C>(w, +1);
+#pragma unroll 1
+    for (int b = 0; b < NBR; b++) {
+        C *tb = tile + b * N * XT;
+        // bond factors for kx = w + 8k (in flight during the forward transform)
+        T bv[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) bv[k] = (b == 0 ? bt0 : bt1)[(w + 8 * k) * PLANE];
+        C a[8];
+#pragma unroll
+        for (int m = 0; m < 8; m++) a[m] = tb[(w + 8 * m) * XT + l];
+        fft64_tile<-1>(a, tb, w, l, wf);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            a[k].x *= bv[k];
+            a[k].y *= bv[k];
+        }
+        fft64_tile<+1>(a, tb, w, l, wi);
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 8; m++) tb[(w + 8 * m) * XT + l] = a[m];
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (w == 0) {
+        for (int r = l; r < NBR * N; r += 32) {
+            const int b = r / N, x = r - b * N;
+            bulk_store(sb + (size_t)b * g.Mc + (size_t)x * PLANE, tile + r * XT, ROWB);
+        }
+        bulk_commit();
+        bulk_wait_read();
+    }
+}
+
+// ------------------------------------------------------------------------
+// K2 / K4, persistent and pipelined: work items are (job, branch, 32-column
+// tile); each CTA walks items blockIdx.x, + gridDim.x, ... with two shared
+// stages, so the bulk load of its next item and the bulk store of its previous
+// one run while it transforms the current one.  Warp 0 issues all copies.
+constexpr int XTILES = PLANE / XT;
+template <typename C> constexpr size_t xpipe_smem() { return 2 * sizeof(C) * (size_t)N * XT + 16; }
+
+template <typename T, int NBR>
+__global__ void __launch_bounds__(NTHR, 3) kp_xpass(GridPlan g, const lfts_step_job *__restrict__ jobs, int nj,
+                                                    int spec_in0, int bsel0, int bsel1) {
+    using C = typename CT<T>::type;
+    constexpr uint32_t ROWB = XT * sizeof(C), TILEB = N * ROWB;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *stage = (C *)smem_raw;
+    uint64_t *bar = (uint64_t *)(stage + 2 * N * XT);
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+    const long long nitems = (long long)nj * NBR * XTILES;
+    // first item at or after it whose job is active and aligned (>= nitems: none)
+    auto next_item = [&](long long it) -> long long {
+        for (; it < nitems; it += gridDim.x) {
+            const lfts_step_job &jb = jobs[it / (NBR * XTILES)];
+            if (jb.active && !jb.active[jb.replica]) continue;
+            if (((uintptr_t)jb.spec | (uintptr_t)g.Mc * sizeof(C)) & 15) {
+                if (tid == 0) kerr_set(KERR_MISALIGNED);
+                continue;
+            }
+            return it;
+        }
+        return nitems;
+    };
+    // spectrum column block of an item: rows x at + x * PLANE
+    auto item_base = [&](long long it) -> C * {
+        const int job = (int)(it / (NBR * XTILES)), rem = (int)(it - (long long)job * NBR * XTILES);
+        const int b = rem / XTILES, t = rem - b * XTILES;
+        return (C *)jobs[job].spec + (size_t)(spec_in0 + b) * g.Mc + (size_t)t * XT;
+    };
+    auto issue_load = [&](long long it, int st) {  // warp 0
+        C *src = item_base(it);
+        if (l == 0) mbar_arrive_expect_tx(bar + st, TILEB);
+        __syncwarp();
+        for (int r = l; r < N; r += 32) bulk_load(stage + (st * N + r) * XT, src + (size_t)r * PLANE, ROWB, bar + st);
+    };
+    long long cur = next_item(blockIdx.x);
+    if (cur >= nitems) return;
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+    }
+    __syncthreads();
+    if (w == 0) issue_load(cur, 0);
+    const C wf = tw_base<C>(w, -1), wi = tw_base<C>(w, +1);
+    for (int u = 0; cur < nitems; u++) {
+        const int st = u & 1;
+        const long long nxt = next_item(cur + gridDim.x);
+        if (w == 0 && nxt < nitems) {
+            bulk_wait_read();  // the previous store out of stage st ^ 1 has read it
+            __syncwarp();
+            issue_load(nxt, st ^ 1);
+        }
+        const int job = (int)(cur / (NBR * XTILES)), rem = (int)(cur - (long long)job * NBR * XTILES);
+        const int b = rem / XTILES, t = rem - b * XTILES;
+        const lfts_step_job &jb = jobs[job];
+        const T *bt = (const T *)((b == 0 ? bsel0 : bsel1) ? jb.bond_half : jb.bond) + t * XT + l;
+        T bv[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) bv[k] = bt[(w + 8 * k) * PLANE];
+        if (!mbar_wait(bar + st, (u >> 1) & 1)) {
+            mbar_wait(bar + st, (u >> 1) & 1);
+            if (w == 0) bulk_wait_read();
+            return;
+        }
+        C *tb = stage + st * N * XT;
+        C a[8];
+#pragma unroll
+        for (int m = 0; m < 8; m++) a[m] = tb[(w + 8 * m) * XT + l];
+        fft64_tile<-1>(a, tb, w, l, wf);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            a[k].x *= bv[k];
+            a[k].y *= bv[k];
+        }
+        fft64_tile<+1>(a, tb, w, l, wi);
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 8; m++) tb[(w + 8 * m) * XT + l] = a[m];
+        fence_proxy_async();
+        __syncthreads();
+        if (w == 0) {
+            C *dst = item_base(cur);
+            for (int r = l; r < N; r += 32) bulk_store(dst + (size_t)r * PLANE, tb + r * XT, ROWB);
+            bulk_commit();
+        }
+        cur = nxt;
+    }
+    if (w == 0) bulk_wait_read();
+}
+
+// ------------------------------------------------------------------------
 // K3: inverse zy, multiply by e = fac^2, forward zy, in place on slot spec_idx
 template <typename T>
-__global__ void __launch_bounds__(NTHR, 2) kr_plane_mid(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_idx) {
+__global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_mid(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_idx) {
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;
@@ -275,7 +567,7 @@ __global__ void __launch_bounds__(NTHR, 2) kr_plane_mid(GridPlan g, const lfts_s
     const C wf = tw_base<C>(j, -1), wi = tw_base<C>(j, +1);
     C *sp = (C *)jb.spec + (size_t)spec_idx * g.Mc + (size_t)x * PLANE;
     const T *fac = (const T *)jb.fac + (long long)x * N * N;
-    for (int kz = grp; kz <= N / 2; kz += GROUPS) y_inverse_paired(P, kz, j, wi, mask, sp + kz);
+    y_inverse_paired(P, grp, j, wi, mask, sp);
     __syncthreads();
     {
         const int u = grp;
@@ -300,7 +592,7 @@ __global__ void __launch_bounds__(NTHR, 2) kr_plane_mid(GridPlan g, const lfts_s
         for (int k = 0; k < 8; k++) P[u * PR + 9 * k + j] = a[k];
     }
     __syncthreads();
-    for (int kz = grp; kz <= N / 2; kz += GROUPS) y_forward_paired(P, kz, j, wf, mask, sp + kz);
+    y_forward_paired(P, grp, j, lane, wf, mask, sp);
 }
 
 // ------------------------------------------------------------------------
@@ -308,7 +600,7 @@ __global__ void __launch_bounds__(NTHR, 2) kr_plane_mid(GridPlan g, const lfts_s
 //   NBR = 2, EPI_RICH: q' = (4 e_h v2 - e_h^2 v1) / 3 (v1 from slot spec_in0);
 //   NBR = 1, EPI_SCALE: q' = f(fac) v.
 template <typename T, int NBR, int EPI>
-__global__ void __launch_bounds__(NTHR, 2) kr_plane_inverse(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
+__global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_inverse(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
                                                             int spec_in0, int fm0) {
     static_assert((NBR == 2 && EPI == EPI_RICH) || (NBR == 1 && EPI == EPI_SCALE), "supported epilogues");
     using C = typename CT<T>::type;
@@ -324,34 +616,32 @@ __global__ void __launch_bounds__(NTHR, 2) kr_plane_inverse(GridPlan g, const lf
     const T *fac = (const T *)jb.fac + poff;
     T *qout = (T *)jb.out + s * jb.out_stride + poff;
     if (NBR == 2) {
-        for (int kz = grp; kz <= N / 2; kz += GROUPS) {
-            const int kc = (N - kz) & (N - 1);
+        {
+            const int kz = grp;
             C A[8], B[8];
-#pragma unroll
-            for (int m = 0; m < 8; m++) {
-                A[m] = in[(j + 8 * m) * NZC + kz];
-                B[m] = in[g.Mc + (j + 8 * m) * NZC + kz];
-            }
+            get_columns(in, kz, A, j);
+            get_columns(in + g.Mc, kz, B, j);
             fft64<+1>(A, ColS<C>{P + xpad(kz)}, j, wi, mask);
-            fft64<+1>(B, ColS<C>{P + xpad(kc)}, j, wi, mask);
-            if (kz == 0 || kz == N / 2) {
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    A[k].y = 0;
-                    B[k].y = 0;
-                }
-            }
+            fft64<+1>(B, ColS<C>{P + xpad(kz == 0 ? N / 2 : N - kz)}, j, wi, mask);
+            // z-line y = j + 8k: A + i B (Hermitian extension at 64 - kz)
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 const int y = j + 8 * k;
                 C z;
-                z.x = A[k].x - B[k].y;
-                z.y = A[k].y + B[k].x;
-                P[y * PR + xpad(kz)] = z;
-                if (kc != kz) {
+                if (kz != 0) {
+                    z.x = A[k].x - B[k].y;
+                    z.y = A[k].y + B[k].x;
+                    P[y * PR + xpad(kz)] = z;
                     z.x = A[k].x + B[k].y;
                     z.y = -A[k].y + B[k].x;
-                    P[y * PR + xpad(kc)] = z;
+                    P[y * PR + xpad(N - kz)] = z;
+                } else {
+                    z.x = A[k].x;  // A(kz = 0) + i B(kz = 0)
+                    z.y = B[k].x;
+                    P[y * PR] = z;
+                    z.x = A[k].y;  // A(kz = 32) + i B(kz = 32)
+                    z.y = B[k].y;
+                    P[y * PR + xpad(N / 2)] = z;
                 }
             }
         }
@@ -369,7 +659,7 @@ __global__ void __launch_bounds__(NTHR, 2) kr_plane_inverse(GridPlan g, const lf
             for (int k = 0; k < 8; k++) qout[y * N + j + 8 * k] = ((T)4 * eh[k] * a[k].y - eh[k] * eh[k] * a[k].x) / (T)3;
         }
     } else {
-        for (int kz = grp; kz <= N / 2; kz += GROUPS) y_inverse_paired(P, kz, j, wi, mask, in + kz);
+        y_inverse_paired(P, grp, j, wi, mask, in);
         __syncthreads();
         const int u = grp;
         T fa[8], fb[8];
