@@ -265,32 +265,33 @@ __global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_forward(GridPlan 
             for (int k = 0; k < 8; k++) P[y * PR + 9 * k + j] = a[k];
         }
         __syncthreads();
-        // y-columns: task kz splits the branches and transforms both
-        const int kz = grp;
-        C A[8], B[8];
-        if (kz != 0) {
-            const int kc = N - kz;
+        // y-columns: task kz splits the branches; branch 1 waits in its own
+        // column (xkc) while branch 0 is transformed and stored
+        const int kz = grp, xkz = xpad(kz), xkc = xpad(kz == 0 ? N / 2 : N - kz);
+        C A[8];
 #pragma unroll
-            for (int m = 0; m < 8; m++) {
-                const int y = j + 8 * m;
-                split_pair(P[y * PR + xpad(kz)], cconj(P[y * PR + xpad(kc)]), A[m], B[m]);
+        for (int m = 0; m < 8; m++) {
+            const int y = j + 8 * m;
+            const C zk = P[y * PR + xkz], zc = P[y * PR + xkc];
+            C b;
+            if (kz != 0) {
+                split_pair(zk, cconj(zc), A[m], b);
+            } else {
+                A[m].x = zk.x;  // branch 0: DC + i Nyquist
+                A[m].y = zc.x;
+                b.x = zk.y;  // branch 1
+                b.y = zc.y;
             }
-        } else {
-#pragma unroll
-            for (int m = 0; m < 8; m++) {
-                const int y = j + 8 * m;
-                const C z0 = P[y * PR], z32 = P[y * PR + xpad(N / 2)];
-                A[m].x = z0.x;  // branch 0: DC + i Nyquist
-                A[m].y = z32.x;
-                B[m].x = z0.y;  // branch 1
-                B[m].y = z32.y;
-            }
+            P[y * PR + xkc] = b;
         }
         __syncwarp(mask);
-        fft64<-1>(A, ColS<C>{P + xpad(kz)}, j, wf, mask);
-        fft64<-1>(B, ColS<C>{P + xpad(kz == 0 ? N / 2 : N - kz)}, j, wf, mask);
+        fft64<-1>(A, ColS<C>{P + xkz}, j, wf, mask);
         put_columns(out, kz, A, j, lane, mask);
-        put_columns(out + g.Mc, kz, B, j, lane, mask);
+#pragma unroll
+        for (int m = 0; m < 8; m++) A[m] = P[(j + 8 * m) * PR + xkc];
+        __syncwarp(mask);
+        fft64<-1>(A, ColS<C>{P + xkc}, j, wf, mask);
+        put_columns(out + g.Mc, kz, A, j, lane, mask);
     } else {
         // z-lines: rows u and u + 32 packed as real / imaginary part
         {
@@ -617,31 +618,36 @@ __global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_inverse(GridPlan 
     T *qout = (T *)jb.out + s * jb.out_stride + poff;
     if (NBR == 2) {
         {
-            const int kz = grp;
-            C A[8], B[8];
+            // branch 0 first; its inverse column waits in column xkz while
+            // branch 1 is transformed, then both are packed into the z-lines
+            const int kz = grp, xkz = xpad(kz), xkc = xpad(kz == 0 ? N / 2 : N - kz);
+            C A[8];
             get_columns(in, kz, A, j);
-            get_columns(in + g.Mc, kz, B, j);
-            fft64<+1>(A, ColS<C>{P + xpad(kz)}, j, wi, mask);
-            fft64<+1>(B, ColS<C>{P + xpad(kz == 0 ? N / 2 : N - kz)}, j, wi, mask);
+            fft64<+1>(A, ColS<C>{P + xkz}, j, wi, mask);
+#pragma unroll
+            for (int k = 0; k < 8; k++) P[(j + 8 * k) * PR + xkz] = A[k];
+            get_columns(in + g.Mc, kz, A, j);
+            fft64<+1>(A, ColS<C>{P + xkc}, j, wi, mask);
             // z-line y = j + 8k: A + i B (Hermitian extension at 64 - kz)
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 const int y = j + 8 * k;
+                const C a = P[y * PR + xkz], bb = A[k];
                 C z;
                 if (kz != 0) {
-                    z.x = A[k].x - B[k].y;
-                    z.y = A[k].y + B[k].x;
-                    P[y * PR + xpad(kz)] = z;
-                    z.x = A[k].x + B[k].y;
-                    z.y = -A[k].y + B[k].x;
-                    P[y * PR + xpad(N - kz)] = z;
+                    z.x = a.x - bb.y;
+                    z.y = a.y + bb.x;
+                    P[y * PR + xkz] = z;
+                    z.x = a.x + bb.y;
+                    z.y = -a.y + bb.x;
+                    P[y * PR + xkc] = z;
                 } else {
-                    z.x = A[k].x;  // A(kz = 0) + i B(kz = 0)
-                    z.y = B[k].x;
-                    P[y * PR] = z;
-                    z.x = A[k].y;  // A(kz = 32) + i B(kz = 32)
-                    z.y = B[k].y;
-                    P[y * PR + xpad(N / 2)] = z;
+                    z.x = a.x;  // A(kz = 0) + i B(kz = 0)
+                    z.y = bb.x;
+                    P[y * PR + xkz] = z;
+                    z.x = a.y;  // A(kz = 32) + i B(kz = 32)
+                    z.y = bb.y;
+                    P[y * PR + xkc] = z;
                 }
             }
         }
