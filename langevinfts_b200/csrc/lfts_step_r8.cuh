@@ -72,15 +72,26 @@ template <typename C> using ColS = ColX<C, PR>;
 // lanes).  On entry lane j holds x[j + 8m] in a[m]; on exit lane t holds
 // X[t + 8k] in a[k], X[k] = sum_n x[n] exp(SIGN 2 pi i n k / 64).
 // w1 = tw_base(j, SIGN).
+// a[k] *= w1^k for k = 1..7; the powers come from a tree of depth 3
+// (w2 = w1 w1, w3 = w2 w1, w4 = w2 w2, w5 = w4 w1, w6 = w3 w3, w7 = w4 w3),
+// not a serial chain of six dependent multiplies
+template <typename C>
+__device__ __forceinline__ void twiddle8(C (&a)[8], C w1) {
+    const C w2 = cmul(w1, w1);
+    const C w3 = cmul(w2, w1), w4 = cmul(w2, w2);
+    a[1] = cmul(a[1], w1);
+    a[2] = cmul(a[2], w2);
+    a[3] = cmul(a[3], w3);
+    a[4] = cmul(a[4], w4);
+    a[5] = cmul(a[5], cmul(w4, w1));
+    a[6] = cmul(a[6], cmul(w3, w3));
+    a[7] = cmul(a[7], cmul(w4, w3));
+}
+
 template <int SIGN, class AT, typename C>
 __device__ __forceinline__ void fft64(C (&a)[8], const AT &at, int j, C w1, unsigned mask) {
     SmallDFT<8, C>::run(a, SIGN, nullptr, 0);
-    C w = w1;
-#pragma unroll
-    for (int k = 1; k < 8; k++) {
-        a[k] = cmul(a[k], w);
-        if (k < 7) w = cmul(w, w1);
-    }
+    twiddle8(a, w1);
 #pragma unroll
     for (int k = 0; k < 8; k++) at.ref(k, j) = a[k];
     __syncwarp(mask);
@@ -374,12 +385,7 @@ template <typename C, int NBR> constexpr size_t xbulk_smem() { return sizeof(C) 
 template <int SIGN, typename C>
 __device__ __forceinline__ void fft64_tile(C (&a)[8], C *tb, int w, int l, C w1) {
     SmallDFT<8, C>::run(a, SIGN, nullptr, 0);
-    C t = w1;
-#pragma unroll
-    for (int k = 1; k < 8; k++) {
-        a[k] = cmul(a[k], t);
-        if (k < 7) t = cmul(t, w1);
-    }
+    twiddle8(a, w1);
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < 8; k++) tb[(8 * k + w) * XT + l] = a[k];
