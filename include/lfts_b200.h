@@ -265,6 +265,27 @@ int lfts_am_batch_update(lfts_ctx ctx, int R, long long n, int L, const int *hea
                          const double *mix, const double *a, const double *w_cur, long long w_stride, const double *d_cur,
                          long long d_stride, const double *w_hist, const double *d_hist, double *w_out, long long out_stride);
 
+/* ---- structure function (recording of the L-FTS driver) ------------------ */
+
+/* Forward real-to-complex 3D FFT of double fields, unnormalised, in the
+ * numpy.fft.rfftn layout [nx][ny][nz/2+1]: jobs[j].in (M doubles) ->
+ * jobs[j].spec (Mc complex doubles); in_stride, out, fac and the bond tables
+ * are ignored, active/replica mask jobs as in the step calls.  Double-precision
+ * contexts only.  Replaces the host np.fft.rfftn of the structure-function
+ * recording (examples/fts/lfts.py:757-762). */
+int lfts_fft_forward(lfts_ctx ctx, const lfts_step_job *jobs, int njobs);
+
+/* Structure-function accumulation (examples/fts/lfts.py:754-767), for each
+ * replica r and monomer pair p = (a, b) = (pairs[2p], pairs[2p+1]):
+ *   sf[r][p][k] += mu_a(k) * conj(phi_b(k) * inv_m),
+ *   mu_a(k) = sum_{q < I} spec[r][S + q][k] * coef[q*S + a],
+ * where spec[r][s] (s < S) is the transform of phi_s and spec[r][S + q] that of
+ * the q-th real auxiliary field (Mc complex doubles each, replica stride
+ * (S + I)*Mc).  coef (device, I x S) = A_inv[q][a] / eigenvalue[q] / M;
+ * pairs: device ints; sf: device complex doubles [R][npairs][Mc]. */
+int lfts_sf_accumulate(lfts_ctx ctx, int R, int S, int I, const void *spec, const double *coef, double inv_m, int npairs,
+                       const int *pairs, void *sf);
+
 /* ---- allocation-free inner products (no reference counterpart) ----------
  * lfts_dots_static computes what lfts_dots computes,
  *   out[j] = scale_j * sum_{i<M} a_j[i] b_j[i] (/ w_j[i] if w_j != NULL),

@@ -123,6 +123,7 @@ template <typename T, bool GEN> static cudaError_t set_attrs_t(int max_smem) {
     if ((r = allow_smem(k_xpass<T, 1, GEN>, max_smem)) != cudaSuccess) e = r;
     if ((r = allow_smem(k_xpass<T, 2, GEN>, max_smem)) != cudaSuccess) e = r;
     if ((r = allow_smem(k_xstress<T, GEN>, max_smem)) != cudaSuccess) e = r;
+    if ((r = allow_smem(k_xpass_forward<T, GEN>, max_smem)) != cudaSuccess) e = r;
     return e;
 }
 
@@ -1011,6 +1012,80 @@ extern "C" int lfts_field_factors_batch(lfts_ctx c, const double *w, double coef
         k_field_factors<double><<<grid_for(n), NTHR, 0, c->stream>>>(w, coef, (double *)fac_out, n);
     else
         k_field_factors<float><<<grid_for(n), NTHR, 0, c->stream>>>(w, coef, (float *)fac_out, n);
+    c->launches += 1;
+    CKLAUNCH();
+    return 0;
+}
+
+// ---------------------------------------------------------------- forward FFT and structure function
+extern "C" int lfts_fft_forward(lfts_ctx c, const lfts_step_job *jobs, int nj) {
+    if (!c || !jobs) return fail("null argument");
+    if (c->prec != 8) return fail("lfts_fft_forward needs a double-precision context");
+    if (nj <= 0) return 0;
+    if (nj > 65535) return fail("too many jobs in one launch (max 65535)");
+    const GridPlan &g = c->g;
+    const dim3 gp(g.n0, nj), gx(c->ntiles, nj);
+    if (c->gen) {
+        k_plane_forward<double, 1, true><<<gp, NTHR, c->sm_pf1, c->stream>>>(g, jobs, 0, FM_NONE, 0, 0, c->zb);
+        k_xpass_forward<double, true><<<gx, NTHR, c->sm_x1, c->stream>>>(g, jobs, 0, c->TJ);
+    } else {
+        k_plane_forward<double, 1, false><<<gp, NTHR, c->sm_pf1, c->stream>>>(g, jobs, 0, FM_NONE, 0, 0, c->zb);
+        k_xpass_forward<double, false><<<gx, NTHR, c->sm_x1, c->stream>>>(g, jobs, 0, c->TJ);
+    }
+    c->launches += 2;
+    CKLAUNCH();
+    return 0;
+}
+
+// sf[r][p][k] += mu_a(k) conj(phi_b(k) inv_m),  mu_a = sum_q spec[r][S+q][k] coef[q][a]
+__global__ void __launch_bounds__(NTHR) k_sf_accumulate(int R, int S, int I, long long Mc, const double2 *__restrict__ spec,
+                                                        const double *__restrict__ coef, double inv_m, int npairs,
+                                                        const int *__restrict__ pairs, double2 *__restrict__ sf) {
+    const long long n = (long long)R * Mc;
+    for (long long idx = blockIdx.x * (long long)NTHR + threadIdx.x; idx < n; idx += (long long)gridDim.x * NTHR) {
+        const int r = (int)(idx / Mc);
+        const long long k = idx - (long long)r * Mc;
+        const double2 *sr = spec + (size_t)r * (S + I) * Mc + k;
+        double2 mu[LFTS_MAX_MONOMERS];
+#pragma unroll
+        for (int a = 0; a < LFTS_MAX_MONOMERS; a++) mu[a] = make_double2(0.0, 0.0);
+        for (int q = 0; q < I; q++) {
+            const double2 w = sr[(size_t)(S + q) * Mc];
+#pragma unroll
+            for (int a = 0; a < LFTS_MAX_MONOMERS; a++) {
+                if (a < S) {
+                    const double cf = coef[q * S + a];
+                    mu[a].x += w.x * cf;
+                    mu[a].y += w.y * cf;
+                }
+            }
+        }
+        double2 *o = sf + (size_t)r * npairs * Mc + k;
+        for (int p = 0; p < npairs; p++) {
+            const int a = pairs[2 * p], b = pairs[2 * p + 1];
+            double2 ph = sr[(size_t)b * Mc];
+            ph.x *= inv_m;
+            ph.y *= inv_m;
+            double2 m = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int t = 0; t < LFTS_MAX_MONOMERS; t++)
+                if (t == a) m = mu[t];
+            double2 acc = o[(size_t)p * Mc];
+            acc.x += m.x * ph.x + m.y * ph.y;
+            acc.y += m.y * ph.x - m.x * ph.y;
+            o[(size_t)p * Mc] = acc;
+        }
+    }
+}
+
+extern "C" int lfts_sf_accumulate(lfts_ctx c, int R, int S, int I, const void *spec, const double *coef, double inv_m,
+                                  int npairs, const int *pairs, void *sf) {
+    if (!c || !spec || !coef || !pairs || !sf) return fail("null argument");
+    if (R <= 0 || S <= 0 || I < 0 || npairs <= 0) return fail("R, S and npairs must be positive, I non-negative");
+    if (S > LFTS_MAX_MONOMERS) return fail("at most " + std::to_string(LFTS_MAX_MONOMERS) + " monomer types");
+    const long long n = (long long)R * c->g.Mc;
+    k_sf_accumulate<<<grid_for(n), NTHR, 0, c->stream>>>(R, S, I, c->g.Mc, (const double2 *)spec, coef, inv_m, npairs, pairs,
+                                                        (double2 *)sf);
     c->launches += 1;
     CKLAUNCH();
     return 0;

@@ -32,6 +32,8 @@ struct SaddleStats {
     std::vector<double> hamiltonian;  // per replica
     std::vector<int> failed;          // per replica: tolerance not met (fields restored)
     std::vector<double> partitions;   // R x P
+    std::vector<double> aux_mean;     // R x S: <w_aux[i]> at the returned fields (dH/dchiN, lfts.py:265-274)
+    std::vector<double> aux_msq;      // R x S: <w_aux[i]^2>
 };
 
 class BatchedLangevin {
@@ -51,6 +53,16 @@ class BatchedLangevin {
     // Same, with this step's noise already on the device ([R][n_real][M] doubles)
     SaddleStats step_device(const double *noise_dev);
     void *stream() const { return lfts_ctx_stream(ctx_); }
+    // Structure function of every replica (examples/fts/lfts.py:753-767):
+    //   sf[r][p] += mu_a conj(phi_b / M),  mu_a = sum_{q < S-1} F[w_aux_q] coef[q][a],
+    // for the type pairs p = (pairs[2p], pairs[2p+1]); coef (host, (S-1) x S) =
+    // A_inv[q][a] / eigenvalue[q] / M.  A new pair set starts new (zeroed) sums.
+    // Double-precision engines only.
+    void sf_accumulate(const double *coef, const std::vector<int> &pairs);
+    // the sums as host complex doubles [R][npairs][nx][ny][nz/2+1]; reset zeroes them
+    void sf_get(double *out, bool reset);
+    int sf_npairs() const { return sf_np_; }
+    long long n_complex_grid() const;
     GpuComputation &computation() { return *comp_; }
 
    private:
@@ -71,6 +83,10 @@ class BatchedLangevin {
     std::vector<int> n_anderson_, head_;
     std::vector<double> mix_;
     std::vector<std::vector<std::vector<double>>> dot_rows_;
+    // structure-function state: spectra of phi and the real auxiliary fields, sums
+    DevBuf sf_spec_, sf_jobs_, sf_acc_, sf_coef_, sf_pairs_;
+    int sf_np_ = 0;
+    std::vector<int> sf_pairs_host_;
 };
 
 }  // namespace lfts

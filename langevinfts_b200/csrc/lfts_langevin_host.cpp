@@ -232,6 +232,8 @@ SaddleStats BatchedLangevin::find_saddle_point(bool restore_on_failure) {
     check_rc(lfts_memcpy_d2h(ctx_, mean.data(), d_mean, sizeof(double) * mean.size()));
     check_rc(lfts_memcpy_d2h(ctx_, msq.data(), d_var, sizeof(double) * msq.size()));
     st.partitions = comp_->partitions_host();
+    st.aux_mean = mean;
+    st.aux_msq = msq;
     st.hamiltonian.resize(R_);
     for (int r = 0; r < R_; r++) st.hamiltonian[r] = hamiltonian(r, mean, msq, st.partitions);
     // zero-mean pressure field of every replica (lfts.py:866)
@@ -282,6 +284,56 @@ SaddleStats BatchedLangevin::step_device(const double *noise_dev) {
         xi_cur_ = 1 - xi_cur_;  // this step's draw is the next step's "previous" noise (lfts.py:708-709)
     }
     return find_saddle_point(true);
+}
+
+long long BatchedLangevin::n_complex_grid() const {
+    long long M = 0, Mc = 0;
+    check_rc(lfts_ctx_info(ctx_, &M, &Mc, nullptr));
+    return Mc;
+}
+
+void BatchedLangevin::sf_accumulate(const double *coef, const std::vector<int> &pairs) {
+    const int np = (int)pairs.size() / 2;
+    if (np < 1 || (int)pairs.size() != 2 * np) LFTS_THROW("pairs must hold (a, b) monomer type indices");
+    for (int v : pairs)
+        if (v < 0 || v >= S_) LFTS_THROW("monomer type index out of range in pairs");
+    const long long Mc = n_complex_grid();
+    const int W = S_ - 1;    // auxiliary fields 0..S-2 enter mu (lfts.py:760-762)
+    const int F = S_ + W;    // transformed fields per replica: phi_0..phi_{S-1}, w_aux_0..w_aux_{S-2}
+    if (!sf_spec_.get()) {
+        sf_spec_.alloc(ctx_, 2 * sizeof(double) * (size_t)R_ * F * Mc);
+        std::vector<lfts_step_job> jobs((size_t)R_ * F);
+        for (int r = 0; r < R_; r++)
+            for (int f = 0; f < F; f++) {
+                lfts_step_job jb;
+                std::memset(&jb, 0, sizeof jb);
+                jb.in = f < S_ ? (const void *)(phi_ptrs_[f] + (size_t)r * M_)
+                               : (const void *)(w_aux_.as<double>() + ((size_t)r * S_ + (f - S_)) * M_);
+                jb.spec = sf_spec_.as<double>() + 2 * ((size_t)r * F + f) * Mc;
+                jobs[(size_t)r * F + f] = jb;
+            }
+        sf_jobs_.alloc(ctx_, sizeof(lfts_step_job) * jobs.size());
+        check_rc(lfts_memcpy_h2d(ctx_, sf_jobs_.get(), jobs.data(), sf_jobs_.size()));
+        sf_coef_.alloc(ctx_, sizeof(double) * (size_t)std::max(W, 1) * S_);
+    }
+    if (np != sf_np_ || pairs != sf_pairs_host_) {
+        sf_acc_.alloc(ctx_, 2 * sizeof(double) * (size_t)R_ * np * Mc);
+        check_rc(lfts_memset_async(ctx_, sf_acc_.get(), 0, sf_acc_.size()));
+        sf_pairs_.alloc(ctx_, sizeof(int) * pairs.size());
+        check_rc(lfts_memcpy_h2d(ctx_, sf_pairs_.get(), pairs.data(), sf_pairs_.size()));
+        sf_np_ = np;
+        sf_pairs_host_ = pairs;
+    }
+    if (W > 0) check_rc(lfts_memcpy_h2d(ctx_, sf_coef_.get(), coef, sizeof(double) * (size_t)W * S_));
+    check_rc(lfts_fft_forward(ctx_, sf_jobs_.as<lfts_step_job>(), R_ * F));
+    check_rc(lfts_sf_accumulate(ctx_, R_, S_, W, sf_spec_.get(), sf_coef_.as<double>(), 1.0 / (double)M_, np,
+                                sf_pairs_.as<int>(), sf_acc_.get()));
+}
+
+void BatchedLangevin::sf_get(double *out, bool reset) {
+    if (!sf_np_) LFTS_THROW("no structure function has been accumulated");
+    check_rc(lfts_memcpy_d2h(ctx_, out, sf_acc_.get(), sf_acc_.size()));
+    if (reset) check_rc(lfts_memset_async(ctx_, sf_acc_.get(), 0, sf_acc_.size()));
 }
 
 }  // namespace lfts

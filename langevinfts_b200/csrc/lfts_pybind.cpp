@@ -4,6 +4,7 @@
 // platform is "cuda" (FP64) or "cuda-fp32" (FP32 propagators and FFTs, FP64
 // reductions).
 #include <pybind11/numpy.h>
+#include <pybind11/complex.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
@@ -66,6 +67,14 @@ std::map<std::string, const double *> field_map(std::map<std::string, py::array_
 using Arr = py::array_t<double, py::array::c_style | py::array::forcecast>;
 
 }  // namespace
+
+static py::dict stats_dict(const lfts::SaddleStats &s) {
+    py::dict d;
+    d["iterations"] = s.iterations; d["error"] = s.error; d["hamiltonian"] = s.hamiltonian;
+    d["failed"] = s.failed; d["partitions"] = s.partitions;
+    d["aux_mean"] = s.aux_mean; d["aux_msq"] = s.aux_msq;
+    return d;
+}
 
 PYBIND11_MODULE(langevinfts, m) {
     m.doc() = "langevinfts chain-propagator solver on NVIDIA B200 (sm_100a)";
@@ -306,6 +315,7 @@ PYBIND11_MODULE(langevinfts, m) {
         .def("get_model_name", [](Factory &) { return std::string(""); });
 
     // Batched L-FTS engine: n_replicas independent systems on the device.
+
     py::class_<BatchedLangevin>(m, "BatchedLangevin")
         .def(py::init([](Factory &f, ComputationBox *cb, Molecules *mol, PropagatorAnalyzer *pa, int n_replicas, py::dict c) {
             LangevinConfig cfg;
@@ -336,10 +346,7 @@ PYBIND11_MODULE(langevinfts, m) {
                 py::gil_scoped_release nogil;
                 s = b.step_device((const double *)noise_dev);
             }
-            py::dict d;
-            d["iterations"] = s.iterations; d["error"] = s.error; d["hamiltonian"] = s.hamiltonian;
-            d["failed"] = s.failed; d["partitions"] = s.partitions;
-            return d;
+            return stats_dict(s);
         })
         .def("set_fields", [](BatchedLangevin &b, Arr w) {
             py::buffer_info bi = w.request();
@@ -363,11 +370,23 @@ PYBIND11_MODULE(langevinfts, m) {
                 py::gil_scoped_release nogil;
                 s = b.find_saddle_point(false);
             }
-            py::dict d;
-            d["iterations"] = s.iterations; d["error"] = s.error; d["hamiltonian"] = s.hamiltonian;
-            d["failed"] = s.failed; d["partitions"] = s.partitions;
-            return d;
+            return stats_dict(s);
         })
+        .def("sf_accumulate", [](BatchedLangevin &b, Arr coef, std::vector<int> pairs) {
+            py::buffer_info bi = coef.request();
+            if (bi.ndim != 2) throw std::runtime_error("coef must be a (S-1) x S array");
+            py::gil_scoped_release nogil;
+            b.sf_accumulate((const double *)bi.ptr, pairs);
+        }, py::arg("coef"), py::arg("pairs"))
+        .def("get_structure_function", [](BatchedLangevin &b, std::vector<py::ssize_t> shape_k, bool reset) {
+            std::vector<py::ssize_t> shape = {(py::ssize_t)b.n_replicas(), (py::ssize_t)b.sf_npairs()};
+            long long n = 1;
+            for (auto e : shape_k) { shape.push_back(e); n *= e; }
+            if (n != b.n_complex_grid()) throw std::runtime_error("shape_k must describe the half spectrum (nx, ny, nz/2+1)");
+            py::array_t<std::complex<double>> out(shape);
+            b.sf_get((double *)out.request().ptr, reset);
+            return out;
+        }, py::arg("shape_k"), py::arg("reset") = true)
         .def("step", [](BatchedLangevin &b, Arr noise) {
             py::buffer_info bi = noise.request();
             size_check(bi, (long long)b.n_replicas() * b.n_real() * b.n_grid(), "noise ", "n_replicas*n_real*n_grid");
@@ -376,10 +395,7 @@ PYBIND11_MODULE(langevinfts, m) {
                 py::gil_scoped_release nogil;
                 s = b.step((const double *)bi.ptr);
             }
-            py::dict d;
-            d["iterations"] = s.iterations; d["error"] = s.error; d["hamiltonian"] = s.hamiltonian;
-            d["failed"] = s.failed; d["partitions"] = s.partitions;
-            return d;
+            return stats_dict(s);
         });
 
     py::class_<PlatformSelector>(m, "PlatformSelector")

@@ -213,6 +213,41 @@ __global__ void __launch_bounds__(NTHR) k_xpass(GridPlan g, const lfts_step_job 
     }
 }
 
+// Forward x-transform only (no bond factor, no inverse) of one spectrum slot:
+// completes the r2c 3D transform that k_plane_forward<T, 1> began.
+template <typename T, bool GEN>
+__global__ void __launch_bounds__(NTHR) k_xpass_forward(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_in0,
+                                                        int TJ) {
+    using C = typename CT<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n0 = g.n0;
+    C *tile = (C *)smem_raw;
+    C *twx = tile + n0 * TJ;
+    short *px = (short *)(twx + n0);
+    const lfts_step_job jb = jobs[blockIdx.y];
+    if (jb.active && !jb.active[jb.replica]) return;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < n0; i += NTHR) { twx[i] = ((const C *)g.tw[0])[i]; px[i] = g.perm[0][i]; }
+    __syncthreads();
+    const long long plane = (long long)g.n1 * g.nzc;
+    const long long j0 = (long long)blockIdx.x * TJ;
+    const int tot = n0 * TJ;
+    C *spec = (C *)jb.spec + (size_t)spec_in0 * g.Mc;
+    for (int i = tid; i < tot; i += NTHR) {
+        const int jj = i % TJ, x = i / TJ;
+        C v = cmk<C>(0, 0);
+        if (j0 + jj < plane) v = spec[x * plane + j0 + jj];
+        tile[px[x] * TJ + jj] = v;
+    }
+    __syncthreads();
+    const LineMap lmx = {TJ, TJ, n0 * TJ, TJ};
+    dit_lines<C, true, GEN>(tile, lmx, g.ax[0], twx, -1, tid, NTHR);
+    for (int i = tid; i < tot; i += NTHR) {
+        const int jj = i % TJ, x = i / TJ;
+        if (j0 + jj < plane) spec[x * plane + j0 + jj] = tile[x * TJ + jj];
+    }
+}
+
 // inverse y transform of NBR planes loaded from spec (natural -> perm rows)
 template <typename T, int NBR, bool GEN>
 __device__ __forceinline__ void load_and_inverse_y(const GridPlan &g, const lfts_step_job &jb, int spec_in0,

@@ -313,3 +313,41 @@ class BatchedLFTS:
 
     def fields(self):
         return self.engine.get_fields(self.S)
+
+    def sf_pairs(self):
+        """Monomer-type index pairs of the structure function, in the order
+        lfts.py:665-668 builds its dictionary."""
+        import itertools
+        return [tuple(sorted(p)) for p in itertools.combinations_with_replacement(range(self.S), 2)]
+
+    def accumulate_structure_function(self):
+        """Add this step's <u(k) phi(-k)> of every replica to the device sums
+        (lfts.py:753-767): phi_i and the auxiliary fields 0..S-2 are transformed
+        on the device, mu_i = sum_k F[w_aux_k] A_inv[k, i] / eigenvalue_k / M."""
+        coef = np.array([[self.mpt.matrix_a_inv[k, i] / self.mpt.eigenvalues[k] / self.M for i in range(self.S)]
+                         for k in range(self.S - 1)], dtype=np.float64).reshape(max(self.S - 1, 1), self.S)
+        self.engine.sf_accumulate(np.ascontiguousarray(coef), [v for p in self.sf_pairs() for v in p])
+
+    def structure_function(self, reset=True):
+        """The accumulated sums, {"A,B": complex [R, nx, ny, nz//2+1]} (the
+        reference's sf_average before its recording scale, lfts.py:780-782)."""
+        nx = list(self.cb.get_nx())
+        shape_k = nx[:-1] + [nx[-1] // 2 + 1]
+        sf = self.engine.get_structure_function(shape_k, reset)
+        return {self.monomer_types[a] + "," + self.monomer_types[b]: sf[:, p] for p, (a, b) in enumerate(self.sf_pairs())}
+
+    def h_deriv_chin(self, stats):
+        """dH/dchiN of every replica (lfts.py:265-274) from the field moments that
+        find_saddle_point / step return."""
+        mean = np.reshape(stats["aux_mean"], [self.R, self.S])
+        msq = np.reshape(stats["aux_msq"], [self.R, self.S])
+        out = []
+        for r in range(self.R):
+            dH = {}
+            for key in self.chi_n:
+                dH[key] = self.mpt.h_const_deriv_chin[key]
+                for i in range(self.S - 1):
+                    dH[key] += self.mpt.h_coef_mu2_deriv_chin[key][i] * msq[r, i]
+                    dH[key] += self.mpt.h_coef_mu1_deriv_chin[key][i] * mean[r, i]
+            out.append(dH)
+        return out
