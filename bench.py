@@ -211,7 +211,9 @@ def step_traffic_per_job(s_bytes):
 def roofline_step_kernel(nx, njobs, reps=20):
     """Time lfts_step_continuous at the batch shape of the workload (njobs =
     replicas x propagators per schedule slot) with CUDA events on its stream.
-    Inputs (njobs * 2 MB propagator slices) exceed the 126 MB L2."""
+    Every job has its own field factors, as the two keys of a slot of each
+    replica do; inputs, outputs, factors and spectra (njobs x 10 MB at 64^3)
+    exceed the 126 MB L2."""
     import torch
     from langevinfts_b200.capi import Context, StepJob, check
     ctx = Context([nx] * 3, precision=8)
@@ -219,16 +221,16 @@ def roofline_step_kernel(nx, njobs, reps=20):
     lx = (C.c_double * 3)(7.3, 7.3, 7.3)
     bond, bondh = ctx.malloc(Mc * 8), ctx.malloc(Mc * 8)
     check(ctx.lib.lfts_bond_tables(ctx.h, 1.0, 1 / 90, lx, bond, bondh))
-    w = ctx.upload(np.random.default_rng(0).normal(0, 1, M))
-    fac = ctx.malloc(M * 8)
-    check(ctx.lib.lfts_field_factors(ctx.h, w, -1 / 360, fac))
+    w = ctx.upload(np.random.default_rng(0).normal(0, 1, njobs * M))
+    fac = ctx.malloc(njobs * M * 8)
+    check(ctx.lib.lfts_field_factors_batch(ctx.h, w, -1 / 360, fac, njobs))
     q = ctx.malloc(njobs * 2 * M * 8)
     check(ctx.lib.lfts_memset_async(ctx.h, q, 0, njobs * 2 * M * 8))
     ones = np.ones(M)
     for j in range(njobs):
         ctx.h2d(q + j * 2 * M * 8, ones)
     spec = ctx.malloc(njobs * 2 * Mc * 16)
-    jobs = (StepJob * njobs)(*[StepJob(q + j * 2 * M * 8, 0, q + (j * 2 + 1) * M * 8, 0, fac, bond, bondh,
+    jobs = (StepJob * njobs)(*[StepJob(q + j * 2 * M * 8, 0, q + (j * 2 + 1) * M * 8, 0, fac + j * M * 8, bond, bondh,
                                        spec + j * 2 * Mc * 16, None, 0, 0) for j in range(njobs)])
     jp = ctx.upload(np.frombuffer(jobs, dtype=np.uint8))
     stream = torch.cuda.ExternalStream(ctx.lib.lfts_ctx_stream(ctx.h))
