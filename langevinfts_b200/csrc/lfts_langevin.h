@@ -53,6 +53,12 @@ class BatchedLangevin {
     // Same, with this step's noise already on the device ([R][n_real][M] doubles)
     SaddleStats step_device(const double *noise_dev);
     void *stream() const { return lfts_ctx_stream(ctx_); }
+    // The previous step's noise of every replica ([R][n_real][M] host doubles),
+    // the state the Leimkuhler-Matthews update carries between steps
+    // (normal_noise_prev of lfts.py:569-629): read for a checkpoint, written on
+    // resume.
+    void get_noise_prev(double *out) const;
+    void set_noise_prev(const double *in);
     // Structure function of every replica (examples/fts/lfts.py:753-767):
     //   sf[r][p] += mu_a conj(phi_b / M),  mu_a = sum_{q < S-1} F[w_aux_q] coef[q][a],
     // for the type pairs p = (pairs[2p], pairs[2p+1]); coef (host, (S-1) x S) =

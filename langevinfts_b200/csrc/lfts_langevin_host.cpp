@@ -286,6 +286,13 @@ SaddleStats BatchedLangevin::step_device(const double *noise_dev) {
     return find_saddle_point(true);
 }
 
+void BatchedLangevin::get_noise_prev(double *out) const {
+    if (Rr_ > 0) check_rc(lfts_memcpy_d2h(ctx_, out, xi_[xi_cur_].get(), sizeof(double) * (size_t)R_ * Rr_ * M_));
+}
+void BatchedLangevin::set_noise_prev(const double *in) {
+    if (Rr_ > 0) check_rc(lfts_memcpy_h2d(ctx_, xi_[xi_cur_].get(), in, sizeof(double) * (size_t)R_ * Rr_ * M_));
+}
+
 long long BatchedLangevin::n_complex_grid() const {
     long long M = 0, Mc = 0;
     check_rc(lfts_ctx_info(ctx_, &M, &Mc, nullptr));

@@ -372,6 +372,16 @@ PYBIND11_MODULE(langevinfts, m) {
             }
             return stats_dict(s);
         })
+        .def("get_noise_prev", [](BatchedLangevin &b) {
+            py::array_t<double> xi({(py::ssize_t)b.n_replicas(), (py::ssize_t)b.n_real(), (py::ssize_t)b.n_grid()});
+            b.get_noise_prev((double *)xi.request().ptr);
+            return xi;
+        })
+        .def("set_noise_prev", [](BatchedLangevin &b, Arr xi) {
+            py::buffer_info bi = xi.request();
+            size_check(bi, (long long)b.n_replicas() * b.n_real() * b.n_grid(), "normal_noise_prev ", "n_replicas*n_real*n_grid");
+            b.set_noise_prev((const double *)bi.ptr);
+        })
         .def("sf_accumulate", [](BatchedLangevin &b, Arr coef, std::vector<int> pairs) {
             py::buffer_info bi = coef.request();
             if (bi.ndim != 2) throw std::runtime_error("coef must be a (S-1) x S array");

@@ -282,6 +282,8 @@ class BatchedLFTS:
         }
         self.engine = module.BatchedLangevin(factory, self.cb, self.molecules, self.analyzer, self.R, cfg)
         self._pool = None
+        self.params = params
+        self.langevin_step = 0
 
     def start(self, initial_fields):
         """initial_fields: list (per replica) of {monomer type: field}."""
@@ -309,10 +311,70 @@ class BatchedLFTS:
     def step(self, noise=None):
         if noise is None:
             noise = self.draw_noise()
-        return self.engine.step(noise)
+        stats = self.engine.step(noise)
+        self.langevin_step += 1
+        return stats
 
     def fields(self):
         return self.engine.get_fields(self.S)
+
+    def save_simulation_data(self, paths):
+        """Write one checkpoint per replica, paths[r], with the keys and layout of
+        the reference driver's save_simulation_data (lfts.py:569-600): monomer
+        fields, concentrations, the replica's PCG64 state, the step count and
+        the previous step's noise.  Either driver can continue from it."""
+        from scipy.io import savemat
+        if len(paths) != self.R:
+            raise ValueError("one path per replica")
+        w_aux = self.fields()
+        phi = self.engine.get_concentrations(self.S)
+        noise_prev = self.engine.get_noise_prev()
+        for r, path in enumerate(paths):
+            w = self.mpt.to_monomer_fields(w_aux[r])
+            state = self.rngs[r].bit_generator.state
+            mdic = {
+                "initial_params": self.params,
+                "dim": self.cb.get_dim(), "nx": self.cb.get_nx(), "lx": self.cb.get_lx(),
+                "monomer_types": self.monomer_types, "chi_n": dict(self.chi_n),
+                "chain_model": self.params["chain_model"], "ds": self.params["ds"],
+                "dt": self.params["langevin"]["dt"], "nbar": self.params["langevin"]["nbar"],
+                "eigenvalues": self.mpt.eigenvalues,
+                "aux_fields_real": self.mpt.aux_fields_real_idx, "aux_fields_imag": self.mpt.aux_fields_imag_idx,
+                "matrix_a": self.mpt.matrix_a, "matrix_a_inverse": self.mpt.matrix_a_inv,
+                "langevin_step": self.langevin_step,
+                "random_generator": state["bit_generator"],
+                "random_state_state": str(state["state"]["state"]),
+                "random_state_inc": str(state["state"]["inc"]),
+                "normal_noise_prev": noise_prev[r]}
+            for i, name in enumerate(self.monomer_types):
+                mdic["w_" + name] = w[i]
+                mdic["phi_" + name] = phi[r, i]
+            savemat(path, mdic, long_field_names=True, do_compression=True)
+
+    def continue_run(self, paths):
+        """Resume every replica from a checkpoint (lfts.py:602-629): restore its
+        PCG64 state, fields and previous noise, then find the saddle point as
+        the reference's run() does before its first step.  Returns those
+        statistics; the next step() is step langevin_step + 1."""
+        from scipy.io import loadmat
+        if len(paths) != self.R:
+            raise ValueError("one path per replica")
+        fields, noise_prev, steps = [], np.zeros([self.R, self.mpt.R, self.M]), set()
+        for r, path in enumerate(paths):
+            d = loadmat(path, squeeze_me=True)
+            self.rngs[r].bit_generator.state = {
+                "bit_generator": "PCG64",
+                "state": {"state": int(d["random_state_state"]), "inc": int(d["random_state_inc"])},
+                "has_uint32": 0, "uinteger": 0}
+            fields.append({name: np.array(d["w_" + name]) for name in self.monomer_types})
+            noise_prev[r] = np.reshape(d["normal_noise_prev"], [self.mpt.R, self.M])
+            steps.add(int(d["langevin_step"]))
+        if len(steps) != 1:
+            raise ValueError("the checkpoints are at different Langevin steps")
+        stats = self.start(fields)
+        self.engine.set_noise_prev(noise_prev)
+        self.langevin_step = steps.pop()
+        return stats
 
     def sf_pairs(self):
         """Monomer-type index pairs of the structure function, in the order
