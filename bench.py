@@ -35,6 +35,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Langevin steps/s @ saddle err 1e-4 (batched L-FTS, plain FP64)"
+METRIC_FP32 = "Langevin steps/s @ saddle err 1e-4 (batched L-FTS, FP32 propagators, FP64 reductions)"
 UNIT = "replica-steps/s"
 # mean saddle-point iterations per Langevin step of this workload, measured by
 # the GPU arm on B200 (the algorithm and inputs are the reference's, so the
@@ -208,7 +209,7 @@ def step_traffic_per_job(s_bytes):
     return None
 
 
-def roofline_step_kernel(nx, njobs, reps=20):
+def roofline_step_kernel(nx, njobs, reps=20, prec=8):
     """Time lfts_step_continuous at the batch shape of the workload (njobs =
     replicas x propagators per schedule slot) with CUDA events on its stream.
     Every job has its own field factors, as the two keys of a slot of each
@@ -216,22 +217,23 @@ def roofline_step_kernel(nx, njobs, reps=20):
     exceed the 126 MB L2."""
     import torch
     from langevinfts_b200.capi import Context, StepJob, check
-    ctx = Context([nx] * 3, precision=8)
+    ctx = Context([nx] * 3, precision=prec)
     M, Mc = ctx.M, ctx.Mc
+    sb = prec  # bytes per real
     lx = (C.c_double * 3)(7.3, 7.3, 7.3)
-    bond, bondh = ctx.malloc(Mc * 8), ctx.malloc(Mc * 8)
+    bond, bondh = ctx.malloc(Mc * sb), ctx.malloc(Mc * sb)
     check(ctx.lib.lfts_bond_tables(ctx.h, 1.0, 1 / 90, lx, bond, bondh))
     w = ctx.upload(np.random.default_rng(0).normal(0, 1, njobs * M))
-    fac = ctx.malloc(njobs * M * 8)
+    fac = ctx.malloc(njobs * M * sb)
     check(ctx.lib.lfts_field_factors_batch(ctx.h, w, -1 / 360, fac, njobs))
-    q = ctx.malloc(njobs * 2 * M * 8)
-    check(ctx.lib.lfts_memset_async(ctx.h, q, 0, njobs * 2 * M * 8))
-    ones = np.ones(M)
+    q = ctx.malloc(njobs * 2 * M * sb)
+    check(ctx.lib.lfts_memset_async(ctx.h, q, 0, njobs * 2 * M * sb))
+    ones = np.ones(M, dtype=np.float64 if prec == 8 else np.float32)
     for j in range(njobs):
-        ctx.h2d(q + j * 2 * M * 8, ones)
-    spec = ctx.malloc(njobs * 2 * Mc * 16)
-    jobs = (StepJob * njobs)(*[StepJob(q + j * 2 * M * 8, 0, q + (j * 2 + 1) * M * 8, 0, fac + j * M * 8, bond, bondh,
-                                       spec + j * 2 * Mc * 16, None, 0, 0) for j in range(njobs)])
+        ctx.h2d(q + j * 2 * M * sb, ones)
+    spec = ctx.malloc(njobs * 2 * Mc * 2 * sb)
+    jobs = (StepJob * njobs)(*[StepJob(q + j * 2 * M * sb, 0, q + (j * 2 + 1) * M * sb, 0, fac + j * M * sb, bond, bondh,
+                                       spec + j * 2 * Mc * 2 * sb, None, 0, 0) for j in range(njobs)])
     jp = ctx.upload(np.frombuffer(jobs, dtype=np.uint8))
     stream = torch.cuda.ExternalStream(ctx.lib.lfts_ctx_stream(ctx.h))
     for _ in range(3):
@@ -267,7 +269,7 @@ def run_ours(args):
     p = params(args.nx)
     seeds = [1000 + rank * R + r for r in range(R)]
     f = L.PlatformSelector.create_factory("cuda", False)
-    sim = BatchedLFTS(p, seeds, module=L)
+    sim = BatchedLFTS(p, seeds, module=L, platform="cuda" if args.precision == "fp64" else "cuda-fp32")
     M = sim.M
     st0 = sim.start([initial_fields(s, M) for s in seeds])
     for _ in range(args.warmup):
@@ -330,14 +332,14 @@ def run_ours(args):
                      f"failed {fails}, launches {launches}\n")
     # ---- roofline of the fused continuous step at the workload batch shape
     njobs = 2 * R  # two propagators per schedule slot (A and B side) per replica
-    ms, Mg, Mcg = roofline_step_kernel(args.nx, njobs)
+    s_bytes = 8 if args.precision == "fp64" else 4
+    ms, Mg, Mcg = roofline_step_kernel(args.nx, njobs, prec=s_bytes)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    s_bytes = 8
     unit_bytes = s_bytes * (12 * Mg + 24 * Mcg)  # pass-model bytes per (replica, key, contour step)
     achieved = njobs * unit_bytes / (ms * 1e-3) / 1e9
     traffic = step_traffic_per_job(s_bytes) if args.nx == 64 else None
@@ -355,9 +357,9 @@ def run_ours(args):
                    "sample": f"2 saddle-point iterations of 1 replica (64^3, N=90) on the reference CPU platform "
                              f"(first discarded), {r[0]:.2f} s/iteration x {mean_iters:.1f} iterations per step measured above"}
     out = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "metric": METRIC if args.precision == "fp64" else METRIC_FP32, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
+        "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
         "config": {"workload": f"batched L-FTS: {R} replicas/GPU of AB diblock f=0.5 chiN=17 nbar=100 N=90, "
                                f"{args.nx}^3 box 7.3, dt=0.8, saddle tol 1e-4, AM max_hist 20",
                    "replicas_per_gpu": R, "grid": [args.nx] * 3, "N": 90, "parallelism": f"replicas x{world}",
@@ -370,7 +372,7 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "lfts_step_continuous (5 fused FFT-pass kernels)",
                      "launch_ms": ms, "jobs_per_launch": njobs,
-                     "bytes_model": "8*(12M+24Mc) per job (pass model), peak = measured hbm_gbs"},
+                     "bytes_model": f"{s_bytes}*(12M+24Mc) per job (pass model), peak = measured hbm_gbs"},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
@@ -388,6 +390,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--nx", type=int, default=64)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="fp64 (the headline) or fp32 propagators with FP64 reductions (platform cuda-fp32)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--threads", type=int, default=1, help=argparse.SUPPRESS)
@@ -401,8 +405,9 @@ def main():
     if args.kernel_only:
         import torch
         torch.cuda.init()
-        ms, M, Mc = roofline_step_kernel(args.nx, 2 * args.replicas, reps=args.steps)
-        unit = 8 * (12 * M + 24 * Mc)
+        sb = 8 if args.precision == "fp64" else 4
+        ms, M, Mc = roofline_step_kernel(args.nx, 2 * args.replicas, reps=args.steps, prec=sb)
+        unit = sb * (12 * M + 24 * Mc)
         print(json.dumps({"kernel": "lfts_step_continuous", "jobs": 2 * args.replicas, "nx": args.nx, "launch_ms": ms,
                           "pass_model_GBps": 2 * args.replicas * unit / (ms * 1e-3) / 1e9}))
         return 0
