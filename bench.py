@@ -267,7 +267,8 @@ def run_ours(args):
 
     R = args.replicas
     p = params(args.nx)
-    seeds = [1000 + rank * R + r for r in range(R)]
+    from langevinfts_b200.ensemble import max_over_ranks, replica_seeds
+    seeds = replica_seeds(rank, R)
     f = L.PlatformSelector.create_factory("cuda", False)
     sim = BatchedLFTS(p, seeds, module=L, platform="cuda" if args.precision == "fp64" else "cuda-fp32")
     M = sim.M
@@ -318,10 +319,7 @@ def run_ours(args):
     ev2[1].synchronize()
     t_e2e = max(time.perf_counter() - e0, ev2[0].elapsed_time(ev2[1]) / 1000.0)
     ex.shutdown(wait=False)
-    if dist is not None:
-        tt = torch.tensor([t, t_e2e], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t, t_e2e = float(tt[0]), float(tt[1])
+    t, t_e2e = max_over_ranks([t, t_e2e])
     value = world * R * args.steps / t
     e2e = world * R * args.steps / t_e2e
     if rank != 0:
