@@ -147,8 +147,8 @@ template <typename T, int N> static int fast_setup(int max_smem) {
 template <typename T> static int r8_setup(int max_smem) {
     using C = typename CT<T>::type;
     if (r8::plane_smem<C>() > (size_t)max_smem || r8::xpass_smem<C>() > (size_t)max_smem) return 0;
-    if (allow_smem(r8::kr_plane_forward<T, 1>, max_smem) != cudaSuccess) return 0;
-    if (allow_smem(r8::kr_plane_forward<T, 2>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r8::kr_plane_forward<T, 1, FM_NONE, FM_NONE>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r8::kr_plane_mid<T>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r8::kr_plane_inverse<T, 2, EPI_RICH>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r8::kr_plane_inverse<T, 1, EPI_SCALE>, max_smem) != cudaSuccess) return 0;
@@ -520,7 +520,7 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
             }
             const long long it2 = (long long)nj * 2 * r8::XTILES, it1 = (long long)nj * r8::XTILES, cap = 3LL * c->nsm;
             const dim3 px2((unsigned)(it2 < cap ? it2 : cap)), px1((unsigned)(it1 < cap ? it1 : cap));
-            r8::kr_plane_forward<T, 2><<<rp, NTHR, ps, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0);
+            r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC><<<rp, NTHR, ps, st>>>(g, jobs, s, 0);
             r8::kp_xpass<T, 2><<<px2, NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, 0, 1);
             r8::kr_plane_mid<T><<<rp, NTHR, ps, st>>>(g, jobs, 1);
             r8::kp_xpass<T, 1><<<px1, NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 1, 1, 1);
@@ -550,7 +550,7 @@ static int step_disc_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, 
         if (c->r8) {
             const dim3 rp(N, nj), rx(r8::PLANE / r8::GROUPS, nj);
             const size_t ps = r8::plane_smem<C>(), xs = r8::xpass_smem<C>();
-            r8::kr_plane_forward<T, 1><<<rp, NTHR, ps, st>>>(g, jobs, s, FM_NONE, 0, 0);
+            r8::kr_plane_forward<T, 1, FM_NONE, FM_NONE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0);
             const dim3 bx(r8::PLANE / r8::XT, nj);
             if (c->r8 == 2) {
                 const size_t p1 = r8::kb_plane_smem<C>(false);

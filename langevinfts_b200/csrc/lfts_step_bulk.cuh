@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(NTHR, 2) kb_plane_inverse(GridPlan g, const lf
             for (int k = 0; k < 8; k++) {
                 T *f = fst + y * FS + j + 8 * k;
                 const T eh = *f;
-                *f = ((T)4 * eh * a[k].y - eh * eh * a[k].x) / (T)3;
+                *f = ((T)4 * eh * a[k].y - eh * eh * a[k].x) * (T)(1.0 / 3.0);
             }
         }
     } else {

@@ -239,10 +239,13 @@ __device__ __forceinline__ void y_inverse_paired(C *P, int kz, int j, C wi, unsi
 // K1: forward zy transform of one x-plane.
 //   NBR = 2: spectra of f0(fac) q and f1(fac) q (slots spec_out0, +1);
 //   NBR = 1: spectrum of f0(fac) q (slot spec_out0).
-template <typename T, int NBR>
+// The factor modes are template arguments (FM0, FM1): the continuous step
+// uses <2, FM_FAC_SQ, FM_FAC>, the discrete step <1, FM_NONE, FM_NONE>.
+template <typename T, int NBR, int FM0, int FM1>
 __global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_forward(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
-                                                            int fm0, int fm1, int spec_out0) {
+                                                                       int spec_out0) {
     using C = typename CT<T>::type;
+    constexpr int fm0 = FM0, fm1 = FM1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;
     const lfts_step_job jb = jobs[blockIdx.y];
@@ -479,10 +482,10 @@ __global__ void __launch_bounds__(NTHR, 3) kp_xpass(GridPlan g, const lfts_step_
     C *stage = (C *)smem_raw;
     uint64_t *bar = (uint64_t *)(stage + 2 * N * XT);
     const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-    const long long nitems = (long long)nj * NBR * XTILES;
+    const int nitems = nj * NBR * XTILES;  // < 2^31 for nj <= 65535
     // first item at or after it whose job is active and aligned (>= nitems: none)
-    auto next_item = [&](long long it) -> long long {
-        for (; it < nitems; it += gridDim.x) {
+    auto next_item = [&](int it) -> int {
+        for (; it < nitems; it += (int)gridDim.x) {
             const lfts_step_job &jb = jobs[it / (NBR * XTILES)];
             if (jb.active && !jb.active[jb.replica]) continue;
             if (((uintptr_t)jb.spec | (uintptr_t)g.Mc * sizeof(C)) & 15) {
@@ -494,18 +497,18 @@ __global__ void __launch_bounds__(NTHR, 3) kp_xpass(GridPlan g, const lfts_step_
         return nitems;
     };
     // spectrum column block of an item: rows x at + x * PLANE
-    auto item_base = [&](long long it) -> C * {
-        const int job = (int)(it / (NBR * XTILES)), rem = (int)(it - (long long)job * NBR * XTILES);
+    auto item_base = [&](int it) -> C * {
+        const int job = it / (NBR * XTILES), rem = it - job * (NBR * XTILES);
         const int b = rem / XTILES, t = rem - b * XTILES;
         return (C *)jobs[job].spec + (size_t)(spec_in0 + b) * g.Mc + (size_t)t * XT;
     };
-    auto issue_load = [&](long long it, int st) {  // warp 0
+    auto issue_load = [&](int it, int st) {  // warp 0
         C *src = item_base(it);
         if (l == 0) mbar_arrive_expect_tx(bar + st, TILEB);
         __syncwarp();
         for (int r = l; r < N; r += 32) bulk_load(stage + (st * N + r) * XT, src + (size_t)r * PLANE, ROWB, bar + st);
     };
-    long long cur = next_item(blockIdx.x);
+    int cur = next_item(blockIdx.x);
     if (cur >= nitems) return;
     if (tid == 0) {
         mbar_init(bar, 1);
@@ -516,13 +519,13 @@ __global__ void __launch_bounds__(NTHR, 3) kp_xpass(GridPlan g, const lfts_step_
     const C wf = tw_base<C>(w, -1), wi = tw_base<C>(w, +1);
     for (int u = 0; cur < nitems; u++) {
         const int st = u & 1;
-        const long long nxt = next_item(cur + gridDim.x);
+        const int nxt = next_item(cur + (int)gridDim.x);
         if (w == 0 && nxt < nitems) {
             bulk_wait_read();  // the previous store out of stage st ^ 1 has read it
             __syncwarp();
             issue_load(nxt, st ^ 1);
         }
-        const int job = (int)(cur / (NBR * XTILES)), rem = (int)(cur - (long long)job * NBR * XTILES);
+        const int job = cur / (NBR * XTILES), rem = cur - job * (NBR * XTILES);
         const int b = rem / XTILES, t = rem - b * XTILES;
         const lfts_step_job &jb = jobs[job];
         const T *bt = (const T *)((b == 0 ? bsel0 : bsel1) ? jb.bond_half : jb.bond) + t * XT + l;
@@ -622,6 +625,7 @@ __global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_inverse(GridPlan 
     const long long poff = (long long)x * N * N;
     const T *fac = (const T *)jb.fac + poff;
     T *qout = (T *)jb.out + s * jb.out_stride + poff;
+    const T THIRD = (T)(1.0 / 3.0);  // multiply, not divide: no iterative division per element
     if (NBR == 2) {
         {
             // branch 0 first; its inverse column waits in column xkz while
@@ -668,7 +672,7 @@ __global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_inverse(GridPlan 
             __syncwarp(mask);
             fft64<+1>(a, RowX<C>{P + y * PR}, j, wi, mask);
 #pragma unroll
-            for (int k = 0; k < 8; k++) qout[y * N + j + 8 * k] = ((T)4 * eh[k] * a[k].y - eh[k] * eh[k] * a[k].x) / (T)3;
+            for (int k = 0; k < 8; k++) qout[y * N + j + 8 * k] = ((T)4 * eh[k] * a[k].y - eh[k] * eh[k] * a[k].x) * THIRD;
         }
     } else {
         y_inverse_paired(P, grp, j, wi, mask, in);
