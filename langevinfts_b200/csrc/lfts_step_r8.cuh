@@ -132,7 +132,9 @@ template <typename C>
 __device__ __forceinline__ void put_columns(C *st, int kz, const C (&c)[8], int j, int lane, unsigned mask) {
     if (kz != 0) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) st[(j + 8 * k) * NZC + kz] = c[k];
+        C *col = st + j * NZC + kz;  // rows j + 8k at constant offsets
+#pragma unroll
+        for (int k = 0; k < 8; k++) col[8 * k * NZC] = c[k];
     } else {
         C p[8];
         herm_partner(c, p, j, lane, mask);
@@ -140,8 +142,9 @@ __device__ __forceinline__ void put_columns(C *st, int kz, const C (&c)[8], int 
         for (int k = 0; k < 8; k++) {
             C a, b;
             split_pair(c[k], cconj(p[k]), a, b);
-            st[(j + 8 * k) * NZC] = a;
-            st[(j + 8 * k) * NZC + N / 2] = b;
+            C *row = st + (j + 8 * k) * NZC;
+            row[0] = a;
+            row[N / 2] = b;
         }
     }
 }
@@ -152,11 +155,14 @@ template <typename C>
 __device__ __forceinline__ void get_columns(const C *st, int kz, C (&c)[8], int j) {
     if (kz != 0) {
 #pragma unroll
-        for (int m = 0; m < 8; m++) c[m] = st[(j + 8 * m) * NZC + kz];
+        const C *col = st + j * NZC + kz;
+#pragma unroll
+        for (int m = 0; m < 8; m++) c[m] = col[8 * m * NZC];
     } else {
 #pragma unroll
         for (int m = 0; m < 8; m++) {
-            const C a = st[(j + 8 * m) * NZC], b = st[(j + 8 * m) * NZC + N / 2];
+            const C *row = st + (j + 8 * m) * NZC;
+            const C a = row[0], b = row[N / 2];
             c[m].x = a.x - b.y;
             c[m].y = a.y + b.x;
         }
@@ -260,11 +266,12 @@ __global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_forward(GridPlan 
     if (NBR == 2) {
         // z-lines: row y, branches packed as real / imaginary part
         for (int y = grp; y < N; y += GROUPS) {
+            const T *qrow = qin + y * N + j, *frow = fac + y * N + j;  // elements j + 8m at constant offsets
             T qv[8], fv[8];
 #pragma unroll
             for (int m = 0; m < 8; m++) {
-                qv[m] = qin[y * N + j + 8 * m];
-                fv[m] = fm0 == FM_NONE ? (T)1 : fac[y * N + j + 8 * m];
+                qv[m] = qrow[8 * m];
+                fv[m] = fm0 == FM_NONE ? (T)1 : frow[8 * m];
             }
             C a[8];
 #pragma unroll
@@ -581,11 +588,12 @@ __global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_mid(GridPlan g, c
     __syncthreads();
     {
         const int u = grp;
+        const T *frow = fac + u * N + j;
         T ea[8], eb[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-            ea[k] = fac[u * N + j + 8 * k];
-            eb[k] = fac[(u + 32) * N + j + 8 * k];
+            ea[k] = frow[8 * k];
+            eb[k] = frow[32 * N + 8 * k];
         }
         C a[8];
 #pragma unroll
@@ -663,16 +671,18 @@ __global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_inverse(GridPlan 
         }
         __syncthreads();
         for (int y = grp; y < N; y += GROUPS) {
+            const T *frow = fac + y * N + j;
+            T *qrow = qout + y * N + j;
             T eh[8];
 #pragma unroll
-            for (int k = 0; k < 8; k++) eh[k] = fac[y * N + j + 8 * k];
+            for (int k = 0; k < 8; k++) eh[k] = frow[8 * k];
             C a[8];
 #pragma unroll
             for (int m = 0; m < 8; m++) a[m] = P[y * PR + 9 * m + j];
             __syncwarp(mask);
             fft64<+1>(a, RowX<C>{P + y * PR}, j, wi, mask);
 #pragma unroll
-            for (int k = 0; k < 8; k++) qout[y * N + j + 8 * k] = ((T)4 * eh[k] * a[k].y - eh[k] * eh[k] * a[k].x) * THIRD;
+            for (int k = 0; k < 8; k++) qrow[8 * k] = ((T)4 * eh[k] * a[k].y - eh[k] * eh[k] * a[k].x) * THIRD;
         }
     } else {
         y_inverse_paired(P, grp, j, wi, mask, in);
