@@ -518,7 +518,7 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
                 CKLAUNCH();
                 return 0;
             }
-            const long long it2 = (long long)nj * 2 * r8::XTILES, it1 = (long long)nj * r8::XTILES, cap = 3LL * c->nsm;
+            const long long it2 = (long long)nj * 2 * r8::xpipe_tiles<C>(), it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = 3LL * c->nsm;
             const dim3 px2((unsigned)(it2 < cap ? it2 : cap)), px1((unsigned)(it1 < cap ? it1 : cap));
             r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC><<<rp, NTHR, ps, st>>>(g, jobs, s, 0);
             r8::kp_xpass<T, 2><<<px2, NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, 0, 1);
@@ -560,7 +560,7 @@ static int step_disc_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, 
                 CKLAUNCH();
                 return 0;
             }
-            const long long it1 = (long long)nj * r8::XTILES, cap = 3LL * c->nsm;
+            const long long it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = 3LL * c->nsm;
             r8::kp_xpass<T, 1><<<(unsigned)(it1 < cap ? it1 : cap), NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, half, half);
             r8::kr_plane_inverse<T, 1, EPI_SCALE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
             CKLAUNCH();

@@ -27,6 +27,9 @@
 #ifndef LFTS_R8_MINB
 #define LFTS_R8_MINB 2
 #endif
+#ifndef LFTS_R8_MINB_F32
+#define LFTS_R8_MINB_F32 4
+#endif
 
 namespace lfts {
 namespace r8 {
@@ -248,7 +251,7 @@ __device__ __forceinline__ void y_inverse_paired(C *P, int kz, int j, C wi, unsi
 // The factor modes are template arguments (FM0, FM1): the continuous step
 // uses <2, FM_FAC_SQ, FM_FAC>, the discrete step <1, FM_NONE, FM_NONE>.
 template <typename T, int NBR, int FM0, int FM1>
-__global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_forward(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
+__global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFTS_R8_MINB)) kr_plane_forward(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
                                                                        int spec_out0) {
     using C = typename CT<T>::type;
     constexpr int fm0 = FM0, fm1 = FM1;
@@ -477,17 +480,45 @@ __global__ void __launch_bounds__(NTHR, 3) kb_xpass(GridPlan g, const lfts_step_
 // tile); each CTA walks items blockIdx.x, + gridDim.x, ... with two shared
 // stages, so the bulk load of its next item and the bulk store of its previous
 // one run while it transforms the current one.  Warp 0 issues all copies.
-constexpr int XTILES = PLANE / XT;
-template <typename C> constexpr size_t xpipe_smem() { return 2 * sizeof(C) * (size_t)N * XT + 16; }
+// columns per thread: 2 in FP32 (items of 64 columns, 512-byte row copies and
+// twice the work per barrier), 1 in FP64 (32 columns, 512-byte rows)
+template <typename C> __host__ __device__ constexpr int xpipe_cpt() { return sizeof(C) == 8 ? 2 : 1; }
+template <typename C> __host__ __device__ constexpr int xpipe_width() { return XT * xpipe_cpt<C>(); }
+template <typename C> __host__ __device__ constexpr int xpipe_tiles() { return PLANE / xpipe_width<C>(); }
+template <typename C> constexpr size_t xpipe_smem() { return 2 * sizeof(C) * (size_t)N * xpipe_width<C>() + 16; }
+static_assert(PLANE % (2 * XT) == 0, "64-column items cover the plane exactly");
+
+// fft64_tile for CPT columns per thread (columns l + 32c of a tile of row stride XW)
+template <int SIGN, int CPT, int XW, typename C>
+__device__ __forceinline__ void fft64_tile_n(C (&a)[CPT][8], C *tb, int w, int l, C w1) {
+#pragma unroll
+    for (int c = 0; c < CPT; c++) {
+        SmallDFT<8, C>::run(a[c], SIGN, nullptr, 0);
+        twiddle8(a[c], w1);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < CPT; c++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) tb[(8 * k + w) * XW + l + 32 * c] = a[c][k];
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < CPT; c++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[c][k] = tb[(8 * w + k) * XW + l + 32 * c];
+        SmallDFT<8, C>::run(a[c], SIGN, nullptr, 0);
+    }
+}
 
 template <typename T, int NBR>
 __global__ void __launch_bounds__(NTHR, 3) kp_xpass(GridPlan g, const lfts_step_job *__restrict__ jobs, int nj,
                                                     int spec_in0, int bsel0, int bsel1) {
     using C = typename CT<T>::type;
-    constexpr uint32_t ROWB = XT * sizeof(C), TILEB = N * ROWB;
+    constexpr int CPT = xpipe_cpt<C>(), XW = xpipe_width<C>(), XTILES = xpipe_tiles<C>();
+    constexpr uint32_t ROWB = XW * sizeof(C), TILEB = N * ROWB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *stage = (C *)smem_raw;
-    uint64_t *bar = (uint64_t *)(stage + 2 * N * XT);
+    uint64_t *bar = (uint64_t *)(stage + 2 * N * XW);
     const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
     const int nitems = nj * NBR * XTILES;  // < 2^31 for nj <= 65535
     // first item at or after it whose job is active and aligned (>= nitems: none)
@@ -507,13 +538,13 @@ __global__ void __launch_bounds__(NTHR, 3) kp_xpass(GridPlan g, const lfts_step_
     auto item_base = [&](int it) -> C * {
         const int job = it / (NBR * XTILES), rem = it - job * (NBR * XTILES);
         const int b = rem / XTILES, t = rem - b * XTILES;
-        return (C *)jobs[job].spec + (size_t)(spec_in0 + b) * g.Mc + (size_t)t * XT;
+        return (C *)jobs[job].spec + (size_t)(spec_in0 + b) * g.Mc + (size_t)t * XW;
     };
     auto issue_load = [&](int it, int st) {  // warp 0
         C *src = item_base(it);
         if (l == 0) mbar_arrive_expect_tx(bar + st, TILEB);
         __syncwarp();
-        for (int r = l; r < N; r += 32) bulk_load(stage + (st * N + r) * XT, src + (size_t)r * PLANE, ROWB, bar + st);
+        for (int r = l; r < N; r += 32) bulk_load(stage + (st * N + r) * XW, src + (size_t)r * PLANE, ROWB, bar + st);
     };
     int cur = next_item(blockIdx.x);
     if (cur >= nitems) return;
@@ -535,34 +566,42 @@ __global__ void __launch_bounds__(NTHR, 3) kp_xpass(GridPlan g, const lfts_step_
         const int job = cur / (NBR * XTILES), rem = cur - job * (NBR * XTILES);
         const int b = rem / XTILES, t = rem - b * XTILES;
         const lfts_step_job &jb = jobs[job];
-        const T *bt = (const T *)((b == 0 ? bsel0 : bsel1) ? jb.bond_half : jb.bond) + t * XT + l;
-        T bv[8];
+        const T *bt = (const T *)((b == 0 ? bsel0 : bsel1) ? jb.bond_half : jb.bond) + t * XW + l;
+        T bv[CPT][8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) bv[k] = bt[(w + 8 * k) * PLANE];
+        for (int c = 0; c < CPT; c++)
+#pragma unroll
+            for (int k = 0; k < 8; k++) bv[c][k] = bt[(w + 8 * k) * PLANE + 32 * c];
         if (!mbar_wait(bar + st, (u >> 1) & 1)) {
             mbar_wait(bar + st, (u >> 1) & 1);
             if (w == 0) bulk_wait_read();
             return;
         }
-        C *tb = stage + st * N * XT;
-        C a[8];
+        C *tb = stage + st * N * XW;
+        C a[CPT][8];
 #pragma unroll
-        for (int m = 0; m < 8; m++) a[m] = tb[(w + 8 * m) * XT + l];
-        fft64_tile<-1>(a, tb, w, l, wf);
+        for (int c = 0; c < CPT; c++)
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            a[k].x *= bv[k];
-            a[k].y *= bv[k];
-        }
-        fft64_tile<+1>(a, tb, w, l, wi);
+            for (int m = 0; m < 8; m++) a[c][m] = tb[(w + 8 * m) * XW + l + 32 * c];
+        fft64_tile_n<-1, CPT, XW>(a, tb, w, l, wf);
+#pragma unroll
+        for (int c = 0; c < CPT; c++)
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                a[c][k].x *= bv[c][k];
+                a[c][k].y *= bv[c][k];
+            }
+        fft64_tile_n<+1, CPT, XW>(a, tb, w, l, wi);
         __syncthreads();
 #pragma unroll
-        for (int m = 0; m < 8; m++) tb[(w + 8 * m) * XT + l] = a[m];
+        for (int c = 0; c < CPT; c++)
+#pragma unroll
+            for (int m = 0; m < 8; m++) tb[(w + 8 * m) * XW + l + 32 * c] = a[c][m];
         fence_proxy_async();
         __syncthreads();
         if (w == 0) {
             C *dst = item_base(cur);
-            for (int r = l; r < N; r += 32) bulk_store(dst + (size_t)r * PLANE, tb + r * XT, ROWB);
+            for (int r = l; r < N; r += 32) bulk_store(dst + (size_t)r * PLANE, tb + r * XW, ROWB);
             bulk_commit();
         }
         cur = nxt;
@@ -573,7 +612,7 @@ __global__ void __launch_bounds__(NTHR, 3) kp_xpass(GridPlan g, const lfts_step_
 // ------------------------------------------------------------------------
 // K3: inverse zy, multiply by e = fac^2, forward zy, in place on slot spec_idx
 template <typename T>
-__global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_mid(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_idx) {
+__global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFTS_R8_MINB)) kr_plane_mid(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_idx) {
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;
@@ -618,7 +657,7 @@ __global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_mid(GridPlan g, c
 //   NBR = 2, EPI_RICH: q' = (4 e_h v2 - e_h^2 v1) / 3 (v1 from slot spec_in0);
 //   NBR = 1, EPI_SCALE: q' = f(fac) v.
 template <typename T, int NBR, int EPI>
-__global__ void __launch_bounds__(NTHR, LFTS_R8_MINB) kr_plane_inverse(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
+__global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFTS_R8_MINB)) kr_plane_inverse(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
                                                             int spec_in0, int fm0) {
     static_assert((NBR == 2 && EPI == EPI_RICH) || (NBR == 1 && EPI == EPI_SCALE), "supported epilogues");
     using C = typename CT<T>::type;
