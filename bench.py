@@ -209,6 +209,77 @@ def step_traffic_per_job(s_bytes):
     return None
 
 
+# ---------------------------------------------------------------- single-system statistics
+# compute_statistics of one system through the langevinfts API: configs 1 (32^3
+# diblock) and 3 (48^3 discrete branched mixture), seeded normal fields.
+STAT_CONFIGS = {
+    "config1_32cubed_diblock": {
+        "nx": [32, 32, 32], "lx": [4.0, 4.0, 4.0], "model": "continuous", "ds": 0.01, "bonds": {"A": 1.0, "B": 1.0},
+        "polymers": [(1.0, [["A", 0.5, 0, 1], ["B", 0.5, 1, 2]])], "seed": 1, "sigma": 1.0},
+    "config3_48cubed_branched_discrete": {
+        "nx": [48, 48, 48], "lx": [5.0, 5.0, 5.0], "model": "discrete", "ds": 1 / 60,
+        "bonds": {"A": 1.0, "B": 1.0, "C": 1.0},
+        "polymers": [(0.5, [["A", 20 / 60, 0, 1], ["B", 20 / 60, 0, 2], ["C", 20 / 60, 0, 3]]),
+                     (0.3, [["B", 5 / 60, i, i + 1] for i in range(8)] + [["A", 6 / 60, i, 8 + i] for i in range(1, 9)]),
+                     (0.2, [["A", 30 / 60, 0, 1]])], "seed": 3, "sigma": 2.0},
+}
+
+
+def time_statistics(module, platform, cfg, reps, warm):
+    """Median wall time (s) of compute_statistics and the partition functions."""
+    f = module.PlatformSelector.create_factory(platform, False)
+    cb = f.create_computation_box(cfg["nx"], cfg["lx"])
+    mol = f.create_molecules_information(cfg["model"], cfg["ds"], cfg["bonds"])
+    for vf, blocks in cfg["polymers"]:
+        mol.add_polymer(vf, blocks)
+    pa = f.create_propagator_analyzer(mol, True)
+    solver = f.create_pseudospectral_solver(cb, mol, pa)
+    rng = np.random.Generator(np.random.PCG64(cfg["seed"]))
+    M = cb.get_n_grid()
+    w = {t: rng.normal(0, cfg["sigma"], M) for t in sorted(cfg["bonds"])}
+    for _ in range(warm):
+        solver.compute_statistics(w)
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        solver.compute_statistics(w)
+        ts.append(time.perf_counter() - t0)
+    Q = [solver.get_total_partition(p) for p in range(len(cfg["polymers"]))]
+    return float(np.median(ts)), Q
+
+
+def _reference_statistics_child(name, threads):
+    ref = load_reference()
+    if ref is None:
+        return 1
+    t, Q = time_statistics(ref, "cpu-mkl", STAT_CONFIGS[name], reps=3, warm=1)
+    print(json.dumps([t, Q, threads]))
+    return 0
+
+
+def run_statistics(args):
+    """One JSON line per config: GPU and reference-CPU compute_statistics times."""
+    import resource
+    from langevinfts_b200 import langevinfts as L
+    ncpu = os.cpu_count() or 1
+    for name, cfg in STAT_CONFIGS.items():
+        t_gpu, Q_gpu = time_statistics(L, "cuda", cfg, reps=20, warm=3)
+        ref = {}
+        for threads in sorted({1, min(ncpu, 8)}):
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_STACKSIZE="1G")
+            r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-statistics", name, "--threads", str(threads)],
+                               env=env, capture_output=True, text=True, timeout=1800,
+                               preexec_fn=lambda: resource.setrlimit(resource.RLIMIT_STACK,
+                                                                     (resource.RLIM_INFINITY, resource.RLIM_INFINITY)))
+            if r.returncode == 0:
+                t_ref, Q_ref, _ = json.loads(r.stdout.strip().splitlines()[-1])
+                ref[f"{threads}_threads_ms"] = 1e3 * t_ref
+                ref["Q_rel_diff"] = float(np.max(np.abs(np.array(Q_gpu) / np.array(Q_ref) - 1)))
+        print(json.dumps({"statistics": name, "grid": cfg["nx"], "gpu_ms": 1e3 * t_gpu, "reference_cpu": ref,
+                          "timing": "median of 20 (GPU) / 3 (CPU) compute_statistics calls, wall clock"}))
+    return 0
+
+
 def roofline_step_kernel(nx, njobs, reps=20, prec=8):
     """Time lfts_step_continuous at the batch shape of the workload (njobs =
     replicas x propagators per schedule slot) with CUDA events on its stream.
@@ -392,12 +463,19 @@ def main():
                     help="fp64 (the headline) or fp32 propagators with FP64 reductions (platform cuda-fp32)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--ref-statistics", default="", help=argparse.SUPPRESS)
+    ap.add_argument("--statistics", action="store_true",
+                    help="time compute_statistics of single systems (configs 1 and 3) on the GPU and the reference CPU")
     ap.add_argument("--threads", type=int, default=1, help=argparse.SUPPRESS)
     ap.add_argument("--kernel-only", action="store_true",
                     help="only time the fused continuous step at 2*replicas jobs (for profiling)")
     args = ap.parse_args()
     if args.ref_sample:
         return _reference_sample_child(args.ref_sample, args.threads)
+    if args.ref_statistics:
+        return _reference_statistics_child(args.ref_statistics, args.threads)
+    if args.statistics:
+        return run_statistics(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.kernel_only:
