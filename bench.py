@@ -280,6 +280,111 @@ def run_statistics(args):
     return 0
 
 
+# ---------------------------------------------------------------- SCFT (config 2)
+def scft_params(platform_tol=1e-8, max_iter=2000):
+    """64^3 SCFT of a conformationally asymmetric AB diblock: f = 0.36, chiN = 20,
+    epsilon = b_A / b_B = 1.2, box 3.6 per side relaxing with stress, Anderson
+    mixing with 20 histories, tolerance 1e-8.  N = 100 contour steps: with
+    f = 0.36 the A block of an N = 90 chain would have 32.4 segments, which the
+    reference (like this build) rejects."""
+    eps, f = 1.2, 0.36
+    den = eps * eps * f + (1 - f)
+    return {"nx": [64, 64, 64], "lx": [3.6, 3.6, 3.6], "chain_model": "continuous", "ds": 1 / 100,
+            "segment_lengths": {"A": (eps * eps / den) ** 0.5, "B": (1.0 / den) ** 0.5}, "chi_n": {"A,B": 20.0},
+            "distinct_polymers": [{"volume_fraction": 1.0, "blocks": [{"type": "A", "length": f},
+                                                                       {"type": "B", "length": 1 - f}]}],
+            "box_is_altering": True, "scale_stress": 1.0,
+            "optimizer": {"name": "am", "max_hist": 20, "start_error": 1e-2, "mix_min": 0.1, "mix_init": 0.1},
+            "max_iter": max_iter, "tolerance": platform_tol}
+
+
+def scft_initial(nx, chin=20.0):
+    M = int(np.prod(nx))
+    x = np.arange(nx[0]) * 2 * np.pi / nx[0]
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    g = (np.sin(X) * np.cos(Y) + np.sin(Y) * np.cos(Z) + np.sin(Z) * np.cos(X)).reshape(-1)
+    rng = np.random.Generator(np.random.PCG64(2))
+    return {"A": chin * g + 0.1 * rng.normal(0, 1, M), "B": -chin * g + 0.1 * rng.normal(0, 1, M)}
+
+
+def host_scft_sample(module, platform, n_iter):
+    """n_iter iterations of the scft.py loop driven from numpy through the public
+    API of a module (fields to and from the host every iteration); median
+    seconds per iteration after the first."""
+    from langevinfts_b200.scft import build_system
+    p = scft_params()
+    _, _, mpt, f, cb, molecules, analyzer = build_system(p, module, platform)
+    solver = f.create_pseudospectral_solver(cb, molecules, analyzer)
+    M = cb.get_n_grid()
+    dv = cb.get_volume() / M
+    am = f.create_anderson_mixing(2 * M + 3, 20, 1e-2, 0.1, 0.1)
+    init = scft_initial(p["nx"])
+    w = np.array([init["A"], init["B"]])
+    w -= w.mean(axis=1, keepdims=True)
+    err, ts = 1e20, []
+    for _ in range(n_iter):
+        t0 = time.perf_counter()
+        solver.compute_statistics({"A": w[0], "B": w[1]})
+        phi = np.array([solver.get_total_concentration(t) for t in ("A", "B")])
+        wd = mpt.matrix_chi @ phi - mpt.matrix_p @ w
+        wd -= wd.mean(axis=1, keepdims=True)
+        old, err = err, np.sqrt(dv * np.sum(wd ** 2) / (1.0 + dv * np.sum(w ** 2)))
+        solver.compute_stress()
+        st = np.array(solver.get_stress())
+        err += np.sqrt(np.sum(st ** 2))
+        new = am.calculate_new_fields(np.concatenate([w.reshape(-1), cb.get_lx()]),
+                                      np.concatenate([wd.reshape(-1), -st]), old, err)
+        lx0 = np.array(cb.get_lx())
+        cb.set_lx(list((1 + np.clip((new[-3:] - lx0) / lx0, -0.1, 0.1)) * lx0))
+        solver.update_laplacian_operator()
+        w = new[:2 * M].reshape(2, M).copy()
+        w -= w.mean(axis=1, keepdims=True)
+        ts.append(time.perf_counter() - t0)
+    return float(np.median(ts[1:] if len(ts) > 1 else ts))
+
+
+def _reference_scft_child(n_iter, threads):
+    ref = load_reference()
+    if ref is None:
+        return 1
+    print(json.dumps([host_scft_sample(ref, "cpu-mkl", n_iter), threads]))
+    return 0
+
+
+def run_scft(args):
+    """SCFT of config 2 with the device loop in FP64 and FP32, and the time per
+    iteration of the host-driven loop; one JSON line."""
+    from langevinfts_b200.scft import SCFT
+    out = {"scft": "64^3 AB diblock f=0.36 chiN=20 eps=1.2 N=100, box relaxation, AM 20, tolerance 1e-8"}
+    res = {}
+    for platform in ("cuda", "cuda-fp32"):
+        # FP32 propagators level off near 1e-6 in the field error: stop at 1e-5
+        sim = SCFT(scft_params(1e-8 if platform == "cuda" else 1e-5), platform=platform)
+        t0 = time.perf_counter()
+        st = sim.run(scft_initial([64, 64, 64]))
+        t = time.perf_counter() - t0
+        res[platform] = st
+        out[platform] = {"iterations": st["iterations"], "error_level": st["error_level"], "energy": st["energy"],
+                         "lx": list(sim.cb.get_lx()), "seconds": t, "ms_per_iteration": 1e3 * t / st["iterations"]}
+    a, b = res["cuda"], res["cuda-fp32"]
+    out["fp32_vs_fp64"] = {"energy_abs_diff": abs(a["energy"] - b["energy"]),
+                           "lx_max_rel_diff": float(np.max(np.abs(np.array(out["cuda-fp32"]["lx"]) /
+                                                                  np.array(out["cuda"]["lx"]) - 1)))}
+    from langevinfts_b200 import langevinfts as L
+    out["host_driven_ms_per_iteration"] = 1e3 * host_scft_sample(L, "cuda", 20)
+    import resource
+    threads = min(os.cpu_count() or 1, 8)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_STACKSIZE="1G")
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-scft", "3", "--threads", str(threads)], env=env,
+                       capture_output=True, text=True, timeout=1800,
+                       preexec_fn=lambda: resource.setrlimit(resource.RLIMIT_STACK, (resource.RLIM_INFINITY, resource.RLIM_INFINITY)))
+    if r.returncode == 0:
+        out["reference_cpu_ms_per_iteration"] = {f"{threads}_threads": 1e3 * json.loads(r.stdout.strip().splitlines()[-1])[0],
+                                                 "sample": "3 iterations of the same host loop on the reference CPU platform"}
+    print(json.dumps(out))
+    return 0
+
+
 def roofline_step_kernel(nx, njobs, reps=20, prec=8):
     """Time lfts_step_continuous at the batch shape of the workload (njobs =
     replicas x propagators per schedule slot) with CUDA events on its stream.
@@ -464,6 +569,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--ref-statistics", default="", help=argparse.SUPPRESS)
+    ap.add_argument("--ref-scft", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--scft", action="store_true", help="SCFT of the 64^3 asymmetric diblock (device loop, FP64 and FP32)")
     ap.add_argument("--statistics", action="store_true",
                     help="time compute_statistics of single systems (configs 1 and 3) on the GPU and the reference CPU")
     ap.add_argument("--threads", type=int, default=1, help=argparse.SUPPRESS)
@@ -474,8 +581,12 @@ def main():
         return _reference_sample_child(args.ref_sample, args.threads)
     if args.ref_statistics:
         return _reference_statistics_child(args.ref_statistics, args.threads)
+    if args.ref_scft:
+        return _reference_scft_child(args.ref_scft, args.threads)
     if args.statistics:
         return run_statistics(args)
+    if args.scft:
+        return run_scft(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.kernel_only:

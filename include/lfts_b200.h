@@ -265,6 +265,13 @@ int lfts_am_batch_update(lfts_ctx ctx, int R, long long n, int L, const int *hea
                          const double *mix, const double *a, const double *w_cur, long long w_stride, const double *d_cur,
                          long long d_stride, const double *w_hist, const double *d_hist, double *w_out, long long out_stride);
 
+/* Adam field update of the SCFT driver (examples/scft/scft.py:42-54), on n
+ * doubles: m = b1 m + (1-b1) d; v = b2 v + (1-b2) d^2;
+ * w_new = w + lr (m / (1 - b1^count)) / (sqrt(v / (1 - b2^count)) + eps).
+ * m and v (device) carry the moments between calls; count >= 1. */
+int lfts_adam_update(lfts_ctx ctx, double *w_new, const double *w, const double *d, double *m, double *v, long long n,
+                     double lr, double b1, double b2, double eps, int count);
+
 /* ---- structure function (recording of the L-FTS driver) ------------------ */
 
 /* Forward real-to-complex 3D FFT of double fields, unnormalised, in the

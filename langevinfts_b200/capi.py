@@ -62,6 +62,8 @@ _SIGS = {
     "lfts_dots": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
     "lfts_dots_static": [C.c_int, C.c_longlong, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],
     "lfts_fft_forward": [C.c_void_p, C.c_void_p, C.c_int],
+    "lfts_adam_update": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_double,
+                         C.c_double, C.c_double, C.c_double, C.c_int],
     "lfts_sf_accumulate": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p,
                            C.c_void_p],
     "lfts_phi_blocks": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p],

@@ -554,6 +554,8 @@ void GpuComputation::enqueue_statistics() {
 std::vector<double> GpuComputation::partitions_host() {
     std::vector<double> q((size_t)R_ * mol_->get_n_polymer_types());
     check_rc(lfts_memcpy_d2h(ctx_, q.data(), dev_scalars_.get(), sizeof(double) * q.size()));
+    // a single system keeps them for get_total_partition / get_stress, as compute_concentrations does
+    if (R_ == 1) q_poly_.assign(q.begin(), q.end());
     return q;
 }
 
@@ -848,6 +850,20 @@ void GpuAndersonMixing::reset_count() {
 
 void GpuAndersonMixing::calculate_new_fields(double *w_new, const double *w_cur, const double *w_deriv, double old_err,
                                              double err) {
+    step(w_new, w_cur, w_deriv, old_err, err, false);
+}
+void GpuAndersonMixing::calculate_new_fields_device(double *w_new, const double *w_cur, const double *w_deriv, double old_err,
+                                                    double err) {
+    step(w_new, w_cur, w_deriv, old_err, err, true);
+}
+
+void GpuAndersonMixing::step(double *w_new, const double *w_cur, const double *w_deriv, double old_err, double err,
+                             bool device) {
+    // host inputs are copied in synchronously; device inputs by this context's stream
+    auto put = [&](void *dst, const void *src, size_t bytes) {
+        if (device) check_rc(lfts_memcpy_d2d_async(ctx_, dst, src, bytes));
+        else check_rc(lfts_memcpy_h2d(ctx_, dst, src, bytes));
+    };
     if (err < start_error_ || n_anderson_ >= 0) n_anderson_ = n_anderson_ + 1;
     const size_t bytes = sizeof(double) * n_var_;
     const double *dw = nullptr, *dd = nullptr;
@@ -857,8 +873,8 @@ void GpuAndersonMixing::calculate_new_fields(double *w_new, const double *w_cur,
         n_items_ = std::min(n_items_ + 1, ring_len_);
         double *wslot = w_hist_.as<double>() + (size_t)head_ * n_var_;
         double *dslot = d_hist_.as<double>() + (size_t)head_ * n_var_;
-        check_rc(lfts_memcpy_h2d(ctx_, wslot, w_cur, bytes));
-        check_rc(lfts_memcpy_h2d(ctx_, dslot, w_deriv, bytes));
+        put(wslot, w_cur, bytes);
+        put(dslot, w_deriv, bytes);
         dw = wslot;
         dd = dslot;
         // d . d_i for the n_anderson+1 newest histories
@@ -873,8 +889,8 @@ void GpuAndersonMixing::calculate_new_fields(double *w_new, const double *w_cur,
         if (old_err < err) mix_ = std::max(mix_ * 0.7, mix_min_);
         else mix_ = mix_ * 1.01;
         if (!dw) {
-            check_rc(lfts_memcpy_h2d(ctx_, stage_w_.get(), w_cur, bytes));
-            check_rc(lfts_memcpy_h2d(ctx_, stage_d_.get(), w_deriv, bytes));
+            put(stage_w_.get(), w_cur, bytes);
+            put(stage_d_.get(), w_deriv, bytes);
             dw = stage_w_.as<double>();
             dd = stage_d_.as<double>();
         }
@@ -894,7 +910,12 @@ void GpuAndersonMixing::calculate_new_fields(double *w_new, const double *w_cur,
         check_rc(lfts_am_update(ctx_, w_new_.as<double>(), w_hist_.as<double>(), d_hist_.as<double>(), n_var_, n,
                                 a_.as<double>(), n_var_, head_, ring_len_));
     }
-    check_rc(lfts_memcpy_d2h(ctx_, w_new, w_new_.get(), bytes));
+    if (device) {
+        check_rc(lfts_memcpy_d2d_async(ctx_, w_new, w_new_.get(), bytes));
+        check_rc(lfts_synchronize(ctx_));
+    } else {
+        check_rc(lfts_memcpy_d2h(ctx_, w_new, w_new_.get(), bytes));
+    }
 }
 
 }  // namespace lfts

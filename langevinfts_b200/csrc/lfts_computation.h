@@ -170,6 +170,10 @@ class GpuAndersonMixing {
     int get_n_var() const { return n_var_; }
     void calculate_new_fields(double *w_new, const double *w_current, const double *w_deriv, double old_error_level,
                               double error_level);
+    // Same with device arrays of n_var doubles (work on other streams that
+    // produced w_current / w_deriv must be complete); returns with w_new written.
+    void calculate_new_fields_device(double *w_new, const double *w_current, const double *w_deriv,
+                                     double old_error_level, double error_level);
 
    private:
     int n_var_, max_hist_, n_anderson_ = -1;
@@ -179,6 +183,7 @@ class GpuAndersonMixing {
     int ring_len_, head_ = -1, n_items_ = 0;
     // dots ring: row i (0 = newest) holds d_i . d_{i+j} for j <= n_anderson at insertion
     std::vector<std::vector<double>> dot_rows_;
+    void step(double *w_new, const double *w_cur, const double *w_deriv, double old_err, double err, bool device);
 };
 
 }  // namespace lfts

@@ -1017,6 +1017,32 @@ extern "C" int lfts_field_factors_batch(lfts_ctx c, const double *w, double coef
     return 0;
 }
 
+// ---------------------------------------------------------------- Adam field update
+// m = b1 m + (1 - b1) d; v = b2 v + (1 - b2) d^2; w_new = w + lr (m / bc1) / (sqrt(v / bc2) + eps)
+__global__ void __launch_bounds__(NTHR) k_adam(double *__restrict__ w_new, const double *__restrict__ w,
+                                               const double *__restrict__ d, double *__restrict__ m, double *__restrict__ v,
+                                               long long n, double lr, double b1, double b2, double eps, double bc1, double bc2) {
+    for (long long i = blockIdx.x * (long long)NTHR + threadIdx.x; i < n; i += (long long)gridDim.x * NTHR) {
+        const double di = d[i];
+        const double mi = b1 * m[i] + (1.0 - b1) * di;
+        const double vi = b2 * v[i] + (1.0 - b2) * (di * di);
+        m[i] = mi;
+        v[i] = vi;
+        w_new[i] = w[i] + lr * (mi / bc1) / (sqrt(vi / bc2) + eps);
+    }
+}
+
+extern "C" int lfts_adam_update(lfts_ctx c, double *w_new, const double *w, const double *d, double *m, double *v,
+                                long long n, double lr, double b1, double b2, double eps, int count) {
+    if (!c || !w_new || !w || !d || !m || !v) return fail("null argument");
+    if (count < 1) return fail("the Adam step count starts at 1");
+    const double bc1 = 1.0 - std::pow(b1, (double)count), bc2 = 1.0 - std::pow(b2, (double)count);
+    k_adam<<<grid_for(n), NTHR, 0, c->stream>>>(w_new, w, d, m, v, n, lr, b1, b2, eps, bc1, bc2);
+    c->launches += 1;
+    CKLAUNCH();
+    return 0;
+}
+
 // ---------------------------------------------------------------- forward FFT and structure function
 extern "C" int lfts_fft_forward(lfts_ctx c, const lfts_step_job *jobs, int nj) {
     if (!c || !jobs) return fail("null argument");

@@ -13,6 +13,7 @@
 #include "lfts_computation.h"
 #include "lfts_host.h"
 #include "lfts_langevin.h"
+#include "lfts_scft.h"
 
 namespace py = pybind11;
 using namespace lfts;
@@ -313,6 +314,57 @@ PYBIND11_MODULE(langevinfts, m) {
                       << "), device " << f.device << std::endl;
         })
         .def("get_model_name", [](Factory &) { return std::string(""); });
+
+    // Device-resident SCFT iteration (fields, residuals and optimizer in HBM).
+    py::class_<DeviceScft>(m, "DeviceScft")
+        .def(py::init([](Factory &f, ComputationBox *cb, Molecules *mol, PropagatorAnalyzer *pa, py::dict c) {
+            ScftConfig cfg;
+            cfg.monomer_types = c["monomer_types"].cast<std::vector<std::string>>();
+            cfg.chi = c["matrix_chi"].cast<std::vector<double>>();
+            cfg.P = c["matrix_p"].cast<std::vector<double>>();
+            cfg.A_inv = c["matrix_a_inv"].cast<std::vector<double>>();
+            cfg.box_altering = c["box_is_altering"].cast<bool>();
+            cfg.scale_stress = c["scale_stress"].cast<double>();
+            cfg.optimizer = c["optimizer"].cast<std::string>();
+            if (c.contains("am_max_hist")) cfg.am_max_hist = c["am_max_hist"].cast<int>();
+            if (c.contains("am_start_error")) cfg.am_start_error = c["am_start_error"].cast<double>();
+            if (c.contains("am_mix_min")) cfg.am_mix_min = c["am_mix_min"].cast<double>();
+            if (c.contains("am_mix_init")) cfg.am_mix_init = c["am_mix_init"].cast<double>();
+            if (c.contains("adam_lr")) cfg.adam_lr = c["adam_lr"].cast<double>();
+            if (c.contains("adam_gamma")) cfg.adam_gamma = c["adam_gamma"].cast<double>();
+            return new DeviceScft(cb, mol, pa, f.precision, f.device, cfg);
+        }), py::keep_alive<1, 3>(), py::keep_alive<1, 4>(), py::keep_alive<1, 5>())
+        .def("set_fields", [](DeviceScft &d, Arr w) {
+            py::buffer_info bi = w.request();
+            size_check(bi, (long long)d.n_types() * d.n_grid(), "w ", "S*n_grid");
+            d.set_fields((const double *)bi.ptr);
+        })
+        .def("get_fields", [](DeviceScft &d) {
+            py::array_t<double> w({(py::ssize_t)d.n_types(), (py::ssize_t)d.n_grid()});
+            d.get_fields((double *)w.request().ptr);
+            return w;
+        })
+        .def("get_concentrations", [](DeviceScft &d) {
+            py::array_t<double> phi({(py::ssize_t)d.n_types(), (py::ssize_t)d.n_grid()});
+            d.get_concentrations((double *)phi.request().ptr);
+            return phi;
+        })
+        .def("evaluate", [](DeviceScft &d) {
+            ScftStats s;
+            {
+                py::gil_scoped_release nogil;
+                s = d.evaluate();
+            }
+            py::dict r;
+            r["error_level"] = s.error_level; r["mass_error"] = s.mass_error; r["partitions"] = s.partitions;
+            r["stress"] = s.stress; r["lx"] = s.lx; r["aux_mean"] = s.aux_mean; r["aux_msq"] = s.aux_msq;
+            return r;
+        })
+        .def("update", [](DeviceScft &d) {
+            py::gil_scoped_release nogil;
+            d.update();
+        })
+        .def("reset", &DeviceScft::reset);
 
     // Batched L-FTS engine: n_replicas independent systems on the device.
 
