@@ -13,7 +13,6 @@
 
 #include "lfts_step_fast.cuh"
 #include "lfts_step_r8.cuh"
-#include "lfts_step_bulk.cuh"
 
 using namespace lfts;
 
@@ -45,7 +44,7 @@ struct lfts_ctx_s {
     bool gen = false, nbr2 = true;
     int TJ = 16, ntiles = 1, zb = 1;
     int fastN = 0;            // cubic grid handled by the compile-time specialised kernels (0: generic)
-    int r8 = 0;               // 64^3: 1 register-resident 8x8 line transforms, 2 the same with bulk-copy staging
+    int r8 = 0;               // 64^3: register-resident 8x8 line transforms (lfts_step_r8.cuh)
     int nsm = 0;              // streaming multiprocessors of the device
     void *stw = nullptr;
     size_t sm_pf1 = 0, sm_pf2 = 0, sm_mid = 0, sm_inv1 = 0, sm_inv2 = 0, sm_x1 = 0, sm_x2 = 0;
@@ -146,25 +145,15 @@ template <typename T, int N> static int fast_setup(int max_smem) {
 
 template <typename T> static int r8_setup(int max_smem) {
     using C = typename CT<T>::type;
-    if (r8::plane_smem<C>() > (size_t)max_smem || r8::xpass_smem<C>() > (size_t)max_smem) return 0;
+    if (r8::plane_smem<C>() > (size_t)max_smem || r8::xpipe_smem<C>() > (size_t)max_smem) return 0;
     if (allow_smem(r8::kr_plane_forward<T, 1, FM_NONE, FM_NONE>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r8::kr_plane_mid<T>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r8::kr_plane_inverse<T, 2, EPI_RICH>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r8::kr_plane_inverse<T, 1, EPI_SCALE>, max_smem) != cudaSuccess) return 0;
-    if (allow_smem(r8::kr_xpass<T, 1>, max_smem) != cudaSuccess) return 0;
-    if (allow_smem(r8::kr_xpass<T, 2>, max_smem) != cudaSuccess) return 0;
-    if (allow_smem(r8::kb_xpass<T, 1>, max_smem) != cudaSuccess) return 0;
-    if (allow_smem(r8::kb_xpass<T, 2>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r8::kp_xpass<T, 1>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r8::kp_xpass<T, 2>, max_smem) != cudaSuccess) return 0;
-    if (!std::getenv("LFTS_BULK_PLANES") || r8::kb_plane_smem<C>(true) > (size_t)max_smem) return 1;
-    if (allow_smem(r8::kb_plane_forward<T, 1>, max_smem) != cudaSuccess) return 1;
-    if (allow_smem(r8::kb_plane_forward<T, 2>, max_smem) != cudaSuccess) return 1;
-    if (allow_smem(r8::kb_plane_mid<T>, max_smem) != cudaSuccess) return 1;
-    if (allow_smem(r8::kb_plane_inverse<T, 2, EPI_RICH>, max_smem) != cudaSuccess) return 1;
-    if (allow_smem(r8::kb_plane_inverse<T, 1, EPI_SCALE>, max_smem) != cudaSuccess) return 1;
-    return 2;
+    return 1;
 }
 
 template <typename T> static int setup_plan(lfts_ctx c) {
@@ -505,19 +494,8 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
     const size_t x1 = sizeof(C) * ((size_t)N * TJ + fast::stw_size(N) + 1);
     if constexpr (N == r8::N) {
         if (c->r8) {
-            const dim3 rp(N, nj), rx(r8::PLANE / r8::GROUPS, nj);
+            const dim3 rp(N, nj);
             const size_t ps = r8::plane_smem<C>();
-            const dim3 bx(r8::PLANE / r8::XT, nj);
-            if (c->r8 == 2) {
-                const size_t p1 = r8::kb_plane_smem<C>(false), p2 = r8::kb_plane_smem<C>(true);
-                r8::kb_plane_forward<T, 2><<<rp, NTHR, p1, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0);
-                r8::kb_xpass<T, 2><<<bx, NTHR, r8::xbulk_smem<C, 2>(), st>>>(g, jobs, 0, 0, 1);
-                r8::kb_plane_mid<T><<<rp, NTHR, p1, st>>>(g, jobs, 1);
-                r8::kb_xpass<T, 1><<<bx, NTHR, r8::xbulk_smem<C, 1>(), st>>>(g, jobs, 1, 1, 1);
-                r8::kb_plane_inverse<T, 2, EPI_RICH><<<rp, NTHR, p2, st>>>(g, jobs, s, 0, 0);
-                CKLAUNCH();
-                return 0;
-            }
             const long long it2 = (long long)nj * 2 * r8::xpipe_tiles<C>(), it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = 3LL * c->nsm;
             const dim3 px2((unsigned)(it2 < cap ? it2 : cap)), px1((unsigned)(it1 < cap ? it1 : cap));
             r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC><<<rp, NTHR, ps, st>>>(g, jobs, s, 0);
@@ -548,18 +526,9 @@ static int step_disc_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, 
     const size_t x1 = sizeof(C) * ((size_t)N * TJ + fast::stw_size(N) + 1);
     if constexpr (N == r8::N) {
         if (c->r8) {
-            const dim3 rp(N, nj), rx(r8::PLANE / r8::GROUPS, nj);
-            const size_t ps = r8::plane_smem<C>(), xs = r8::xpass_smem<C>();
+            const dim3 rp(N, nj);
+            const size_t ps = r8::plane_smem<C>();
             r8::kr_plane_forward<T, 1, FM_NONE, FM_NONE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0);
-            const dim3 bx(r8::PLANE / r8::XT, nj);
-            if (c->r8 == 2) {
-                const size_t p1 = r8::kb_plane_smem<C>(false);
-                r8::kb_plane_forward<T, 1><<<rp, NTHR, p1, st>>>(g, jobs, s, FM_NONE, 0, 0);
-                r8::kb_xpass<T, 1><<<bx, NTHR, r8::xbulk_smem<C, 1>(), st>>>(g, jobs, 0, half, half);
-                r8::kb_plane_inverse<T, 1, EPI_SCALE><<<rp, NTHR, p1, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
-                CKLAUNCH();
-                return 0;
-            }
             const long long it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = 3LL * c->nsm;
             r8::kp_xpass<T, 1><<<(unsigned)(it1 < cap ? it1 : cap), NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, half, half);
             r8::kr_plane_inverse<T, 1, EPI_SCALE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);

@@ -36,13 +36,11 @@ namespace r8 {
 
 constexpr int N = 64, NZC = N / 2 + 1, PLANE = N * NZC;
 constexpr int PR = 73;  // plane row stride (complex elements)
-constexpr int XG = 72;  // exchange slots per lane group in the x-pass
 constexpr int GROUPS = NTHR / 8;
 static_assert(GROUPS == 32, "one lane group of 8 per 64-point line, 32 lines per CTA");
 static_assert(PLANE % GROUPS == 0, "x-pass tiles cover the plane exactly");
 
 template <typename C> constexpr size_t plane_smem() { return sizeof(C) * (size_t)N * PR; }
-template <typename C> constexpr size_t xpass_smem() { return sizeof(C) * (size_t)GROUPS * XG; }
 
 __device__ __forceinline__ int xpad(int e) { return e + (e >> 3); }
 
@@ -134,7 +132,6 @@ __device__ __forceinline__ void herm_partner(const C (&c)[8], C (&p)[8], int t, 
 template <typename C>
 __device__ __forceinline__ void put_columns(C *st, int kz, const C (&c)[8], int j, int lane, unsigned mask) {
     if (kz != 0) {
-#pragma unroll
         C *col = st + j * NZC + kz;  // rows j + 8k at constant offsets
 #pragma unroll
         for (int k = 0; k < 8; k++) col[8 * k * NZC] = c[k];
@@ -157,7 +154,6 @@ __device__ __forceinline__ void put_columns(C *st, int kz, const C (&c)[8], int 
 template <typename C>
 __device__ __forceinline__ void get_columns(const C *st, int kz, C (&c)[8], int j) {
     if (kz != 0) {
-#pragma unroll
         const C *col = st + j * NZC + kz;
 #pragma unroll
         for (int m = 0; m < 8; m++) c[m] = col[8 * m * NZC];
@@ -344,136 +340,9 @@ __global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFT
 }
 
 // ------------------------------------------------------------------------
-// K2 / K4: x-transform of 32 columns, bond multiply, inverse x-transform
-template <typename T, int NBR>
-__global__ void __launch_bounds__(NTHR, 2) kr_xpass(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_in0,
-                                                 int bsel0, int bsel1) {
-    using C = typename CT<T>::type;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const lfts_step_job jb = jobs[blockIdx.y];
-    if (jb.active && !jb.active[jb.replica]) return;
-    const int tid = threadIdx.x, lane = tid & 31, j = lane & 7, grp = tid >> 3;
-    const unsigned mask = 0xFFu << (lane & 24);
-    const C wf = tw_base<C>(j, -1), wi = tw_base<C>(j, +1);
-    const RowX<C> at{(C *)smem_raw + grp * XG};
-    const int col = blockIdx.x * GROUPS + grp;
-    C *s0 = (C *)jb.spec + (size_t)spec_in0 * g.Mc + col;
-    const T *bt0 = (const T *)(bsel0 ? jb.bond_half : jb.bond) + col;
-    const T *bt1 = (const T *)(bsel1 ? jb.bond_half : jb.bond) + col;
-#pragma unroll
-    for (int b = 0; b < NBR; b++) {
-        C *sb = s0 + (size_t)b * g.Mc;
-        const T *bt = b == 0 ? bt0 : bt1;
-        C a[8];
-        T bv[8];
-#pragma unroll
-        for (int m = 0; m < 8; m++) a[m] = sb[(j + 8 * m) * PLANE];
-#pragma unroll
-        for (int k = 0; k < 8; k++) bv[k] = bt[(j + 8 * k) * PLANE];
-        fft64<-1>(a, at, j, wf, mask);
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            a[k].x *= bv[k];
-            a[k].y *= bv[k];
-        }
-        fft64<+1>(a, at, j, wi, mask);
-#pragma unroll
-        for (int m = 0; m < 8; m++) sb[(j + 8 * m) * PLANE] = a[m];
-    }
-}
-
-// ------------------------------------------------------------------------
-// K2 / K4 with bulk copies: the tile of XT columns x 64 rows of each spectrum
-// arrives in shared memory by cp.async.bulk (one 16-byte-aligned row segment
-// per copy), is transformed there with warp w holding rows w + 8m of column
-// lane, and leaves by bulk stores.  All shared-memory accesses are 32
-// consecutive elements of one row (no bank conflicts).
-constexpr int XT = 32;  // columns per CTA
-static_assert(PLANE % XT == 0, "bulk x-pass tiles cover the plane exactly");
-template <typename C, int NBR> constexpr size_t xbulk_smem() { return sizeof(C) * (size_t)NBR * N * XT + 16; }
-
-// 64-point transform down one tile column: on entry warp w holds x[w + 8m],
-// on exit x -> X with warp t holding X[t + 8k].  Uses the column itself as the
-// exchange space (rows 8k + j), bracketed by block barriers.
-template <int SIGN, typename C>
-__device__ __forceinline__ void fft64_tile(C (&a)[8], C *tb, int w, int l, C w1) {
-    SmallDFT<8, C>::run(a, SIGN, nullptr, 0);
-    twiddle8(a, w1);
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 8; k++) tb[(8 * k + w) * XT + l] = a[k];
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 8; k++) a[k] = tb[(8 * w + k) * XT + l];
-    SmallDFT<8, C>::run(a, SIGN, nullptr, 0);
-}
-
-template <typename T, int NBR>
-__global__ void __launch_bounds__(NTHR, 3) kb_xpass(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_in0,
-                                                    int bsel0, int bsel1) {
-    using C = typename CT<T>::type;
-    constexpr uint32_t ROWB = XT * sizeof(C);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *tile = (C *)smem_raw;
-    uint64_t *bar = (uint64_t *)(tile + NBR * N * XT);
-    const lfts_step_job jb = jobs[blockIdx.y];
-    if (jb.active && !jb.active[jb.replica]) return;
-    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-    const int col0 = blockIdx.x * XT;
-    C *sb = (C *)jb.spec + (size_t)spec_in0 * g.Mc + col0;
-    if (((uintptr_t)sb | (uintptr_t)g.Mc * sizeof(C)) & 15) {
-        if (tid == 0) kerr_set(KERR_MISALIGNED);
-        return;
-    }
-    if (tid == 0) mbar_init(bar, 1);
-    __syncthreads();
-    if (w == 0) {
-        if (l == 0) mbar_arrive_expect_tx(bar, NBR * N * ROWB);
-        __syncwarp();
-        for (int r = l; r < NBR * N; r += 32) {
-            const int b = r / N, x = r - b * N;
-            bulk_load(tile + r * XT, sb + (size_t)b * g.Mc + (size_t)x * PLANE, ROWB, bar);
-        }
-    }
-    const T *bt0 = (const T *)(bsel0 ? jb.bond_half : jb.bond) + col0 + l;
-    const T *bt1 = (const T *)(bsel1 ? jb.bond_half : jb.bond) + col0 + l;
-    if (!mbar_wait(bar, 0)) {
-        mbar_wait(bar, 0);
-        return;
-    }
-    const C wf = tw_base<C>(w, -1), wi = tw_base<C>(w, +1);
-#pragma unroll 1
-    for (int b = 0; b < NBR; b++) {
-        C *tb = tile + b * N * XT;
-        // bond factors for kx = w + 8k (in flight during the forward transform)
-        T bv[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) bv[k] = (b == 0 ? bt0 : bt1)[(w + 8 * k) * PLANE];
-        C a[8];
-#pragma unroll
-        for (int m = 0; m < 8; m++) a[m] = tb[(w + 8 * m) * XT + l];
-        fft64_tile<-1>(a, tb, w, l, wf);
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            a[k].x *= bv[k];
-            a[k].y *= bv[k];
-        }
-        fft64_tile<+1>(a, tb, w, l, wi);
-        __syncthreads();
-#pragma unroll
-        for (int m = 0; m < 8; m++) tb[(w + 8 * m) * XT + l] = a[m];
-    }
-    fence_proxy_async();
-    __syncthreads();
-    if (w == 0) {
-        for (int r = l; r < NBR * N; r += 32) {
-            const int b = r / N, x = r - b * N;
-            bulk_store(sb + (size_t)b * g.Mc + (size_t)x * PLANE, tile + r * XT, ROWB);
-        }
-        bulk_commit();
-        bulk_wait_read();
-    }
-}
+// x-pass geometry: items of XT columns (FP64) or 2 XT (FP32) by 64 rows
+constexpr int XT = 32;
+static_assert(PLANE % XT == 0, "x-pass tiles cover the plane exactly");
 
 // ------------------------------------------------------------------------
 // K2 / K4, persistent and pipelined: work items are (job, branch, 32-column
