@@ -43,6 +43,14 @@ UNIT = "replica-steps/s"
 ITERS_PER_STEP = 44.0
 
 
+def workload_config(R, nx):
+    """The benchmark workload as both arms report it."""
+    return {"workload": f"batched L-FTS: {R} replicas/GPU of AB diblock f=0.5 chiN=17 nbar=100 N=90, "
+                        f"{nx}^3 box 7.3, dt=0.8, saddle tol 1e-4, AM max_hist 20",
+            "replicas_per_gpu": R, "grid": [nx] * 3, "N": 90,
+            "l2": "inputs (64 replicas x 4 propagators x 46 slices x 2 MB) far exceed the 126 MB L2"}
+
+
 def params(nx=64, lx=7.3):
     return {
         "nx": [nx] * 3, "lx": [lx] * 3, "chain_model": "continuous", "ds": 1 / 90,
@@ -182,8 +190,9 @@ def run_reference(args):
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "batched L-FTS AB diblock 64^3 N=90 (reference CPU: one replica)", "grid": [64, 64, 64],
-                      "N": 90, "replicas": 1},
+           "config": dict(workload_config(args.replicas, args.nx), parallelism="reference CPU platform, OpenMP threads",
+                          reference_sample="one replica at a time; replica-steps/s = 1 / (seconds per saddle iteration "
+                                           "x saddle iterations per Langevin step)"),
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
                             "sample": f"{args.steps} timed saddle-point iterations (after 1 untimed) of 1 replica, 64^3, N=90, "
                                       f"x {ITERS_PER_STEP} iterations per Langevin step; reference CPU platform, project FFT "
@@ -534,10 +543,7 @@ def run_ours(args):
         "metric": METRIC if args.precision == "fp64" else METRIC_FP32, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
-        "config": {"workload": f"batched L-FTS: {R} replicas/GPU of AB diblock f=0.5 chiN=17 nbar=100 N=90, "
-                               f"{args.nx}^3 box 7.3, dt=0.8, saddle tol 1e-4, AM max_hist 20",
-                   "replicas_per_gpu": R, "grid": [args.nx] * 3, "N": 90, "parallelism": f"replicas x{world}",
-                   "l2": "inputs (64 replicas x 4 propagators x 46 slices x 2 MB) far exceed the 126 MB L2",
+        "config": {**workload_config(R, args.nx), "parallelism": f"replicas x{world}",
                    "mean_saddle_iterations": float(np.mean(iters)) if iters else None, "failed_steps": fails,
                    "initial_saddle_iterations": max(st0["iterations"])},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": R * nreal * M * 8,
