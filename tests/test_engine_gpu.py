@@ -83,6 +83,47 @@ def test_step_continuous(nx, lx, prec):
     ctx.close()
 
 
+@pytest.mark.parametrize("nx,lx", [((64, 64, 64), (7.3, 7.3, 7.3)), ((32, 32, 32), (4.0, 4.0, 4.0)),
+                                   ((23, 27, 25), (3.2, 3.3, 3.4))])
+@pytest.mark.parametrize("prec", [8, 4])
+def test_step_active_mask(nx, lx, prec):
+    """Jobs of inactive replicas leave their output untouched; the others step
+    as usual (the batched saddle loop stops converged replicas this way)."""
+    from langevinfts_b200.capi import StepJob, check
+    dt = np.dtype(np.float64 if prec == 8 else np.float32)
+    ctx = _ctx(nx, prec)
+    M = ctx.M
+    rng = np.random.default_rng(11)
+    ds, b2, R = 0.01, 1.0, 3
+    g = orc.Grid(nx, lx)
+    bond, bondh = _tables(ctx, nx, lx, b2, ds, dt)
+    active = np.array([1, 0, 1], dtype=np.int32)
+    act = ctx.upload(active)
+    jobs, w, q0 = [], [], []
+    for r in range(R):
+        w.append(rng.normal(0, 1.0, M))
+        q0.append(1.0 + 0.3 * rng.random(M))
+        wd = ctx.upload(w[r])
+        fac = ctx.malloc(M * dt.itemsize)
+        check(ctx.lib.lfts_field_factors(ctx.h, wd, -ds / 4, fac))
+        q = ctx.malloc(2 * M * dt.itemsize)
+        ctx.h2d(q, np.concatenate([q0[r], np.full(M, -7.0)]).astype(dt))  # slice 1 holds a sentinel
+        spec = ctx.malloc(2 * ctx.Mc * 2 * dt.itemsize)
+        jobs.append(StepJob(q, M, q + M * dt.itemsize, M, fac, bond, bondh, spec, act, r, 0))
+    jp = _jobs(ctx, jobs)
+    check(ctx.lib.lfts_step_continuous(ctx.h, jp, R, 0))
+    ctx.sync()
+    bo, bh = orc.boltz_bond(nx, lx, b2, ds), orc.boltz_bond(nx, lx, b2 / 2, ds)
+    for r in range(R):
+        got = ctx.d2h(jobs[r].in_, (2, M), dt)[1].astype(float)
+        if active[r]:
+            ref = orc.step_continuous(g, q0[r], np.exp(-w[r] * ds / 2), np.exp(-w[r] * ds / 4), bo, bh)
+            assert _rel(got, ref) < (1e-12 if prec == 8 else 2e-5)
+        else:
+            assert np.all(got == -7.0)
+    ctx.close()
+
+
 @pytest.mark.parametrize("nx,lx,prec", [(n, l, 8) for n, l in GRIDS[:4] + GRIDS[5:6] + GRIDS[9:10]] +
                          [(n, l, 4) for n, l in GRIDS[2:3] + GRIDS[9:10]])
 @pytest.mark.parametrize("half,with_fac", [(0, 1), (1, 0), (1, 1)])
