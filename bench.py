@@ -43,22 +43,38 @@ UNIT = "replica-steps/s"
 ITERS_PER_STEP = 44.0
 
 
-def workload_config(R, nx):
+# The batched L-FTS workloads: config4 is the headline (64^3, 64 replicas);
+# config5 is the system of the learned-start study run with the plain solver.
+WORKLOADS = {
+    "config4": {"nx": 64, "lx": 7.3, "f": 0.5, "chin": 17.0, "nbar": 100, "replicas": 64, "seed": 1000,
+                "iters_per_step": ITERS_PER_STEP},
+    "config5": {"nx": 96, "lx": 8.0, "f": 0.4, "chin": 18.0, "nbar": 200, "replicas": 16, "seed": 2000,
+                "iters_per_step": 54.3},  # measured by the GPU arm on this workload
+}
+
+
+def workload_config(R, nx, name="config4"):
     """The benchmark workload as both arms report it."""
-    return {"workload": f"batched L-FTS: {R} replicas/GPU of AB diblock f=0.5 chiN=17 nbar=100 N=90, "
-                        f"{nx}^3 box 7.3, dt=0.8, saddle tol 1e-4, AM max_hist 20",
+    w = WORKLOADS[name]
+    return {"workload": f"batched L-FTS: {R} replicas/GPU of AB diblock f={w['f']} chiN={w['chin']:g} nbar={w['nbar']} "
+                        f"N=90, {nx}^3 box {w['lx']}, dt=0.8, saddle tol 1e-4, AM max_hist 20",
             "replicas_per_gpu": R, "grid": [nx] * 3, "N": 90,
-            "l2": "inputs (64 replicas x 4 propagators x 46 slices x 2 MB) far exceed the 126 MB L2"}
+            "l2": f"inputs ({R} replicas x 4 propagators x 46 slices x {8 * nx ** 3 / 2 ** 20:.0f} MB) far exceed the 126 MB L2"}
 
 
-def params(nx=64, lx=7.3):
+def params(nx=64, lx=7.3, f=0.5, chin=17.0, nbar=100):
     return {
         "nx": [nx] * 3, "lx": [lx] * 3, "chain_model": "continuous", "ds": 1 / 90,
-        "segment_lengths": {"A": 1.0, "B": 1.0}, "chi_n": {"A,B": 17.0},
-        "distinct_polymers": [{"volume_fraction": 1.0, "blocks": [{"type": "A", "length": 0.5}, {"type": "B", "length": 0.5}]}],
-        "langevin": {"dt": 0.8, "nbar": 100}, "saddle": {"max_iter": 100, "tolerance": 1e-4},
+        "segment_lengths": {"A": 1.0, "B": 1.0}, "chi_n": {"A,B": chin},
+        "distinct_polymers": [{"volume_fraction": 1.0, "blocks": [{"type": "A", "length": f}, {"type": "B", "length": 1 - f}]}],
+        "langevin": {"dt": 0.8, "nbar": nbar}, "saddle": {"max_iter": 100, "tolerance": 1e-4},
         "am": {"max_hist": 20, "start_error": 5e-1, "mix_min": 0.01, "mix_init": 0.01},
     }
+
+
+def workload_params(name, nx=None):
+    w = WORKLOADS[name]
+    return params(nx or w["nx"], w["lx"], w["f"], w["chin"], w["nbar"])
 
 
 def initial_fields(seed, M):
@@ -123,7 +139,7 @@ def load_reference():
     return mod
 
 
-def reference_sample(n_iter, threads, timeout=900):
+def reference_sample(n_iter, threads, timeout=900, workload="config4"):
     """Time n_iter saddle-point iterations of one replica on the reference CPU
     platform through the same driver; returns (seconds per iteration, threads).
     Runs in a child process: the reference keeps two grids of reals and two of
@@ -135,7 +151,8 @@ def reference_sample(n_iter, threads, timeout=900):
 
     def unlimited_stack():
         resource.setrlimit(resource.RLIMIT_STACK, (resource.RLIM_INFINITY, resource.RLIM_INFINITY))
-    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-sample", str(n_iter), "--threads", str(threads)],
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-sample", str(n_iter), "--threads", str(threads),
+                        "--workload", workload],
                        env=env, preexec_fn=unlimited_stack, capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
         sys.stderr.write(r.stdout[-2000:] + r.stderr[-2000:])
@@ -143,15 +160,16 @@ def reference_sample(n_iter, threads, timeout=900):
     return tuple(json.loads(r.stdout.strip().splitlines()[-1]))
 
 
-def _reference_sample_child(n_iter, threads):
+def _reference_sample_child(n_iter, threads, workload="config4"):
     ref = load_reference()
     if ref is None:
         return None
     from langevinfts_b200.lfts import LFTS
-    p = params()
-    sim = LFTS(p, random_seed=1000, module=ref, platform="cpu-mkl")
+    p = workload_params(workload)
+    seed = WORKLOADS[workload]["seed"]
+    sim = LFTS(p, random_seed=seed, module=ref, platform="cpu-mkl")
     M = sim.M
-    w = initial_fields(1000, M)
+    w = initial_fields(seed, M)
     S = len(sim.monomer_types)
     w_aux = sim.mpt.to_aux_fields(np.array([w[t] for t in sim.monomer_types]))
     sim.am.reset_count()
@@ -181,21 +199,22 @@ def run_reference(args):
     if ref is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) is missing"}))
         return 0
-    r = reference_sample(args.steps, threads)
+    r = reference_sample(args.steps, threads, workload=args.workload)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "the reference CPU platform failed on this host (see stderr)"}))
         return 0
     t_iter = r[0]
-    v = 1.0 / (t_iter * ITERS_PER_STEP)
+    ips = WORKLOADS[args.workload]["iters_per_step"]
+    v = 1.0 / (t_iter * ips)
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": dict(workload_config(args.replicas, args.nx), parallelism="reference CPU platform, OpenMP threads",
+           "config": dict(workload_config(args.replicas, args.nx, args.workload), parallelism="reference CPU platform, OpenMP threads",
                           reference_sample="one replica at a time; replica-steps/s = 1 / (seconds per saddle iteration "
                                            "x saddle iterations per Langevin step)"),
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
                             "sample": f"{args.steps} timed saddle-point iterations (after 1 untimed) of 1 replica, 64^3, N=90, "
-                                      f"x {ITERS_PER_STEP} iterations per Langevin step; reference CPU platform, project FFT "
+                                      f"x {ips} iterations per Langevin step; reference CPU platform, project FFT "
                                       "in place of MKL"},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -451,9 +470,9 @@ def run_ours(args):
     from langevinfts_b200.lfts import BatchedLFTS
 
     R = args.replicas
-    p = params(args.nx)
+    p = workload_params(args.workload, args.nx)
     from langevinfts_b200.ensemble import max_over_ranks, replica_seeds
-    seeds = replica_seeds(rank, R)
+    seeds = replica_seeds(rank, R, base=WORKLOADS[args.workload]["seed"])
     f = L.PlatformSelector.create_factory("cuda", False)
     sim = BatchedLFTS(p, seeds, module=L, platform="cuda" if args.precision == "fp64" else "cuda-fp32")
     M = sim.M
@@ -532,18 +551,18 @@ def run_ours(args):
     cpu = None
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        r = reference_sample(1, threads)
+        r = reference_sample(1, threads, workload=args.workload)
         sys.stderr.write(f"[bench] reference CPU sample: {r}\n")
         if r is not None:
             mean_iters = float(np.mean(iters)) if iters else ITERS_PER_STEP
             cpu = {"value": 1.0 / (r[0] * mean_iters), "unit": UNIT, "cores": r[1], "kind": "reference",
-                   "sample": f"2 saddle-point iterations of 1 replica (64^3, N=90) on the reference CPU platform "
+                   "sample": f"2 saddle-point iterations of 1 replica ({args.nx}^3, N=90) on the reference CPU platform "
                              f"(first discarded), {r[0]:.2f} s/iteration x {mean_iters:.1f} iterations per step measured above"}
     out = {
         "metric": METRIC if args.precision == "fp64" else METRIC_FP32, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
-        "config": {**workload_config(R, args.nx), "parallelism": f"replicas x{world}",
+        "config": {**workload_config(R, args.nx, args.workload), "parallelism": f"replicas x{world}",
                    "mean_saddle_iterations": float(np.mean(iters)) if iters else None, "failed_steps": fails,
                    "initial_saddle_iterations": max(st0["iterations"])},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": R * nreal * M * 8,
@@ -568,8 +587,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--replicas", type=int, default=64)
-    ap.add_argument("--nx", type=int, default=64)
+    ap.add_argument("--workload", default="config4", choices=sorted(WORKLOADS),
+                    help="config4: 64^3, 64 replicas (the headline); config5: 96^3, 16 replicas")
+    ap.add_argument("--replicas", type=int, default=None)
+    ap.add_argument("--nx", type=int, default=None)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
                     help="fp64 (the headline) or fp32 propagators with FP64 reductions (platform cuda-fp32)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -583,8 +604,12 @@ def main():
     ap.add_argument("--kernel-only", action="store_true",
                     help="only time the fused continuous step at 2*replicas jobs (for profiling)")
     args = ap.parse_args()
+    if args.replicas is None:
+        args.replicas = WORKLOADS[args.workload]["replicas"]
+    if args.nx is None:
+        args.nx = WORKLOADS[args.workload]["nx"]
     if args.ref_sample:
-        return _reference_sample_child(args.ref_sample, args.threads)
+        return _reference_sample_child(args.ref_sample, args.threads, args.workload)
     if args.ref_statistics:
         return _reference_statistics_child(args.ref_statistics, args.threads)
     if args.ref_scft:
