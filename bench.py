@@ -213,7 +213,7 @@ def run_reference(args):
                           reference_sample="one replica at a time; replica-steps/s = 1 / (seconds per saddle iteration "
                                            "x saddle iterations per Langevin step)"),
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                            "sample": f"{args.steps} timed saddle-point iterations (after 1 untimed) of 1 replica, 64^3, N=90, "
+                            "sample": f"{args.steps} timed saddle-point iterations (after 1 untimed) of 1 replica, {args.nx}^3, N=90, "
                                       f"x {ips} iterations per Langevin step; reference CPU platform, project FFT "
                                       "in place of MKL"},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
