@@ -127,15 +127,22 @@ template <typename T, bool GEN> static cudaError_t set_attrs_t(int max_smem) {
 }
 
 // Attributes of the cubic fast kernels; 0 when their shared memory does not fit.
+// Threads per CTA of the two-branch cubic plane kernels (continuous K1 and K5).
+// Their shared memory holds two N x (N/2+1) spectrum planes; at 96^3 FP64
+// that is 176 KB with 8 warps, so one CTA fits per SM and 512 threads double
+// the warps that hide its load and shared-memory latency.
+template <typename T, int N> constexpr int fast_nt2() { return (sizeof(T) == 8 && N == 96) ? 512 : NTHR; }
+
 template <typename T, int N> static int fast_setup(int max_smem) {
     using C = typename CT<T>::type;
-    const size_t f2 = fast::FSmem<C, N, 2, 1>::BYTES, f1 = fast::FSmem<C, N, 1, 1>::BYTES;
+    constexpr int NT2 = fast_nt2<T, N>();
+    const size_t f2 = fast::FSmem<C, N, 2, 1, NT2>::BYTES, f1 = fast::FSmem<C, N, 1, 1>::BYTES;
     const size_t x2 = sizeof(C) * (2 * (size_t)N * (sizeof(T) == 8 ? 16 : 32) + fast::stw_size(N) + 1);
     if (f2 > (size_t)max_smem || x2 > (size_t)max_smem) return 0;
     if (allow_smem(fast::kf_plane_forward<T, 1, N>, max_smem) != cudaSuccess) return 0;
-    if (allow_smem(fast::kf_plane_forward<T, 2, N>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(fast::kf_plane_forward<T, 2, N, NT2>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(fast::kf_plane_mid<T, N>, max_smem) != cudaSuccess) return 0;
-    if (allow_smem(fast::kf_plane_inverse<T, 2, EPI_RICH, N>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(fast::kf_plane_inverse<T, 2, EPI_RICH, N, NT2>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(fast::kf_plane_inverse<T, 1, EPI_SCALE, N>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(fast::kf_xpass<T, 1, N>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(fast::kf_xpass<T, 2, N>, max_smem) != cudaSuccess) return 0;
@@ -489,7 +496,8 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
     cudaStream_t st = c->stream;
     constexpr int TJ = sizeof(T) == 8 ? 16 : 32;
     const dim3 gp(N, nj), gx((unsigned)(((long long)N * (N / 2 + 1) + TJ - 1) / TJ), nj);
-    const size_t f2 = fast::FSmem<C, N, 2, 1>::BYTES, f1 = fast::FSmem<C, N, 1, 1>::BYTES;
+    constexpr int NT2 = fast_nt2<T, N>();
+    const size_t f2 = fast::FSmem<C, N, 2, 1, NT2>::BYTES, f1 = fast::FSmem<C, N, 1, 1>::BYTES;
     const size_t x2 = sizeof(C) * (2 * (size_t)N * TJ + fast::stw_size(N) + 1);
     const size_t x1 = sizeof(C) * ((size_t)N * TJ + fast::stw_size(N) + 1);
     if constexpr (N == r8::N) {
@@ -507,11 +515,11 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
             return 0;
         }
     }
-    fast::kf_plane_forward<T, 2, N><<<gp, NTHR, f2, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0);
+    fast::kf_plane_forward<T, 2, N, NT2><<<gp, NT2, f2, st>>>(g, jobs, s, FM_FAC_SQ, FM_FAC, 0);
     fast::kf_xpass<T, 2, N><<<gx, NTHR, x2, st>>>(g, jobs, 0, 0, 1);
     fast::kf_plane_mid<T, N><<<gp, NTHR, f1, st>>>(g, jobs, 1);
     fast::kf_xpass<T, 1, N><<<gx, NTHR, x1, st>>>(g, jobs, 1, 1, 1);
-    fast::kf_plane_inverse<T, 2, EPI_RICH, N><<<gp, NTHR, f2, st>>>(g, jobs, s, 0, 0);
+    fast::kf_plane_inverse<T, 2, EPI_RICH, N, NT2><<<gp, NT2, f2, st>>>(g, jobs, s, 0, 0);
     CKLAUNCH();
     return 0;
 }

@@ -142,28 +142,28 @@ __device__ __forceinline__ void dif(C *buf, const C *stw, int sign, int tid, int
 }
 
 // shared-memory layout of the fast plane kernels
-template <typename C, int N, int NBR, int NZL>
+template <typename C, int N, int NBR, int NZL, int NT = NTHR>
 struct FSmem {
     static constexpr int NZC = N / 2 + 1;
     static constexpr int PL = padded(N);
     static constexpr int ZB = zlines(N);
     static constexpr size_t P_ELEMS = (size_t)NBR * N * NZC;
-    static constexpr size_t Z_ELEMS = (size_t)NZL * NWARP * ZB * PL;
+    static constexpr size_t Z_ELEMS = (size_t)NZL * (NT / 32) * ZB * PL;
     static constexpr size_t BYTES = sizeof(C) * (P_ELEMS + Z_ELEMS + stw_size(N) + 1);
 };
 
-template <typename C, int N>
+template <typename C, int N, int NT = NTHR>
 __device__ __forceinline__ void load_stw(C *dst, const void *src) {
-    for (int i = threadIdx.x; i < stw_size(N); i += NTHR) dst[i] = ((const C *)src)[i];
+    for (int i = threadIdx.x; i < stw_size(N); i += NT) dst[i] = ((const C *)src)[i];
 }
 
 // ------------------------------------------------------------------------
 // K1 (fast): forward zy transform of one x-plane
-template <typename T, int NBR, int N>
-__global__ void __launch_bounds__(NTHR) kf_plane_forward(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
+template <typename T, int NBR, int N, int NT = NTHR>
+__global__ void __launch_bounds__(NT) kf_plane_forward(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
                                                          int fm0, int fm1, int spec_out0) {
     using C = typename CT<T>::type;
-    using SM = FSmem<C, N, NBR, 1>;
+    using SM = FSmem<C, N, NBR, 1, NT>;
     constexpr int NZC = SM::NZC, PL = SM::PL, ZB = SM::ZB, NU = (NBR == 2) ? N : N / 2;
     using LZ = Lines<ZB, 1, PL, 1, true, false>;
     using LY = Lines<NBR * NZC, NZC, N * NZC, NZC, false, true>;
@@ -174,12 +174,12 @@ __global__ void __launch_bounds__(NTHR) kf_plane_forward(GridPlan g, const lfts_
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    load_stw<C, N>(stw, g.stw);
+    load_stw<C, N, NT>(stw, g.stw);
     const long long poff = (long long)x * N * N;
     const T *qin = (const T *)jb.in + s * jb.in_stride + poff;
     const T *fac = (const T *)jb.fac + poff;
     C *zw = zl + warp * ZB * PL;
-    for (int u0 = warp * ZB; u0 < NU; u0 += NWARP * ZB) {
+    for (int u0 = warp * ZB; u0 < NU; u0 += (NT / 32) * ZB) {
         constexpr int PER = (N + 31) / 32;
         T qa[ZB][PER], qb[ZB][PER], fa[ZB][PER], fb[ZB][PER];
 #pragma unroll
@@ -241,12 +241,12 @@ __global__ void __launch_bounds__(NTHR) kf_plane_forward(GridPlan g, const lfts_
         __syncwarp();
     }
     __syncthreads();
-    dit<LY, N, true>(P, stw, -1, tid, NTHR);
+    dit<LY, N, true>(P, stw, -1, tid, NT);
 #pragma unroll
     for (int b = 0; b < NBR; b++) {
         C *out = (C *)jb.spec + (size_t)(spec_out0 + b) * g.Mc + (size_t)x * N * NZC;
         const C *src = P + b * N * NZC;
-        for (int i = tid; i < N * NZC; i += NTHR) out[i] = src[i];
+        for (int i = tid; i < N * NZC; i += NT) out[i] = src[i];
     }
 }
 
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(NTHR) kf_xpass(GridPlan g, const lfts_step_job
 }
 
 // load NBR spectra planes and run the inverse y transform (rows end at perm positions)
-template <typename C, int N, int NBR>
+template <typename C, int N, int NBR, int NT>
 __device__ __forceinline__ void fload_inverse_y(const GridPlan &g, const lfts_step_job &jb, int spec_in0, C *P, const C *stw) {
     constexpr int NZC = N / 2 + 1;
     using LY = Lines<NBR * NZC, NZC, N * NZC, NZC, false, true>;
@@ -309,18 +309,18 @@ __device__ __forceinline__ void fload_inverse_y(const GridPlan &g, const lfts_st
         const C *src = (const C *)jb.spec + (size_t)(spec_in0 + b) * g.Mc + (size_t)blockIdx.x * N * NZC;
         C *dst = P + b * N * NZC;
 #pragma unroll 4
-        for (int i = threadIdx.x; i < N * NZC; i += NTHR) dst[i] = src[i];
+        for (int i = threadIdx.x; i < N * NZC; i += NT) dst[i] = src[i];
     }
     __syncthreads();
-    dif<LY, N, true>(P, stw, +1, threadIdx.x, NTHR);
+    dif<LY, N, true>(P, stw, +1, threadIdx.x, NT);
 }
 
 // ------------------------------------------------------------------------
 // K3 (fast): inverse zy, multiply by e = fac^2, forward zy, in place on a spectrum slot
-template <typename T, int N>
-__global__ void __launch_bounds__(NTHR) kf_plane_mid(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_idx) {
+template <typename T, int N, int NT = NTHR>
+__global__ void __launch_bounds__(NT) kf_plane_mid(GridPlan g, const lfts_step_job *__restrict__ jobs, int spec_idx) {
     using C = typename CT<T>::type;
-    using SM = FSmem<C, N, 1, 1>;
+    using SM = FSmem<C, N, 1, 1, NT>;
     constexpr int NZC = SM::NZC, PL = SM::PL, ZB = SM::ZB, NU = N / 2;
     using LZ = Lines<ZB, 1, PL, 1, true, false>;
     using LY = Lines<NZC, NZC, N * NZC, NZC, false, true>;
@@ -331,13 +331,13 @@ __global__ void __launch_bounds__(NTHR) kf_plane_mid(GridPlan g, const lfts_step
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    load_stw<C, N>(stw, g.stw);
+    load_stw<C, N, NT>(stw, g.stw);
     __syncthreads();
-    fload_inverse_y<C, N, 1>(g, jb, spec_idx, P, stw);
+    fload_inverse_y<C, N, 1, NT>(g, jb, spec_idx, P, stw);
     const T *fac = (const T *)jb.fac + (long long)x * N * N;
     C *zw = zl + warp * ZB * PL;
     constexpr int PER = (N + 31) / 32;
-    for (int u0 = warp * ZB; u0 < NU; u0 += NWARP * ZB) {
+    for (int u0 = warp * ZB; u0 < NU; u0 += (NT / 32) * ZB) {
         T ea[ZB][PER], eb[ZB][PER];
 #pragma unroll
         for (int b = 0; b < ZB; b++) {
@@ -398,18 +398,18 @@ __global__ void __launch_bounds__(NTHR) kf_plane_mid(GridPlan g, const lfts_step
         __syncwarp();
     }
     __syncthreads();
-    dit<LY, N, true>(P, stw, -1, tid, NTHR);
+    dit<LY, N, true>(P, stw, -1, tid, NT);
     C *out = (C *)jb.spec + (size_t)spec_idx * g.Mc + (size_t)x * N * NZC;
-    for (int i = tid; i < N * NZC; i += NTHR) out[i] = P[i];
+    for (int i = tid; i < N * NZC; i += NT) out[i] = P[i];
 }
 
 // ------------------------------------------------------------------------
 // K5 (fast): inverse zy of NBR planes with the step epilogue (see k_plane_inverse)
-template <typename T, int NBR, int EPI, int N>
-__global__ void __launch_bounds__(NTHR) kf_plane_inverse(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
+template <typename T, int NBR, int EPI, int N, int NT = NTHR>
+__global__ void __launch_bounds__(NT) kf_plane_inverse(GridPlan g, const lfts_step_job *__restrict__ jobs, int s,
                                                          int spec_in0, int fm0) {
     using C = typename CT<T>::type;
-    using SM = FSmem<C, N, NBR, 1>;
+    using SM = FSmem<C, N, NBR, 1, NT>;
     constexpr int NZC = SM::NZC, PL = SM::PL, ZB = SM::ZB, NU = (NBR == 2) ? N : N / 2;
     using LZ = Lines<ZB, 1, PL, 1, true, false>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -419,15 +419,15 @@ __global__ void __launch_bounds__(NTHR) kf_plane_inverse(GridPlan g, const lfts_
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    load_stw<C, N>(stw, g.stw);
+    load_stw<C, N, NT>(stw, g.stw);
     __syncthreads();
-    fload_inverse_y<C, N, NBR>(g, jb, spec_in0, P, stw);
+    fload_inverse_y<C, N, NBR, NT>(g, jb, spec_in0, P, stw);
     const long long poff = (long long)x * N * N;
     const T *fac = (const T *)jb.fac + poff;
     T *qout = (T *)jb.out + s * jb.out_stride + poff;
     C *zw = zl + warp * ZB * PL;
     constexpr int PER = (N + 31) / 32;
-    for (int u0 = warp * ZB; u0 < NU; u0 += NWARP * ZB) {
+    for (int u0 = warp * ZB; u0 < NU; u0 += (NT / 32) * ZB) {
         T fa[ZB][PER], fb[ZB][PER], qa[ZB][PER], qb[ZB][PER];
 #pragma unroll
         for (int b = 0; b < ZB; b++) {

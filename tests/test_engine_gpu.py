@@ -15,6 +15,7 @@ GRIDS = [((5, 4, 3), (4.0, 3.0, 2.0)), ((8, 8, 8), (3.0, 3.0, 3.0)), ((32, 32, 3
          ((23, 27, 25), (3.2, 3.3, 3.4)), ((64,), (5.0,)), ((16, 12), (3.0, 2.5)), ((48, 48, 48), (5.0, 5.0, 5.0)),
          ((31, 49, 23), (4.0, 4.5, 3.5)), ((16, 16, 16), (3.0, 3.0, 3.0)), ((64, 64, 64), (7.3, 7.3, 7.3)),
          ((96, 96, 96), (8.0, 8.0, 8.0))]
+GRID_IDS = ["x".join(map(str, nx)) for nx, _ in GRIDS]
 
 
 def _ctx(nx, prec=8):
@@ -44,7 +45,7 @@ def _jobs(ctx, jobs):
     return p
 
 
-@pytest.mark.parametrize("nx,lx", GRIDS)
+@pytest.mark.parametrize("nx,lx", GRIDS, ids=GRID_IDS)
 @pytest.mark.parametrize("prec", [8, 4])
 def test_step_continuous(nx, lx, prec):
     from langevinfts_b200.capi import StepJob, check
