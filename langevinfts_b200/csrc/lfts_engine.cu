@@ -13,6 +13,7 @@
 
 #include "lfts_step_fast.cuh"
 #include "lfts_step_r8.cuh"
+#include "lfts_step_r12.cuh"
 
 using namespace lfts;
 
@@ -45,6 +46,7 @@ struct lfts_ctx_s {
     int TJ = 16, ntiles = 1, zb = 1;
     int fastN = 0;            // cubic grid handled by the compile-time specialised kernels (0: generic)
     int r8 = 0;               // 64^3: register-resident 8x8 line transforms (lfts_step_r8.cuh)
+    int r12 = 0;              // 96^3: register-resident 12x8 plane kernels (lfts_step_r12.cuh)
     int nsm = 0;              // streaming multiprocessors of the device
     void *stw = nullptr;
     size_t sm_pf1 = 0, sm_pf2 = 0, sm_mid = 0, sm_inv1 = 0, sm_inv2 = 0, sm_x1 = 0, sm_x2 = 0;
@@ -150,6 +152,15 @@ template <typename T, int N> static int fast_setup(int max_smem) {
     return 1;
 }
 
+template <typename T> static int r12_setup(int max_smem) {
+    using C = typename CT<T>::type;
+    if (r12::plane_smem<C>(r12::N) > (size_t)max_smem) return 0;
+    if (allow_smem(r12::kq_plane_forward<T, FM_FAC_SQ, FM_FAC>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r12::kq_plane_mid<T>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r12::kq_plane_inverse<T>, max_smem) != cudaSuccess) return 0;
+    return 1;
+}
+
 template <typename T> static int r8_setup(int max_smem) {
     using C = typename CT<T>::type;
     if (r8::plane_smem<C>() > (size_t)max_smem || r8::xpipe_smem<C>() > (size_t)max_smem) return 0;
@@ -247,6 +258,7 @@ template <typename T> static int setup_plan(lfts_ctx c) {
             g.stw = c->stw;
             c->fastN = N;
             if (N == 64 && !std::getenv("LFTS_NO_R8")) c->r8 = r8_setup<T>(max_smem);
+            if (N == 96 && !std::getenv("LFTS_NO_R12")) c->r12 = r12_setup<T>(max_smem);
         }
     }
     return 0;
@@ -511,6 +523,18 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
             r8::kr_plane_mid<T><<<rp, NTHR, ps, st>>>(g, jobs, 1);
             r8::kp_xpass<T, 1><<<px1, NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 1, 1, 1);
             r8::kr_plane_inverse<T, 2, EPI_RICH><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, 0);
+            CKLAUNCH();
+            return 0;
+        }
+    }
+    if constexpr (N == r12::N) {
+        if (c->r12) {
+            const size_t p2 = r12::plane_smem<C>(N), p1 = r12::plane_smem<C>(N / 2);
+            r12::kq_plane_forward<T, FM_FAC_SQ, FM_FAC><<<gp, r12::NT, p2, st>>>(g, jobs, s, 0);
+            fast::kf_xpass<T, 2, N><<<gx, NTHR, x2, st>>>(g, jobs, 0, 0, 1);
+            r12::kq_plane_mid<T><<<gp, r12::NT, p1, st>>>(g, jobs, 1);
+            fast::kf_xpass<T, 1, N><<<gx, NTHR, x1, st>>>(g, jobs, 1, 1, 1);
+            r12::kq_plane_inverse<T><<<gp, r12::NT, p2, st>>>(g, jobs, s, 0);
             CKLAUNCH();
             return 0;
         }
