@@ -158,6 +158,8 @@ template <typename T> static int r12_setup(int max_smem) {
     if (allow_smem(r12::kq_plane_forward<T, FM_FAC_SQ, FM_FAC>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r12::kq_plane_mid<T>, max_smem) != cudaSuccess) return 0;
     if (allow_smem(r12::kq_plane_inverse<T>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r12::kq_xpass<T, 1>, max_smem) != cudaSuccess) return 0;
+    if (allow_smem(r12::kq_xpass<T, 2>, max_smem) != cudaSuccess) return 0;
     return 1;
 }
 
@@ -529,11 +531,13 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
     }
     if constexpr (N == r12::N) {
         if (c->r12) {
-            const size_t p2 = r12::plane_smem<C>(N), p1 = r12::plane_smem<C>(N / 2);
+            const size_t p2 = r12::plane_smem<C>(N), p1 = r12::plane_smem<C>(N / 2), xs = r12::xpipe_smem<C>();
+            const long long it2 = (long long)nj * 2 * r12::XTILES, it1 = (long long)nj * r12::XTILES;
+            const long long cap = (long long)r12::minb_xpass<T>() * c->nsm;
             r12::kq_plane_forward<T, FM_FAC_SQ, FM_FAC><<<gp, r12::NT, p2, st>>>(g, jobs, s, 0);
-            fast::kf_xpass<T, 2, N><<<gx, NTHR, x2, st>>>(g, jobs, 0, 0, 1);
+            r12::kq_xpass<T, 2><<<(unsigned)(it2 < cap ? it2 : cap), NTHR, xs, st>>>(g, jobs, nj, 0, 0, 1);
             r12::kq_plane_mid<T><<<gp, r12::NT, p1, st>>>(g, jobs, 1);
-            fast::kf_xpass<T, 1, N><<<gx, NTHR, x1, st>>>(g, jobs, 1, 1, 1);
+            r12::kq_xpass<T, 1><<<(unsigned)(it1 < cap ? it1 : cap), NTHR, xs, st>>>(g, jobs, nj, 1, 1, 1);
             r12::kq_plane_inverse<T><<<gp, r12::NT, p2, st>>>(g, jobs, s, 0);
             CKLAUNCH();
             return 0;

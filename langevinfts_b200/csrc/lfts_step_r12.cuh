@@ -470,5 +470,151 @@ __global__ void __launch_bounds__(NT, minb_two_branch<T>()) kq_plane_inverse(Gri
     }
 }
 
+// ------------------------------------------------------------------------
+// K2 / K4, persistent and pipelined: work items are (job, branch, tile of XW
+// columns of the [kx][ky][kz] spectrum), 96 rows each.  Warp 0 bulk-loads the
+// next item into the other of two shared stages while the CTA transforms the
+// current one, and bulk-stores each finished tile.  Thread (w, l) owns column
+// l of the tile: variant A forward over rows w + 8m (warps w < 4 take the
+// second round of 8-point DFTs), the bond multiply on rows w + 12k and
+// 8 + w + 12k, then variant B inverse, which starts from exactly those rows.
+// (A split over 12 warps that balances the 8-point DFTs measured slower: one
+// CTA per SM at its FP64 register need, or spills at two.)
+constexpr int XW = 32;  // columns per item (512-byte rows in FP64, 256 in FP32)
+constexpr int XTILES = PLANE / XW;
+static_assert(PLANE % XW == 0, "x-pass tiles cover the plane exactly");
+template <typename C> constexpr size_t xpipe_smem() { return 2 * sizeof(C) * (size_t)N * XW + 16; }
+template <typename T> __host__ __device__ constexpr int minb_xpass() { return sizeof(T) == 4 ? 3 : 2; }
+
+template <typename T, int NBR>
+__global__ void __launch_bounds__(NTHR, minb_xpass<T>()) kq_xpass(GridPlan g, const lfts_step_job *__restrict__ jobs, int nj,
+                                                                  int spec_in0, int bsel0, int bsel1) {
+    using C = typename CT<T>::type;
+    constexpr uint32_t ROWB = XW * sizeof(C), TILEB = N * ROWB;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *stage = (C *)smem_raw;
+    uint64_t *bar = (uint64_t *)(stage + 2 * N * XW);
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+    const int nitems = nj * NBR * XTILES;  // < 2^31 for nj <= 65535
+    // first item at or after it whose job is active and aligned (>= nitems: none)
+    auto next_item = [&](int it) -> int {
+        for (; it < nitems; it += (int)gridDim.x) {
+            const lfts_step_job &jb = jobs[it / (NBR * XTILES)];
+            if (jb.active && !jb.active[jb.replica]) continue;
+            if (((uintptr_t)jb.spec | (uintptr_t)g.Mc * sizeof(C)) & 15) {
+                if (tid == 0) kerr_set(KERR_MISALIGNED);
+                continue;
+            }
+            return it;
+        }
+        return nitems;
+    };
+    // spectrum column block of an item: rows x at + x * PLANE
+    auto item_base = [&](int it) -> C * {
+        const int job = it / (NBR * XTILES), rem = it - job * (NBR * XTILES);
+        const int b = rem / XTILES, t = rem - b * XTILES;
+        return (C *)jobs[job].spec + (size_t)(spec_in0 + b) * g.Mc + (size_t)t * XW;
+    };
+    auto issue_load = [&](int it, int st) {  // warp 0
+        C *src = item_base(it);
+        if (l == 0) mbar_arrive_expect_tx(bar + st, TILEB);
+        __syncwarp();
+        for (int r = l; r < N; r += 32) bulk_load(stage + (st * N + r) * XW, src + (size_t)r * PLANE, ROWB, bar + st);
+    };
+    int cur = next_item(blockIdx.x);
+    if (cur >= nitems) return;
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+    }
+    __syncthreads();
+    if (w == 0) issue_load(cur, 0);
+    const C wf = tw96<C>(w, -1), vi0 = tw96<C>(w, +1), vi1 = tw96<C>(8 + w, +1);
+    for (int u = 0; cur < nitems; u++) {
+        const int st = u & 1;
+        const int nxt = next_item(cur + (int)gridDim.x);
+        if (w == 0 && nxt < nitems) {
+            bulk_wait_read();  // the previous store out of stage st ^ 1 has read it
+            __syncwarp();
+            issue_load(nxt, st ^ 1);
+        }
+        const int job = cur / (NBR * XTILES), rem = cur - job * (NBR * XTILES);
+        const int b = rem / XTILES, t = rem - b * XTILES;
+        const lfts_step_job &jb = jobs[job];
+        const T *bt = (const T *)((b == 0 ? bsel0 : bsel1) ? jb.bond_half : jb.bond) + t * XW + l;
+        if (!mbar_wait(bar + st, (u >> 1) & 1)) {
+            mbar_wait(bar + st, (u >> 1) & 1);
+            if (w == 0) bulk_wait_read();
+            return;
+        }
+        C *tb = stage + st * N * XW + l;
+        // forward: rows w + 8m -> X[w + 12k] (o0), X[8 + w + 12k] (o1, w < 4)
+        C a[12], o0[8], o1[8];
+#pragma unroll
+        for (int m = 0; m < 12; m++) a[m] = tb[(w + 8 * m) * XW];
+        dft12<-1>(a);
+        twiddle12(a, wf);
+        __syncthreads();
+#pragma unroll
+        for (int k2 = 0; k2 < 12; k2++) tb[slot(k2, w) * XW] = a[k2];
+        // bond factors of rows w + 12k and 8 + w + 12k (loaded here, not before
+        // the forward stage, to keep the FP64 register count within two CTAs)
+        T bv0[8], bv1[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) bv0[k] = bt[(w + 12 * k) * PLANE];
+        if (w < 4) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) bv1[k] = bt[(8 + w + 12 * k) * PLANE];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 8; i++) o0[i] = tb[slot(w, i) * XW];
+        SmallDFT<8, C>::run(o0, -1, nullptr, 0);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            o0[k].x *= bv0[k];
+            o0[k].y *= bv0[k];
+        }
+        if (w < 4) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) o1[i] = tb[slot(8 + w, i) * XW];
+            SmallDFT<8, C>::run(o1, -1, nullptr, 0);
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                o1[k].x *= bv1[k];
+                o1[k].y *= bv1[k];
+            }
+        }
+        // inverse, variant B: the slots rewritten here are the ones this
+        // thread has just read
+        SmallDFT<8, C>::run(o0, +1, nullptr, 0);
+        r8::twiddle8(o0, vi0);
+#pragma unroll
+        for (int k1 = 0; k1 < 8; k1++) tb[slot(w, k1) * XW] = o0[k1];
+        if (w < 4) {
+            SmallDFT<8, C>::run(o1, +1, nullptr, 0);
+            r8::twiddle8(o1, vi1);
+#pragma unroll
+            for (int k1 = 0; k1 < 8; k1++) tb[slot(8 + w, k1) * XW] = o1[k1];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int n2 = 0; n2 < 12; n2++) a[n2] = tb[slot(n2, w) * XW];
+        dft12<+1>(a);
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 12; k++) tb[(w + 8 * k) * XW] = a[k];
+        fence_proxy_async();
+        __syncthreads();
+        if (w == 0) {
+            C *dst = item_base(cur);
+            for (int r = l; r < N; r += 32) bulk_store(dst + (size_t)r * PLANE, stage + (st * N + r) * XW, ROWB);
+            bulk_commit();
+        }
+        cur = nxt;
+    }
+    if (w == 0) bulk_wait_read();
+}
+
 }  // namespace r12
 }  // namespace lfts

@@ -84,8 +84,11 @@ def test_step_continuous(nx, lx, prec):
     ctx.close()
 
 
-@pytest.mark.parametrize("nx,lx", [((64, 64, 64), (7.3, 7.3, 7.3)), ((32, 32, 32), (4.0, 4.0, 4.0)),
-                                   ((23, 27, 25), (3.2, 3.3, 3.4))])
+MASK_GRIDS = [((64, 64, 64), (7.3, 7.3, 7.3)), ((96, 96, 96), (8.0, 8.0, 8.0)), ((32, 32, 32), (4.0, 4.0, 4.0)),
+              ((23, 27, 25), (3.2, 3.3, 3.4))]
+
+
+@pytest.mark.parametrize("nx,lx", MASK_GRIDS, ids=["x".join(map(str, nx)) for nx, _ in MASK_GRIDS])
 @pytest.mark.parametrize("prec", [8, 4])
 def test_step_active_mask(nx, lx, prec):
     """Jobs of inactive replicas leave their output untouched; the others step
