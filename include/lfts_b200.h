@@ -55,6 +55,16 @@ int lfts_memcpy_h2d(lfts_ctx ctx, void *dst, const void *src, size_t bytes);
 int lfts_memcpy_d2h(lfts_ctx ctx, void *dst, const void *src, size_t bytes);
 int lfts_memcpy_d2d_async(lfts_ctx ctx, void *dst, const void *src, size_t bytes);
 int lfts_synchronize(lfts_ctx ctx);
+/* Status words read one step behind the GPU: lfts_status_post enqueues a copy
+ * of one device int into pinned host slot `slot` (< LFTS_STATUS_SLOTS) and
+ * records an event after it; lfts_status_wait waits for that event only and
+ * returns the copied value (then checks the device error word).  The device
+ * saddle loop polls its "any replica still active" word this way while the
+ * next iteration is already queued.  No counterpart in the reference, whose
+ * driver synchronises on every scalar it reads. */
+#define LFTS_STATUS_SLOTS 4
+int lfts_status_post(lfts_ctx ctx, const int *d_word, int slot);
+int lfts_status_wait(lfts_ctx ctx, int slot, int *value);
 
 /* CUDA graph capture of everything enqueued on the context stream between
  * begin and end (replaces the reference's per-step launches driven by OpenMP
@@ -264,6 +274,39 @@ int lfts_am_batch_dots(lfts_ctx ctx, int R, long long n, int L, const int *head,
 int lfts_am_batch_update(lfts_ctx ctx, int R, long long n, int L, const int *head, const int *mode, const int *nh,
                          const double *mix, const double *a, const double *w_cur, long long w_stride, const double *d_cur,
                          long long d_stride, const double *w_hist, const double *d_hist, double *w_out, long long out_stride);
+
+/* Device control of one saddle-point iteration of every replica: the host
+ * loop of examples/fts/lfts.py:807-868 with the Anderson-mixing bookkeeping of
+ * src/platforms/cpu/CpuAndersonMixing.cpp:86-121, per replica, without a host
+ * round trip.  For each replica r with active[r]:
+ *   e = max_c sqrt(max(var[r*I+c], 0)) / scale[c] (a NaN wins), err_old = err,
+ *   err = e, iter = it; e < tolerance ends the replica (active = 0); otherwise
+ *   n_anderson advances (once e < am_start_error or already >= 0, capped at
+ *   am_max_hist), head_raw advances in the ring of L = am_max_hist + 1 slots
+ *   with flag = 1, ndots = n_anderson + 1, and mode = 1 (simple mixing, mix
+ *   x0.7 floored at am_mix_min when the error grew, else x1.01) while
+ *   n_anderson <= 0, else mode = 2 with nh = n_anderson.
+ * Every replica gets head = max(head_raw, 0), and flag/ndots/mode/nh = 0 unless
+ * set above; *any_active (reset here) becomes 1 if a replica stays active.
+ * All pointers in st are device pointers; scale is host (I values). */
+typedef struct {
+    int *active, *n_anderson, *head_raw, *iter, *head, *flag, *ndots, *mode, *nh, *any_active;
+    double *err, *err_old, *mix;
+} lfts_saddle_state;
+int lfts_saddle_control(lfts_ctx ctx, int R, int I, int it, const double *var, const double *scale, double tolerance,
+                        double am_start_error, int am_max_hist, double am_mix_min, const lfts_saddle_state *st);
+/* Anderson-mixing coefficients of every replica on the device
+ * (src/common/AndersonMixing.cpp:19-47 and CpuAndersonMixing.cpp:122-146):
+ * where ndots[r] > 0 the new dot row dots[r*L + i] (i < ndots[r]) enters the
+ * ring dot_ring[r][head[r]][0..L); where mode[r] == 2, with rows k = (head - k)
+ * mod L, U_ij = r0[0] - r0[i+1] - r0[j+1] + r_{min(i,j)+1}[|i-j|] and
+ * V_i = r0[0] - r0[i+1] are solved by Gaussian elimination without pivoting, in
+ * the reference's operation order with every product and sum rounded on its
+ * own, into a[r*L + i], i < nh[r].  dot_ring: R*L*L device doubles.
+ * Holds at most LFTS_AM_SOLVE_MAX_HIST history vectors (L <= 33). */
+#define LFTS_AM_SOLVE_MAX_HIST 32
+int lfts_am_batch_solve(lfts_ctx ctx, int R, int L, const int *head, const int *ndots, const int *mode, const int *nh,
+                        const double *dots, double *dot_ring, double *a);
 
 /* Adam field update of the SCFT driver (examples/scft/scft.py:42-54), on n
  * doubles: m = b1 m + (1-b1) d; v = b2 v + (1-b2) d^2;

@@ -89,6 +89,12 @@ _SIGS = {
     "lfts_am_batch_update": [C.c_void_p, C.c_int, C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                              C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p,
                              C.c_void_p, C.c_longlong],
+    "lfts_saddle_control": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int,
+                            C.c_double, C.c_void_p],
+    "lfts_am_batch_solve": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                            C.c_void_p, C.c_void_p],
+    "lfts_status_post": [C.c_void_p, C.c_void_p, C.c_int],
+    "lfts_status_wait": [C.c_void_p, C.c_int, C.c_void_p],
 }
 
 _lib = None

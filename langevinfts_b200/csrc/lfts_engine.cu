@@ -55,6 +55,8 @@ struct lfts_ctx_s {
     lfts_step_job *sjobs = nullptr;
     int sjobs_cap = 0;
     lfts_step_job *sjobs_host = nullptr;
+    int *status_host = nullptr;           // pinned words read by lfts_status_wait
+    cudaEvent_t status_ev[LFTS_STATUS_SLOTS] = {};
     long long launches = 0;  // kernels enqueued through this context (graph replays excluded)
 };
 
@@ -299,10 +301,16 @@ extern "C" int lfts_ctx_create(lfts_ctx *out, int device, int dim, const int *nx
     c->sjobs_cap = 2048;
     if (cudaMalloc(&c->partials, sizeof(double) * c->partials_cap) != cudaSuccess ||
         cudaMalloc(&c->sjobs, sizeof(lfts_step_job) * c->sjobs_cap) != cudaSuccess ||
-        cudaMallocHost(&c->sjobs_host, sizeof(lfts_step_job) * c->sjobs_cap) != cudaSuccess) {
+        cudaMallocHost(&c->sjobs_host, sizeof(lfts_step_job) * c->sjobs_cap) != cudaSuccess ||
+        cudaMallocHost(&c->status_host, sizeof(int) * LFTS_STATUS_SLOTS) != cudaSuccess) {
         lfts_ctx_destroy(c);
         return fail("workspace allocation failed");
     }
+    for (int i = 0; i < LFTS_STATUS_SLOTS; i++)
+        if (cudaEventCreateWithFlags(&c->status_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            lfts_ctx_destroy(c);
+            return fail("event creation failed");
+        }
     *out = c;
     return 0;
 }
@@ -315,6 +323,9 @@ extern "C" int lfts_ctx_destroy(lfts_ctx c) {
     if (c->partials) cudaFree(c->partials);
     if (c->sjobs) cudaFree(c->sjobs);
     if (c->sjobs_host) cudaFreeHost(c->sjobs_host);
+    if (c->status_host) cudaFreeHost(c->status_host);
+    for (int i = 0; i < LFTS_STATUS_SLOTS; i++)
+        if (c->status_ev[i]) cudaEventDestroy(c->status_ev[i]);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return 0;
@@ -376,6 +387,20 @@ extern "C" int lfts_memcpy_d2h(lfts_ctx c, void *dst, const void *src, size_t by
 extern "C" int lfts_memcpy_d2d_async(lfts_ctx c, void *dst, const void *src, size_t bytes) {
     CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
     return 0;
+}
+extern "C" int lfts_status_post(lfts_ctx c, const int *d_word, int slot) {
+    if (!c || !d_word) return fail("null argument");
+    if (slot < 0 || slot >= LFTS_STATUS_SLOTS) return fail("status slot out of range");
+    CK(cudaMemcpyAsync(c->status_host + slot, d_word, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaEventRecord(c->status_ev[slot], c->stream));
+    return 0;
+}
+extern "C" int lfts_status_wait(lfts_ctx c, int slot, int *value) {
+    if (!c || !value) return fail("null argument");
+    if (slot < 0 || slot >= LFTS_STATUS_SLOTS) return fail("status slot out of range");
+    CK(cudaEventSynchronize(c->status_ev[slot]));
+    *value = c->status_host[slot];
+    return check_kernel_errors();
 }
 extern "C" int lfts_synchronize(lfts_ctx c) {
     CK(cudaStreamSynchronize(c->stream));

@@ -230,6 +230,107 @@ __global__ void k_am_batch_update(int R, long long n, int L, const int *__restri
     }
 }
 
+// ---- device control of the saddle-point loop (one thread per replica)
+struct SaddleArgs {
+    lfts_saddle_state st;
+    double scale[LFTS_MAX_MONOMERS];
+    double tol, start, mix_min;
+    int R, I, it, maxh, L;
+};
+
+__global__ void k_saddle_control(SaddleArgs a, const double *__restrict__ var) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.R) return;
+    const lfts_saddle_state &s = a.st;
+    s.flag[r] = 0;
+    s.ndots[r] = 0;
+    s.mode[r] = 0;
+    s.nh[r] = 0;
+    if (s.active[r]) {
+        double e = 0.0;
+        for (int c = 0; c < a.I; c++) {
+            const double v = var[(long long)r * a.I + c];
+            const double sd = sqrt(v < 0.0 ? 0.0 : v) / a.scale[c];  // a NaN variance stays NaN
+            e = (c == 0 || sd > e || isnan(sd)) ? sd : e;
+        }
+        const double eo = s.err[r];
+        s.err_old[r] = eo;
+        s.err[r] = e;
+        s.iter[r] = a.it;
+        if (e < a.tol) {
+            s.active[r] = 0;  // converged: fields and statistics stay as they are
+        } else {
+            int na = s.n_anderson[r];
+            if (e < a.start || na >= 0) na++;
+            if (na >= 0) {
+                na = na < a.maxh ? na : a.maxh;
+                s.head_raw[r] = (s.head_raw[r] + 1) % a.L;
+                s.flag[r] = 1;
+                s.ndots[r] = na + 1;
+            }
+            if (na <= 0) {
+                const double m = s.mix[r], m7 = m * 0.7;
+                s.mix[r] = (eo < e) ? (m7 < a.mix_min ? a.mix_min : m7) : m * 1.01;
+                s.mode[r] = 1;
+            } else {
+                s.mode[r] = 2;
+                s.nh[r] = na;
+            }
+            s.n_anderson[r] = na;
+            atomicOr(s.any_active, 1);
+        }
+    }
+    s.head[r] = s.head_raw[r] > 0 ? s.head_raw[r] : 0;
+}
+
+// Largest Anderson history the device solve holds (shared memory of one block).
+constexpr int AM_SOLVE_MAX = LFTS_AM_SOLVE_MAX_HIST;
+
+// One block of 32 threads per replica; U and V in shared memory.  The threads
+// split the rows j of each elimination step i, which leaves every element's
+// sequence of operations that of the serial loop.
+__global__ void k_am_solve(int R, int L, const int *__restrict__ head, const int *__restrict__ ndots,
+                           const int *__restrict__ mode, const int *__restrict__ nh, const double *__restrict__ dots,
+                           double *__restrict__ dot_ring, double *__restrict__ a) {
+    __shared__ double u[AM_SOLVE_MAX][AM_SOLVE_MAX + 1], v[AM_SOLVE_MAX], x[AM_SOLVE_MAX];
+    const int r = blockIdx.x, t = threadIdx.x;
+    const int nd = ndots[r];
+    if (nd == 0) return;
+    const int hd = head[r];
+    double *row0 = dot_ring + ((long long)r * L + hd) * L;
+    for (int i = t; i < nd; i += 32) row0[i] = dots[(long long)r * L + i];
+    __syncthreads();
+    if (mode[r] != 2) return;
+    const int n = nh[r];
+    for (int e = t; e < n * n; e += 32) {
+        const int i = e / n, j = e - i * n;
+        const int k = (i < j ? i : j) + 1, d = i > j ? i - j : j - i;
+        const double *rk = dot_ring + ((long long)r * L + ((hd - k) % L + L) % L) * L;
+        u[i][j] = row0[0] - row0[i + 1] - row0[j + 1] + rk[d];
+    }
+    for (int i = t; i < n; i += 32) v[i] = row0[0] - row0[i + 1];
+    __syncthreads();
+    // elimination without pivoting; products and sums rounded separately (no
+    // fused multiply-add), as the host computes them
+    for (int i = 0; i < n; i++) {
+        for (int j = i + 1 + t; j < n; j += 32) {
+            const double f = u[j][i] / u[i][i];
+            v[j] = __dsub_rn(v[j], __dmul_rn(v[i], f));
+            for (int k = i + 1; k < n; k++) u[j][k] = __dsub_rn(u[j][k], __dmul_rn(u[i][k], f));
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        x[n - 1] = v[n - 1] / u[n - 1][n - 1];
+        for (int i = n - 2; i >= 0; i--) {
+            double sum = 0.0;
+            for (int j = i + 1; j < n; j++) sum = __dadd_rn(sum, __dmul_rn(u[i][j], x[j]));
+            x[i] = (v[i] - sum) / u[i][i];
+        }
+        for (int i = 0; i < n; i++) a[(long long)r * L + i] = x[i];
+    }
+}
+
 int grid1(long long n, int cap) {
     long long b = (n + NT - 1) / NT;
     if (b > cap) b = cap;
@@ -345,6 +446,40 @@ extern "C" int lfts_am_batch_update(lfts_ctx ctx, int R, long long n, int L, con
                                     double *w_out, long long out_stride) {
     k_am_batch_update<<<dim3(grid1(n, 1024), R), NT, 0, (cudaStream_t)lfts_ctx_stream(ctx)>>>(
         R, n, L, head, mode, nh, mix, a, w_cur, w_stride, d_cur, d_stride, w_hist, d_hist, w_out, out_stride);
+    lfts_internal_count(ctx, 1);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_saddle_control(lfts_ctx ctx, int R, int I, int it, const double *var, const double *scale, double tolerance,
+                                   double am_start_error, int am_max_hist, double am_mix_min, const lfts_saddle_state *st) {
+    if (!ctx || !var || !scale || !st) return lfts_internal_fail("null argument");
+    if (R < 1 || I < 1 || I > LFTS_MAX_MONOMERS) return lfts_internal_fail("saddle control: bad replica or field count");
+    if (am_max_hist < 0) return lfts_internal_fail("saddle control: am_max_hist must be >= 0");
+    SaddleArgs a;
+    a.st = *st;
+    for (int c = 0; c < I; c++) a.scale[c] = scale[c];
+    a.tol = tolerance;
+    a.start = am_start_error;
+    a.mix_min = am_mix_min;
+    a.R = R;
+    a.I = I;
+    a.it = it;
+    a.maxh = am_max_hist;
+    a.L = am_max_hist + 1;
+    cudaStream_t s = (cudaStream_t)lfts_ctx_stream(ctx);
+    LCK(cudaMemsetAsync(st->any_active, 0, sizeof(int), s));
+    k_saddle_control<<<(R + 63) / 64, 64, 0, s>>>(a, var);
+    lfts_internal_count(ctx, 1);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_am_batch_solve(lfts_ctx ctx, int R, int L, const int *head, const int *ndots, const int *mode, const int *nh,
+                                   const double *dots, double *dot_ring, double *a) {
+    if (!ctx || !head || !ndots || !mode || !nh || !dots || !dot_ring || !a) return lfts_internal_fail("null argument");
+    if (L < 1 || L - 1 > AM_SOLVE_MAX) return lfts_internal_fail("device Anderson solve holds at most 32 history vectors");
+    k_am_solve<<<R, 32, 0, (cudaStream_t)lfts_ctx_stream(ctx)>>>(R, L, head, ndots, mode, nh, dots, dot_ring, a);
     lfts_internal_count(ctx, 1);
     LCK(cudaPeekAtLastError());
     return 0;

@@ -48,6 +48,11 @@ class BatchedLangevin {
     void get_fields(double *w_aux) const;
     void get_concentrations(double *phi) const;  // host [R][S][M], monomer_types order
     SaddleStats find_saddle_point(bool restore_on_failure = false);
+    // Saddle-point control on the host (one round trip per iteration for the
+    // errors and one for the Anderson dots) instead of on the device; the two
+    // give the same iterates.  The host form also serves am_max_hist > 32.
+    void set_host_control(bool on) { host_control_ = on; }
+    bool host_control() const { return host_control_; }
     // One Langevin step of every replica; noise host [R][n_real][M] (the draw of this step)
     SaddleStats step(const double *noise);
     // Same, with this step's noise already on the device ([R][n_real][M] doubles)
@@ -73,6 +78,8 @@ class BatchedLangevin {
 
    private:
     void am_reset();
+    void saddle_loop_host(SaddleStats &st);
+    void saddle_loop_device(SaddleStats &st);
     double hamiltonian(int r, const std::vector<double> &mean, const std::vector<double> &msq, const std::vector<double> &Q) const;
 
     LangevinConfig cfg_;
@@ -82,6 +89,10 @@ class BatchedLangevin {
     lfts_ctx ctx_;
     Molecules *mol_;
     DevBuf w_aux_, w_save_, phi_save_, d_cur_, xi_[2], partials_, stats_, ctl_, am_w_, am_d_, am_dots_, am_a_;
+    // device saddle control: n_anderson, head_raw, iter (R ints each) + the
+    // any-active word; err, err_old (R doubles each); dot ring R*L*L
+    DevBuf sint_, sdbl_, dot_ring_;
+    bool host_control_ = false;
     int xi_cur_ = 0;
     std::vector<double *> phi_ptrs_, w_mono_ptrs_;
     // per replica Anderson-mixing control (CpuAndersonMixing.cpp:76-161)

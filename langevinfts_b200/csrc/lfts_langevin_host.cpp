@@ -66,6 +66,9 @@ BatchedLangevin::BatchedLangevin(ComputationBox *cb, Molecules *mol, PropagatorA
     am_d_.alloc(ctx_, sizeof(double) * (size_t)R_ * L_ * I_ * M_);
     am_dots_.alloc(ctx_, sizeof(double) * (size_t)R_ * L_);
     am_a_.alloc(ctx_, sizeof(double) * (size_t)R_ * (L_ + 1));
+    sint_.alloc(ctx_, sizeof(int) * ((size_t)3 * R_ + 1));
+    sdbl_.alloc(ctx_, sizeof(double) * (size_t)2 * R_);
+    dot_ring_.alloc(ctx_, sizeof(double) * (size_t)R_ * L_ * L_);
     for (const auto &t : cfg.monomer_types) {
         phi_ptrs_.push_back(comp_->phi_type_device(t));
         w_mono_ptrs_.push_back(comp_->w_device(t));
@@ -79,6 +82,7 @@ BatchedLangevin::BatchedLangevin(ComputationBox *cb, Molecules *mol, PropagatorA
 BatchedLangevin::~BatchedLangevin() {
     w_aux_.release(); w_save_.release(); phi_save_.release(); d_cur_.release(); xi_[0].release(); xi_[1].release();
     partials_.release(); stats_.release(); ctl_.release(); am_w_.release(); am_d_.release(); am_dots_.release(); am_a_.release();
+    sint_.release(); sdbl_.release(); dot_ring_.release();
     comp_.reset();
 }
 
@@ -121,6 +125,43 @@ SaddleStats BatchedLangevin::find_saddle_point(bool restore_on_failure) {
     st.iterations.assign(R_, 0);
     st.error.assign(R_, 1e20);
     st.failed.assign(R_, 0);
+    if (host_control_ || cfg_.am_max_hist > LFTS_AM_SOLVE_MAX_HIST) saddle_loop_host(st);
+    else saddle_loop_device(st);
+    double *d_mean = stats_.as<double>(), *d_var = d_mean + (size_t)R_ * S_;
+    // Hamiltonian at the final fields (before the pressure shift, as the reference prints it)
+    check_rc(lfts_lfts_row_moments(ctx_, w_aux_.as<double>(), R_, S_, M_, M_, (long long)S_ * M_, nullptr, partials_.as<double>(),
+                                   d_mean, d_var));
+    std::vector<double> mean((size_t)R_ * S_), msq((size_t)R_ * S_);
+    check_rc(lfts_memcpy_d2h(ctx_, mean.data(), d_mean, sizeof(double) * mean.size()));
+    check_rc(lfts_memcpy_d2h(ctx_, msq.data(), d_var, sizeof(double) * msq.size()));
+    st.partitions = comp_->partitions_host();
+    st.aux_mean = mean;
+    st.aux_msq = msq;
+    st.hamiltonian.resize(R_);
+    for (int r = 0; r < R_; r++) st.hamiltonian[r] = hamiltonian(r, mean, msq, st.partitions);
+    // zero-mean pressure field of every replica (lfts.py:866)
+    std::vector<double> pmean(R_);
+    for (int r = 0; r < R_; r++) pmean[r] = mean[(size_t)r * S_ + S_ - 1];
+    check_rc(lfts_memcpy_h2d(ctx_, d_mean, pmean.data(), sizeof(double) * R_));
+    check_rc(lfts_lfts_subtract_mean(ctx_, w_aux_.as<double>(), R_, S_, S_ - 1, M_, d_mean, nullptr));
+    for (int r = 0; r < R_; r++) st.failed[r] = (std::isnan(st.error[r]) || st.error[r] >= cfg_.tolerance) ? 1 : 0;
+    if (restore_on_failure) {
+        const size_t SM = (size_t)S_ * M_;
+        for (int r = 0; r < R_; r++) {
+            if (!st.failed[r]) continue;
+            check_rc(lfts_memcpy_d2d_async(ctx_, w_aux_.as<double>() + r * SM, w_save_.as<double>() + r * SM, sizeof(double) * SM));
+            for (int s = 0; s < S_; s++)
+                check_rc(lfts_memcpy_d2d_async(ctx_, phi_ptrs_[s] + (size_t)r * M_, phi_save_.as<double>() + r * SM + (size_t)s * M_,
+                                               sizeof(double) * M_));
+        }
+    }
+    check_rc(lfts_synchronize(ctx_));
+    return st;
+}
+
+// The saddle-point iterations with the per-replica control on the host: one
+// round trip per iteration for the errors and one for the Anderson dots.
+void BatchedLangevin::saddle_loop_host(SaddleStats &st) {
     am_reset();
     const long long nI = (long long)I_ * M_;
     std::vector<int> active(R_, 1), head_flag(R_), ndots(R_), mode(R_), nh(R_);
@@ -225,35 +266,83 @@ SaddleStats BatchedLangevin::find_saddle_point(bool restore_on_failure) {
                                       d_cur_.as<double>(), nI, am_w_.as<double>(), am_d_.as<double>(), w_imag,
                                       (long long)S_ * M_));
     }
-    // Hamiltonian at the final fields (before the pressure shift, as the reference prints it)
-    check_rc(lfts_lfts_row_moments(ctx_, w_aux_.as<double>(), R_, S_, M_, M_, (long long)S_ * M_, nullptr, partials_.as<double>(),
-                                   d_mean, d_var));
-    std::vector<double> mean((size_t)R_ * S_), msq((size_t)R_ * S_);
-    check_rc(lfts_memcpy_d2h(ctx_, mean.data(), d_mean, sizeof(double) * mean.size()));
-    check_rc(lfts_memcpy_d2h(ctx_, msq.data(), d_var, sizeof(double) * msq.size()));
-    st.partitions = comp_->partitions_host();
-    st.aux_mean = mean;
-    st.aux_msq = msq;
-    st.hamiltonian.resize(R_);
-    for (int r = 0; r < R_; r++) st.hamiltonian[r] = hamiltonian(r, mean, msq, st.partitions);
-    // zero-mean pressure field of every replica (lfts.py:866)
-    std::vector<double> pmean(R_);
-    for (int r = 0; r < R_; r++) pmean[r] = mean[(size_t)r * S_ + S_ - 1];
-    check_rc(lfts_memcpy_h2d(ctx_, d_mean, pmean.data(), sizeof(double) * R_));
-    check_rc(lfts_lfts_subtract_mean(ctx_, w_aux_.as<double>(), R_, S_, S_ - 1, M_, d_mean, nullptr));
-    for (int r = 0; r < R_; r++) st.failed[r] = (std::isnan(st.error[r]) || st.error[r] >= cfg_.tolerance) ? 1 : 0;
-    if (restore_on_failure) {
-        const size_t SM = (size_t)S_ * M_;
-        for (int r = 0; r < R_; r++) {
-            if (!st.failed[r]) continue;
-            check_rc(lfts_memcpy_d2d_async(ctx_, w_aux_.as<double>() + r * SM, w_save_.as<double>() + r * SM, sizeof(double) * SM));
-            for (int s = 0; s < S_; s++)
-                check_rc(lfts_memcpy_d2d_async(ctx_, phi_ptrs_[s] + (size_t)r * M_, phi_save_.as<double>() + r * SM + (size_t)s * M_,
-                                               sizeof(double) * M_));
+}
+
+// The same iterations with the control on the device (lfts_saddle_control,
+// lfts_am_batch_solve): no host round trip inside an iteration.  The host
+// polls the "any replica active" word of iteration it - 1 while iteration it
+// is queued; an iteration queued after the last replica converged changes
+// nothing (every kernel skips inactive replicas or recomputes the same values).
+void BatchedLangevin::saddle_loop_device(SaddleStats &st) {
+    const long long nI = (long long)I_ * M_;
+    int *d_active = comp_->active_device();
+    int *d_head = ctl_.as<int>(), *d_flag = d_head + R_, *d_ndots = d_flag + R_, *d_mode = d_ndots + R_, *d_nh = d_mode + R_;
+    double *d_mix = am_a_.as<double>(), *d_a = d_mix + R_;
+    double *d_mean = stats_.as<double>(), *d_var = d_mean + (size_t)R_ * S_;
+    double *w_imag = w_aux_.as<double>() + (size_t)(S_ - I_) * M_;
+    std::vector<double> scale(I_);
+    for (int c = 0; c < I_; c++) scale[c] = cfg_.dt_scaling[cfg_.imag_idx[c]];
+    lfts_saddle_state ss;
+    int *si = sint_.as<int>();
+    ss.active = d_active;
+    ss.n_anderson = si;
+    ss.head_raw = si + R_;
+    ss.iter = si + 2 * R_;
+    ss.any_active = si + 3 * R_;
+    ss.head = d_head;
+    ss.flag = d_flag;
+    ss.ndots = d_ndots;
+    ss.mode = d_mode;
+    ss.nh = d_nh;
+    ss.err = sdbl_.as<double>();
+    ss.err_old = ss.err + R_;
+    ss.mix = d_mix;
+    // initial state of every replica: active, no Anderson history (am_reset)
+    {
+        std::vector<int> ints((size_t)3 * R_);
+        std::fill(ints.begin(), ints.begin() + 2 * R_, -1);
+        std::vector<int> ones(R_, 1);
+        std::vector<double> err((size_t)2 * R_, 1e20), mix(R_, cfg_.am_mix_init);
+        check_rc(lfts_memcpy_h2d(ctx_, si, ints.data(), sizeof(int) * ints.size()));
+        check_rc(lfts_memcpy_h2d(ctx_, d_active, ones.data(), sizeof(int) * R_));
+        check_rc(lfts_memcpy_h2d(ctx_, ss.err, err.data(), sizeof(double) * err.size()));
+        check_rc(lfts_memcpy_h2d(ctx_, d_mix, mix.data(), sizeof(double) * R_));
+    }
+    for (int it = 1; it <= cfg_.max_iter; it++) {
+        check_rc(lfts_lfts_monomer_fields(ctx_, R_, S_, M_, cfg_.A.data(), w_aux_.as<double>(), w_mono_ptrs_.data()));
+        comp_->enqueue_statistics();
+        check_rc(lfts_lfts_field_deriv(ctx_, R_, S_, M_, I_, cfg_.imag_idx.data(), scale.data(), cfg_.A.data(),
+                                       cfg_.h_coef_mu1.data(), cfg_.h_coef_mu2.data(), w_aux_.as<double>(),
+                                       (const double *const *)phi_ptrs_.data(), d_cur_.as<double>(), d_active));
+        check_rc(lfts_lfts_row_moments(ctx_, d_cur_.as<double>(), R_, I_, M_, M_, nI, nullptr, partials_.as<double>(), d_mean,
+                                       d_var));
+        check_rc(lfts_lfts_row_moments(ctx_, d_cur_.as<double>(), R_, I_, M_, M_, nI, d_mean, partials_.as<double>(),
+                                       stats_.as<double>() + 2 * (size_t)R_ * S_, d_var));
+        check_rc(lfts_saddle_control(ctx_, R_, I_, it, d_var, scale.data(), cfg_.tolerance, cfg_.am_start_error,
+                                     cfg_.am_max_hist, cfg_.am_mix_min, &ss));
+        check_rc(lfts_am_batch_insert(ctx_, R_, nI, L_, d_head, d_flag, w_imag, (long long)S_ * M_, d_cur_.as<double>(), nI,
+                                      am_w_.as<double>(), am_d_.as<double>()));
+        check_rc(lfts_am_batch_dots(ctx_, R_, nI, L_, d_head, d_ndots, am_d_.as<double>(), partials_.as<double>(),
+                                    am_dots_.as<double>()));
+        check_rc(lfts_am_batch_solve(ctx_, R_, L_, d_head, d_ndots, d_mode, d_nh, am_dots_.as<double>(), dot_ring_.as<double>(),
+                                     d_a));
+        check_rc(lfts_am_batch_update(ctx_, R_, nI, L_, d_head, d_mode, d_nh, d_mix, d_a, w_imag, (long long)S_ * M_,
+                                      d_cur_.as<double>(), nI, am_w_.as<double>(), am_d_.as<double>(), w_imag,
+                                      (long long)S_ * M_));
+        check_rc(lfts_status_post(ctx_, ss.any_active, it % LFTS_STATUS_SLOTS));
+        if (it >= 2) {
+            int any = 1;
+            check_rc(lfts_status_wait(ctx_, (it - 1) % LFTS_STATUS_SLOTS, &any));
+            if (!any) break;  // iteration it, already queued, finds no active replica
         }
     }
-    check_rc(lfts_synchronize(ctx_));
-    return st;
+    std::vector<int> iter(R_);
+    check_rc(lfts_memcpy_d2h(ctx_, iter.data(), ss.iter, sizeof(int) * R_));
+    check_rc(lfts_memcpy_d2h(ctx_, st.error.data(), ss.err, sizeof(double) * R_));
+    st.iterations.assign(iter.begin(), iter.end());
+    // leave every replica active for propagator computations outside the loop
+    const std::vector<int> ones(R_, 1);
+    check_rc(lfts_memcpy_h2d(ctx_, d_active, ones.data(), sizeof(int) * R_));
 }
 
 SaddleStats BatchedLangevin::step(const double *noise) {

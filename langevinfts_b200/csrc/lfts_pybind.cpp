@@ -389,6 +389,8 @@ PYBIND11_MODULE(langevinfts, m) {
             return new BatchedLangevin(cb, mol, pa, f.precision, f.device, n_replicas, cfg);
         }), py::keep_alive<1, 3>(), py::keep_alive<1, 4>(), py::keep_alive<1, 5>())
         .def("n_replicas", &BatchedLangevin::n_replicas)
+        .def("set_host_control", &BatchedLangevin::set_host_control)
+        .def("host_control", &BatchedLangevin::host_control)
         .def("stream_ptr", [](BatchedLangevin &b) { return (std::uintptr_t)b.stream(); })
         .def("kernel_launches", [](BatchedLangevin &b) { return b.computation().kernel_launches(); })
         .def("context_ptr", [](BatchedLangevin &b) { return (std::uintptr_t)b.computation().context(); })

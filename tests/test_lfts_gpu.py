@@ -81,6 +81,34 @@ def test_batched_replicas_follow_their_own_reference_trajectories():
             assert np.max(np.abs(w[r] - refs[r][k][3])) < 1e-8 * np.max(np.abs(refs[r][k][3]))
 
 
+@pytest.mark.parametrize("seeds", [[31, 32, 33, 34], [35]])
+def test_device_saddle_control_matches_host_control(seeds):
+    """The saddle loop with its per-replica control and Anderson solve on the
+    device (lfts_saddle_control, lfts_am_batch_solve; no host round trip inside
+    an iteration) gives the iterates of the same loop controlled from the host:
+    equal iteration counts, fields and errors to 1e-12.  One replica exercises
+    the step launches without an active mask."""
+    from langevinfts_b200 import langevinfts as L
+    from langevinfts_b200.lfts import BatchedLFTS
+    p = small_params()
+    runs = []
+    for host in (True, False):
+        sim = BatchedLFTS(p, seeds, module=L)
+        sim.engine.set_host_control(host)
+        assert sim.engine.host_control() == host
+        st = sim.start([init(s, sim.M) for s in seeds])
+        hist = [(list(st["iterations"]), np.array(st["error"]), sim.fields())]
+        for _ in range(3):
+            st = sim.step()
+            assert not any(st["failed"])
+            hist.append((list(st["iterations"]), np.array(st["error"]), sim.fields()))
+        runs.append(hist)
+    for (ih, eh, wh), (idv, ed, wd) in zip(*runs):
+        assert ih == idv
+        np.testing.assert_allclose(ed, eh, rtol=1e-12)
+        assert np.max(np.abs(wd - wh)) <= 1e-12 * np.max(np.abs(wh))
+
+
 def test_failed_saddle_point_restores_fields():
     """max_iter too small: the step fails and the fields go back (lfts.py:713-730)."""
     from langevinfts_b200 import langevinfts as L
