@@ -121,6 +121,16 @@ typedef struct {
  * CudaSolverPseudo::advance_propagator_continuous (CudaSolverPseudo.cu:345-412)
  * and CpuSolverPseudo::advance_propagator_continuous (CpuSolverPseudo.cpp:120-188). */
 int lfts_step_continuous(lfts_ctx ctx, const lfts_step_job *jobs, int njobs, int s);
+/* Step autotuner (no counterpart in the reference, whose cuFFT plans are fixed):
+ * times lfts_step_continuous for every implementation this grid supports
+ * (register-resident line transforms at 64^3 / 96^3 with their x-pass CTA
+ * residencies, the compile-time cubic kernels, the generic mixed-radix
+ * kernels) on njobs synthetic jobs, reps timed calls each, and makes the
+ * fastest the context's step implementation (continuous and discrete).  The
+ * most specialised one stays unless another is more than 5 % faster.  It
+ * allocates and frees its own buffers, synchronises, and must not run inside a
+ * graph capture.  report (may be NULL) receives the timings and the choice. */
+int lfts_autotune(lfts_ctx ctx, int njobs, int reps, char *report, size_t report_cap);
 /* Discrete chain: out = [fac *] F^-1[ b * F[in] ] with b = bond (half=0) or
  * bond_half (half=1), multiplied by fac when with_fac=1.  (half=0, with_fac=1)
  * replaces advance_propagator_discrete (CudaSolverPseudo.cu:413-450);

@@ -95,6 +95,7 @@ _SIGS = {
                             C.c_void_p, C.c_void_p],
     "lfts_status_post": [C.c_void_p, C.c_void_p, C.c_int],
     "lfts_status_wait": [C.c_void_p, C.c_int, C.c_void_p],
+    "lfts_autotune": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_size_t],
 }
 
 _lib = None

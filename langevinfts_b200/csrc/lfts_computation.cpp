@@ -321,6 +321,7 @@ void GpuComputation::build_plan() {
     }
     // per-job spectra scratch; patch spec indices into device addresses
     spec_.alloc(ctx_, (size_t)max_jobs * 2 * Mc_ * 2 * esz_);
+    max_jobs_ = max_jobs;
     for (auto &L : plan_) {
         if (L.kind != 1 && L.kind != 2) continue;
         auto *jobs = (lfts_step_job *)(arena_host_.data() + L.jobs);
@@ -529,6 +530,13 @@ void GpuComputation::enqueue_concentrations() {
         }
         check_rc(lfts_lincomb(ctx_, kv.second.as<double>(), (int)srcs.size(), srcs.data(), nullptr, (long long)M_ * R_));
     }
+}
+
+std::string GpuComputation::autotune(int reps) {
+    if (stats_graph_ || graph_) LFTS_THROW("autotune must run before the first propagator computation (captured graphs keep their kernels)");
+    char buf[512];
+    check_rc(lfts_autotune(ctx_, max_jobs_, reps, buf, sizeof buf));
+    return std::string(buf);
 }
 
 void GpuComputation::enqueue_statistics() {

@@ -91,6 +91,11 @@ class GpuComputation {
     std::vector<double> partitions_host();
     // kernels launched so far: direct launches + kernels replayed in graphs
     long long kernel_launches() const { return lfts_ctx_launches(ctx_) + graph_kernels_replayed_; }
+    // largest step launch of the schedule (jobs), the batch lfts_autotune times
+    int max_jobs_per_launch() const { return max_jobs_; }
+    // time the step implementations at that batch and keep the fastest (before
+    // the first captured graph); returns lfts_autotune's report
+    std::string autotune(int reps = 5);
 
    private:
     struct KeyStore {
@@ -139,6 +144,7 @@ class GpuComputation {
     std::map<BlockKey, DevBuf> phi_block_;
     std::map<std::string, DevBuf> phi_type_;
     std::vector<DevBuf> phi_solvent_;
+    int max_jobs_ = 1;
     DevBuf active_, phi_tmp_, spec_, arena_, dev_scalars_, basis_, phi_jobs_, coefs_, stress_jobs_, stress_out_, stress_spec_;
     std::vector<Launch> plan_;
     size_t phi_jobs_cont_ = 0, phi_jobs_disc_ = 0, coef_off_ = 0;

@@ -48,6 +48,7 @@ struct lfts_ctx_s {
     int r8 = 0;               // 64^3: register-resident 8x8 line transforms (lfts_step_r8.cuh)
     int r12 = 0;              // 96^3: register-resident 12x8 plane kernels (lfts_step_r12.cuh)
     int nsm = 0;              // streaming multiprocessors of the device
+    int xcap = 0;             // CTAs per SM of the persistent x-passes (0: the kernel's own residency)
     void *stw = nullptr;
     size_t sm_pf1 = 0, sm_pf2 = 0, sm_mid = 0, sm_inv1 = 0, sm_inv2 = 0, sm_x1 = 0, sm_x2 = 0;
     double *partials = nullptr;
@@ -543,7 +544,7 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
         if (c->r8) {
             const dim3 rp(N, nj);
             const size_t ps = r8::plane_smem<C>();
-            const long long it2 = (long long)nj * 2 * r8::xpipe_tiles<C>(), it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = 3LL * c->nsm;
+            const long long it2 = (long long)nj * 2 * r8::xpipe_tiles<C>(), it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = (long long)(c->xcap ? c->xcap : 3) * c->nsm;
             const dim3 px2((unsigned)(it2 < cap ? it2 : cap)), px1((unsigned)(it1 < cap ? it1 : cap));
             r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC><<<rp, NTHR, ps, st>>>(g, jobs, s, 0);
             r8::kp_xpass<T, 2><<<px2, NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, 0, 1);
@@ -558,7 +559,7 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
         if (c->r12) {
             const size_t p2 = r12::plane_smem<C>(N), p1 = r12::plane_smem<C>(N / 2), xs = r12::xpipe_smem<C>();
             const long long it2 = (long long)nj * 2 * r12::XTILES, it1 = (long long)nj * r12::XTILES;
-            const long long cap = (long long)r12::minb_xpass<T>() * c->nsm;
+            const long long cap = (long long)(c->xcap ? c->xcap : r12::minb_xpass<T>()) * c->nsm;
             r12::kq_plane_forward<T, FM_FAC_SQ, FM_FAC><<<gp, r12::NT, p2, st>>>(g, jobs, s, 0);
             r12::kq_xpass<T, 2><<<(unsigned)(it2 < cap ? it2 : cap), NTHR, xs, st>>>(g, jobs, nj, 0, 0, 1);
             r12::kq_plane_mid<T><<<gp, r12::NT, p1, st>>>(g, jobs, 1);
@@ -590,7 +591,7 @@ static int step_disc_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, 
             const dim3 rp(N, nj);
             const size_t ps = r8::plane_smem<C>();
             r8::kr_plane_forward<T, 1, FM_NONE, FM_NONE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0);
-            const long long it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = 3LL * c->nsm;
+            const long long it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = (long long)(c->xcap ? c->xcap : 3) * c->nsm;
             r8::kp_xpass<T, 1><<<(unsigned)(it1 < cap ? it1 : cap), NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, half, half);
             r8::kr_plane_inverse<T, 1, EPI_SCALE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
             CKLAUNCH();
@@ -1193,4 +1194,128 @@ extern "C" int lfts_dots_static(int precision, long long M, const lfts_dot_job *
                                            1.0, out, 1, 1);
     CKLAUNCH();
     return 0;
+}
+
+// ---------------------------------------------------------------- autotuner
+// Times lfts_step_continuous for every step family the grid supports, and the
+// persistent x-pass residency of the register families, on njobs synthetic
+// jobs (q = 1, fac = 1, bond tables of a box of edge n), and keeps the fastest.
+// The most specialised family (register-resident, then cubic, then generic) is
+// the default; another one is taken only when it is more than 5 % faster, so
+// the choice (and with it the last bits of the results) is stable.
+namespace {
+struct TuneCand {
+    int fastN, r8, r12, xcap;
+    const char *name;
+};
+}  // namespace
+
+extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size_t report_cap) {
+    if (!c) return fail("null context");
+    if (njobs < 1 || njobs > 65535) return fail("autotune: njobs must be 1..65535");
+    if (reps < 1) reps = 5;
+    const int fastN = c->fastN, r8v = c->r8, r12v = c->r12, xcap0 = c->xcap;
+    std::vector<TuneCand> cands;
+    if (r8v) {
+        cands.push_back({fastN, 1, 0, 0, "register-64"});
+        cands.push_back({fastN, 1, 0, 2, "register-64 xcap2"});
+    }
+    if (r12v) {
+        cands.push_back({fastN, 0, 1, 0, "register-96"});
+        cands.push_back({fastN, 0, 1, 1, "register-96 xcap1"});
+    }
+    if (fastN) cands.push_back({fastN, 0, 0, 0, "cubic"});
+    cands.push_back({0, 0, 0, 0, "generic"});
+    const size_t sb = (size_t)c->prec, M = (size_t)c->g.M, Mc = (size_t)c->g.Mc;
+    void *q = nullptr, *fac = nullptr, *bond = nullptr, *spec = nullptr, *w = nullptr;
+    lfts_step_job *djobs = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::string rep;
+    int best = 0, rc = 0;
+    auto cleanup = [&]() {
+        if (q) cudaFree(q);
+        if (fac) cudaFree(fac);
+        if (bond) cudaFree(bond);
+        if (spec) cudaFree(spec);
+        if (w) cudaFree(w);
+        if (djobs) cudaFree(djobs);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    };
+    CK(cudaSetDevice(c->device));
+    if (cudaMalloc(&q, (size_t)njobs * 2 * M * sb) != cudaSuccess || cudaMalloc(&fac, M * sb) != cudaSuccess ||
+        cudaMalloc(&bond, 2 * Mc * sb) != cudaSuccess || cudaMalloc(&spec, (size_t)njobs * 2 * Mc * 2 * sb) != cudaSuccess ||
+        cudaMalloc(&w, M * sizeof(double)) != cudaSuccess || cudaMalloc(&djobs, sizeof(lfts_step_job) * njobs) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cleanup();
+        return fail("autotune: allocation of the synthetic jobs failed");
+    }
+    {
+        // q = 1 everywhere (bit pattern of 1.0 in the ctx precision), fac = exp(0) = 1
+        std::vector<unsigned char> one(sb);
+        if (sb == 8) { const double v = 1.0; std::memcpy(one.data(), &v, 8); }
+        else { const float v = 1.0f; std::memcpy(one.data(), &v, 4); }
+        std::vector<unsigned char> row(M * sb);
+        for (size_t i = 0; i < M; i++) std::memcpy(row.data() + i * sb, one.data(), sb);
+        for (int jb = 0; jb < njobs; jb++)
+            CK(cudaMemcpy((char *)q + (size_t)jb * 2 * M * sb, row.data(), M * sb, cudaMemcpyHostToDevice));
+        CK(cudaMemset(w, 0, M * sizeof(double)));
+        if ((rc = lfts_field_factors(c, (const double *)w, 0.0, fac)) != 0) { cleanup(); return rc; }
+        const double lx[3] = {(double)c->nx[0], (double)c->nx[1], (double)c->nx[2]};
+        if ((rc = lfts_bond_tables(c, 1.0, 0.01, lx, bond, (char *)bond + Mc * sb)) != 0) { cleanup(); return rc; }
+        std::vector<lfts_step_job> hj(njobs);
+        for (int jb = 0; jb < njobs; jb++) {
+            lfts_step_job &j = hj[jb];
+            std::memset(&j, 0, sizeof j);
+            j.in = (char *)q + (size_t)jb * 2 * M * sb;
+            j.out = (char *)q + ((size_t)jb * 2 + 1) * M * sb;
+            j.fac = fac;
+            j.bond = bond;
+            j.bond_half = (char *)bond + Mc * sb;
+            j.spec = (char *)spec + (size_t)jb * 2 * Mc * 2 * sb;
+        }
+        CK(cudaMemcpy(djobs, hj.data(), sizeof(lfts_step_job) * njobs, cudaMemcpyHostToDevice));
+    }
+    std::vector<float> ms(cands.size(), 0.f);
+    for (size_t k = 0; k < cands.size() && rc == 0; k++) {
+        c->fastN = cands[k].fastN;
+        c->r8 = cands[k].r8;
+        c->r12 = cands[k].r12;
+        c->xcap = cands[k].xcap;
+        for (int i = 0; i < 2 && rc == 0; i++) rc = lfts_step_continuous(c, djobs, njobs, 0);
+        if (rc) break;
+        CK(cudaEventRecord(e0, c->stream));
+        for (int i = 0; i < reps && rc == 0; i++) rc = lfts_step_continuous(c, djobs, njobs, 0);
+        CK(cudaEventRecord(e1, c->stream));
+        CK(cudaEventSynchronize(e1));
+        CK(cudaEventElapsedTime(&ms[k], e0, e1));
+        ms[k] /= (float)reps;
+    }
+    if (rc == 0) rc = check_kernel_errors();
+    if (rc == 0) {
+        for (size_t k = 1; k < cands.size(); k++)
+            if (ms[k] < 0.95f * ms[best]) best = (int)k;
+        c->fastN = cands[best].fastN;
+        c->r8 = cands[best].r8;
+        c->r12 = cands[best].r12;
+        c->xcap = cands[best].xcap;
+        char buf[96];
+        for (size_t k = 0; k < cands.size(); k++) {
+            std::snprintf(buf, sizeof buf, "%s%s %.4f ms", k ? "; " : "", cands[k].name, (double)ms[k]);
+            rep += buf;
+        }
+        std::snprintf(buf, sizeof buf, " -> %s (%d jobs)", cands[best].name, njobs);
+        rep += buf;
+    } else {
+        c->fastN = fastN;
+        c->r8 = r8v;
+        c->r12 = r12v;
+        c->xcap = xcap0;
+    }
+    cleanup();
+    if (report && report_cap) {
+        std::strncpy(report, rep.c_str(), report_cap - 1);
+        report[report_cap - 1] = 0;
+    }
+    return rc;
 }

@@ -390,6 +390,10 @@ PYBIND11_MODULE(langevinfts, m) {
         }), py::keep_alive<1, 3>(), py::keep_alive<1, 4>(), py::keep_alive<1, 5>())
         .def("n_replicas", &BatchedLangevin::n_replicas)
         .def("set_host_control", &BatchedLangevin::set_host_control)
+        .def("autotune", [](BatchedLangevin &b, int reps) {
+            py::gil_scoped_release nogil;
+            return b.computation().autotune(reps);
+        }, py::arg("reps") = 5)
         .def("host_control", &BatchedLangevin::host_control)
         .def("stream_ptr", [](BatchedLangevin &b) { return (std::uintptr_t)b.stream(); })
         .def("kernel_launches", [](BatchedLangevin &b) { return b.computation().kernel_launches(); })

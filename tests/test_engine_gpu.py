@@ -47,10 +47,15 @@ def _jobs(ctx, jobs):
 
 @pytest.mark.parametrize("nx,lx", GRIDS, ids=GRID_IDS)
 @pytest.mark.parametrize("prec", [8, 4])
-def test_step_continuous(nx, lx, prec):
+def test_step_continuous(nx, lx, prec, autotune=False):
     from langevinfts_b200.capi import StepJob, check
     dt = np.dtype(np.float64 if prec == 8 else np.float32)
     ctx = _ctx(nx, prec)
+    if autotune:
+        report = C.create_string_buffer(512)
+        check(ctx.lib.lfts_autotune(ctx.h, 4, 3, report, 512))
+        text = report.value.decode()
+        assert "generic" in text and " -> " in text, text
     M = ctx.M
     rng = np.random.default_rng(7)
     ds, b2, nsteps, njobs = 0.01, 1.3, 4, 3
@@ -82,6 +87,14 @@ def test_step_continuous(nx, lx, prec):
             tol = 1e-12 if prec == 8 else 2e-5
             assert _rel(got[s + 1].astype(float), ref) < tol * (s + 1), (j, s, _rel(got[s + 1], ref))
     ctx.close()
+
+
+@pytest.mark.parametrize("nx,lx", [GRIDS[9], GRIDS[10], GRIDS[2], GRIDS[3]], ids=["64x64x64", "96x96x96", "32x32x32", "23x27x25"])
+@pytest.mark.parametrize("prec", [8, 4])
+def test_step_after_autotune(nx, lx, prec):
+    """lfts_autotune times every step implementation the grid has (register,
+    cubic, generic) and keeps one; the step still matches the oracle."""
+    test_step_continuous(nx, lx, prec, autotune=True)
 
 
 MASK_GRIDS = [((64, 64, 64), (7.3, 7.3, 7.3)), ((96, 96, 96), (8.0, 8.0, 8.0)), ((32, 32, 32), (4.0, 4.0, 4.0)),
