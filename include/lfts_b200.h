@@ -318,6 +318,23 @@ int lfts_saddle_control(lfts_ctx ctx, int R, int I, int it, const double *var, c
 int lfts_am_batch_solve(lfts_ctx ctx, int R, int L, const int *head, const int *ndots, const int *mode, const int *nh,
                         const double *dots, double *dot_ring, double *a);
 
+/* PCG64 streams on the device: the generator of numpy's PCG64 (128-bit LCG
+ * state = state * 0x2360ED051FC65DA44385DF649FCCF645 + inc, then the XSL-RR
+ * output of the new state), one per stream, states[4*s..4*s+3] = state hi,
+ * state lo, inc hi, inc lo (device uint64; take them from
+ * numpy's bit_generator.state).  Replaces the host draws of lfts.py:700
+ * (numpy Generator.normal) for the batched driver.
+ * raw:    out[s][i], i < n = the next n raw outputs of stream s (numpy's
+ *         PCG64.random_raw(n), bit for bit).
+ * normal: out[s][i] = sigma * N(0, 1) by Box-Muller on pairs of 53-bit
+ *         uniforms from consecutive raw outputs (2*ceil(n/2) raw outputs used).
+ *         The normal transform is this library's, not numpy's ziggurat: the
+ *         normals are N(0, 1) but not numpy's sequence.
+ * Both advance every state by the raw outputs used, so calls continue the
+ * streams. */
+int lfts_pcg64_raw(lfts_ctx ctx, unsigned long long *states, int nstreams, long long n, unsigned long long *out);
+int lfts_pcg64_normal(lfts_ctx ctx, unsigned long long *states, int nstreams, long long n, double sigma, double *out);
+
 /* Adam field update of the SCFT driver (examples/scft/scft.py:42-54), on n
  * doubles: m = b1 m + (1-b1) d; v = b2 v + (1-b2) d^2;
  * w_new = w + lr (m / (1 - b1^count)) / (sqrt(v / (1 - b2^count)) + eps).

@@ -96,6 +96,8 @@ _SIGS = {
     "lfts_status_post": [C.c_void_p, C.c_void_p, C.c_int],
     "lfts_status_wait": [C.c_void_p, C.c_int, C.c_void_p],
     "lfts_autotune": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_size_t],
+    "lfts_pcg64_raw": [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p],
+    "lfts_pcg64_normal": [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_double, C.c_void_p],
 }
 
 _lib = None

@@ -331,6 +331,85 @@ __global__ void k_am_solve(int R, int L, const int *__restrict__ head, const int
     }
 }
 
+// ---- PCG64 streams on the device (O'Neill's PCG, 128-bit LCG with the XSL-RR
+// 64-bit output; the generator numpy's PCG64 implements): per stream four
+// uint64 (state hi, lo, increment hi, lo).  Each thread jumps to its offset by
+// Brown's O(log k) LCG jump-ahead and draws RAW_PER_THREAD consecutive outputs.
+typedef unsigned __int128 u128;
+constexpr unsigned long long PCG_MULT_HI = 0x2360ED051FC65DA4ULL, PCG_MULT_LO = 0x4385DF649FCCF645ULL;
+constexpr int RAW_PER_THREAD = 16;
+
+__device__ __forceinline__ u128 u128_of(unsigned long long hi, unsigned long long lo) { return ((u128)hi << 64) | lo; }
+__device__ __forceinline__ unsigned long long pcg_output(u128 s) {
+    const unsigned long long hi = (unsigned long long)(s >> 64), lo = (unsigned long long)s;
+    const unsigned long long x = hi ^ lo;
+    const unsigned r = (unsigned)(hi >> 58);
+    return (x >> r) | (x << ((64 - r) & 63));
+}
+// state after k steps of s -> s * MULT + inc
+__device__ u128 pcg_jump(u128 s, u128 inc, unsigned long long k) {
+    u128 acc_mult = 1, acc_plus = 0, cur_mult = u128_of(PCG_MULT_HI, PCG_MULT_LO), cur_plus = inc;
+    while (k) {
+        if (k & 1) {
+            acc_mult *= cur_mult;
+            acc_plus = acc_plus * cur_mult + cur_plus;
+        }
+        cur_plus = (cur_mult + 1) * cur_plus;
+        cur_mult *= cur_mult;
+        k >>= 1;
+    }
+    return acc_mult * s + acc_plus;
+}
+
+// MODE 0: raw outputs to out_raw; MODE 1: sigma * N(0,1) by Box-Muller on
+// pairs (u1, u2) = 53-bit uniforms of raw outputs 2p, 2p + 1:
+// z = sqrt(-2 ln(1 - u1)) (cos, sin)(2 pi u2)
+template <int MODE>
+__global__ void k_pcg64(const unsigned long long *__restrict__ states, long long n, double sigma,
+                        unsigned long long *__restrict__ out_raw, double *__restrict__ out) {
+    const int st = blockIdx.y;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long first = t * RAW_PER_THREAD;
+    const long long nraw = MODE == 0 ? n : 2 * ((n + 1) / 2);
+    if (first >= nraw) return;
+    const unsigned long long *sp = states + 4 * (long long)st;
+    const u128 inc = u128_of(sp[2], sp[3]);
+    u128 s = pcg_jump(u128_of(sp[0], sp[1]), inc, (unsigned long long)first);
+    const u128 mult = u128_of(PCG_MULT_HI, PCG_MULT_LO);
+    unsigned long long raw[RAW_PER_THREAD];
+#pragma unroll
+    for (int i = 0; i < RAW_PER_THREAD; i++) {
+        s = s * mult + inc;
+        raw[i] = pcg_output(s);
+    }
+    if (MODE == 0) {
+        unsigned long long *o = out_raw + (long long)st * n + first;
+#pragma unroll
+        for (int i = 0; i < RAW_PER_THREAD; i++)
+            if (first + i < n) o[i] = raw[i];
+    } else {
+        double *o = out + (long long)st * n + first;
+#pragma unroll
+        for (int i = 0; i < RAW_PER_THREAD; i += 2) {
+            const double u1 = (double)(raw[i] >> 11) * 0x1.0p-53, u2 = (double)(raw[i + 1] >> 11) * 0x1.0p-53;
+            const double r = sqrt(-2.0 * log1p(-u1));
+            double sn, cs;
+            sincospi(2.0 * u2, &sn, &cs);
+            if (first + i < n) o[i] = sigma * r * cs;
+            if (first + i + 1 < n) o[i + 1] = sigma * r * sn;
+        }
+    }
+}
+
+__global__ void k_pcg64_advance(unsigned long long *__restrict__ states, int nstreams, unsigned long long k) {
+    const int st = blockIdx.x * blockDim.x + threadIdx.x;
+    if (st >= nstreams) return;
+    unsigned long long *sp = states + 4 * (long long)st;
+    const u128 s = pcg_jump(u128_of(sp[0], sp[1]), u128_of(sp[2], sp[3]), k);
+    sp[0] = (unsigned long long)(s >> 64);
+    sp[1] = (unsigned long long)s;
+}
+
 int grid1(long long n, int cap) {
     long long b = (n + NT - 1) / NT;
     if (b > cap) b = cap;
@@ -483,4 +562,31 @@ extern "C" int lfts_am_batch_solve(lfts_ctx ctx, int R, int L, const int *head, 
     lfts_internal_count(ctx, 1);
     LCK(cudaPeekAtLastError());
     return 0;
+}
+
+static int pcg64_launch(lfts_ctx ctx, unsigned long long *states, int nstreams, long long n, double sigma,
+                        unsigned long long *out_raw, double *out) {
+    if (!ctx || !states || (!out_raw && !out)) return lfts_internal_fail("null argument");
+    if (nstreams < 1 || nstreams > 65535 || n < 0) return lfts_internal_fail("pcg64: nstreams must be 1..65535 and n >= 0");
+    if (n == 0) return 0;
+    const long long nraw = out_raw ? n : 2 * ((n + 1) / 2);
+    const long long threads = (nraw + RAW_PER_THREAD - 1) / RAW_PER_THREAD;
+    const long long blocks = (threads + NT - 1) / NT;
+    if (blocks > 0x7fffffffLL) return lfts_internal_fail("pcg64: too many draws in one call");
+    cudaStream_t s = (cudaStream_t)lfts_ctx_stream(ctx);
+    if (out_raw) k_pcg64<0><<<dim3((unsigned)blocks, nstreams), NT, 0, s>>>(states, n, sigma, out_raw, nullptr);
+    else k_pcg64<1><<<dim3((unsigned)blocks, nstreams), NT, 0, s>>>(states, n, sigma, nullptr, out);
+    k_pcg64_advance<<<(nstreams + 63) / 64, 64, 0, s>>>(states, nstreams, (unsigned long long)nraw);
+    lfts_internal_count(ctx, 2);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_pcg64_normal(lfts_ctx ctx, unsigned long long *states, int nstreams, long long n, double sigma,
+                                 double *out) {
+    return pcg64_launch(ctx, states, nstreams, n, sigma, nullptr, out);
+}
+
+extern "C" int lfts_pcg64_raw(lfts_ctx ctx, unsigned long long *states, int nstreams, long long n, unsigned long long *out) {
+    return pcg64_launch(ctx, states, nstreams, n, 0.0, out, nullptr);
 }

@@ -64,6 +64,14 @@ class BatchedLangevin {
     // resume.
     void get_noise_prev(double *out) const;
     void set_noise_prev(const double *in);
+    // Noise drawn on the device from one PCG64 stream per replica
+    // (lfts_pcg64_normal): states host [R][4] uint64 (state hi, lo, inc hi,
+    // lo), the state of numpy's PCG64 of the replica.  step_device_rng draws
+    // this step's noise (sigma * N(0, 1), [R][n_real][M]) and steps.
+    void set_noise_streams(const unsigned long long *states);
+    void get_noise_streams(unsigned long long *states) const;
+    bool has_noise_streams() const { return pcg_.get() != nullptr; }
+    SaddleStats step_device_rng(double sigma);
     // Structure function of every replica (examples/fts/lfts.py:753-767):
     //   sf[r][p] += mu_a conj(phi_b / M),  mu_a = sum_{q < S-1} F[w_aux_q] coef[q][a],
     // for the type pairs p = (pairs[2p], pairs[2p+1]); coef (host, (S-1) x S) =
@@ -92,6 +100,7 @@ class BatchedLangevin {
     // device saddle control: n_anderson, head_raw, iter (R ints each) + the
     // any-active word; err, err_old (R doubles each); dot ring R*L*L
     DevBuf sint_, sdbl_, dot_ring_;
+    DevBuf pcg_, noise_buf_;  // device noise: PCG64 states [R][4], this step's draw [R][n_real][M]
     bool host_control_ = false;
     int xi_cur_ = 0;
     std::vector<double *> phi_ptrs_, w_mono_ptrs_;

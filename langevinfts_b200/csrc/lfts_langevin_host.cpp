@@ -82,7 +82,7 @@ BatchedLangevin::BatchedLangevin(ComputationBox *cb, Molecules *mol, PropagatorA
 BatchedLangevin::~BatchedLangevin() {
     w_aux_.release(); w_save_.release(); phi_save_.release(); d_cur_.release(); xi_[0].release(); xi_[1].release();
     partials_.release(); stats_.release(); ctl_.release(); am_w_.release(); am_d_.release(); am_dots_.release(); am_a_.release();
-    sint_.release(); sdbl_.release(); dot_ring_.release();
+    sint_.release(); sdbl_.release(); dot_ring_.release(); pcg_.release(); noise_buf_.release();
     comp_.reset();
 }
 
@@ -373,6 +373,24 @@ SaddleStats BatchedLangevin::step_device(const double *noise_dev) {
         xi_cur_ = 1 - xi_cur_;  // this step's draw is the next step's "previous" noise (lfts.py:708-709)
     }
     return find_saddle_point(true);
+}
+
+void BatchedLangevin::set_noise_streams(const unsigned long long *states) {
+    if (Rr_ < 1) LFTS_THROW("no real auxiliary field draws noise");
+    if (!pcg_.get()) {
+        pcg_.alloc(ctx_, sizeof(unsigned long long) * 4 * (size_t)R_);
+        noise_buf_.alloc(ctx_, sizeof(double) * (size_t)R_ * Rr_ * M_);
+    }
+    check_rc(lfts_memcpy_h2d(ctx_, pcg_.get(), states, pcg_.size()));
+}
+void BatchedLangevin::get_noise_streams(unsigned long long *states) const {
+    if (!pcg_.get()) LFTS_THROW("no device noise streams (set_noise_streams first)");
+    check_rc(lfts_memcpy_d2h(ctx_, states, pcg_.get(), pcg_.size()));
+}
+SaddleStats BatchedLangevin::step_device_rng(double sigma) {
+    if (!pcg_.get()) LFTS_THROW("no device noise streams (set_noise_streams first)");
+    check_rc(lfts_pcg64_normal(ctx_, pcg_.as<unsigned long long>(), R_, (long long)Rr_ * M_, sigma, noise_buf_.as<double>()));
+    return step_device(noise_buf_.as<double>());
 }
 
 void BatchedLangevin::get_noise_prev(double *out) const {

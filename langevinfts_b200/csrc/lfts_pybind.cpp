@@ -390,6 +390,25 @@ PYBIND11_MODULE(langevinfts, m) {
         }), py::keep_alive<1, 3>(), py::keep_alive<1, 4>(), py::keep_alive<1, 5>())
         .def("n_replicas", &BatchedLangevin::n_replicas)
         .def("set_host_control", &BatchedLangevin::set_host_control)
+        .def("set_noise_streams", [](BatchedLangevin &b, py::array_t<unsigned long long, py::array::c_style | py::array::forcecast> st) {
+            py::buffer_info bi = st.request();
+            if (bi.size != 4LL * b.n_replicas()) throw std::runtime_error("noise streams must be an n_replicas x 4 uint64 array");
+            b.set_noise_streams((const unsigned long long *)bi.ptr);
+        })
+        .def("get_noise_streams", [](BatchedLangevin &b) {
+            py::array_t<unsigned long long> st({(py::ssize_t)b.n_replicas(), (py::ssize_t)4});
+            b.get_noise_streams((unsigned long long *)st.request().ptr);
+            return st;
+        })
+        .def("has_noise_streams", &BatchedLangevin::has_noise_streams)
+        .def("step_rng", [](BatchedLangevin &b, double sigma) {
+            SaddleStats s;
+            {
+                py::gil_scoped_release nogil;
+                s = b.step_device_rng(sigma);
+            }
+            return stats_dict(s);
+        }, py::arg("sigma"))
         .def("autotune", [](BatchedLangevin &b, int reps) {
             py::gil_scoped_release nogil;
             return b.computation().autotune(reps);

@@ -259,9 +259,17 @@ class LFTS:
 
 
 class BatchedLFTS:
-    """Many L-FTS replicas on the device-resident batched engine."""
+    """Many L-FTS replicas on the device-resident batched engine.
 
-    def __init__(self, params, random_seeds, module=None, platform="cuda"):
+    noise="host" (default) draws each step's noise with numpy's
+    Generator(PCG64(seed)).normal on the host, exactly as lfts.py:700 does, so
+    replica r follows the reference trajectory of its seed.  noise="device"
+    draws it on the GPU (lfts_pcg64_normal) from the same PCG64 streams: the
+    same raw 64-bit stream, a different normal transform (Box-Muller, not
+    numpy's ziggurat), so the noise is N(0, sigma^2) but not the reference's
+    sequence.  Checkpoints keep the PCG64 state either way."""
+
+    def __init__(self, params, random_seeds, module=None, platform="cuda", noise="host"):
         if module is None:
             from langevinfts_b200 import langevinfts as module
         (self.monomer_types, self.chi_n, self.mpt, factory, self.cb, self.molecules, self.analyzer, self.dt_scaling,
@@ -284,6 +292,29 @@ class BatchedLFTS:
         self._pool = None
         self.params = params
         self.langevin_step = 0
+        if noise not in ("host", "device"):
+            raise ValueError('noise must be "host" or "device"')
+        self.noise = noise
+        if noise == "device":
+            self._upload_streams()
+
+    def _upload_streams(self):
+        """PCG64 states of the replicas' generators -> the device streams."""
+        st = np.zeros([self.R, 4], dtype=np.uint64)
+        m64 = (1 << 64) - 1
+        for r, g in enumerate(self.rngs):
+            s = g.bit_generator.state["state"]
+            st[r] = [s["state"] >> 64, s["state"] & m64, s["inc"] >> 64, s["inc"] & m64]
+        self.engine.set_noise_streams(st)
+
+    def _download_streams(self):
+        """Device stream states -> the replicas' numpy generators (for checkpoints)."""
+        st = self.engine.get_noise_streams()
+        for r, g in enumerate(self.rngs):
+            g.bit_generator.state = {
+                "bit_generator": "PCG64",
+                "state": {"state": (int(st[r, 0]) << 64) | int(st[r, 1]), "inc": (int(st[r, 2]) << 64) | int(st[r, 3])},
+                "has_uint32": 0, "uinteger": 0}
 
     def start(self, initial_fields):
         """initial_fields: list (per replica) of {monomer type: field}."""
@@ -309,6 +340,10 @@ class BatchedLFTS:
         return out
 
     def step(self, noise=None):
+        if noise is None and self.noise == "device":
+            stats = self.engine.step_rng(self.sigma)
+            self.langevin_step += 1
+            return stats
         if noise is None:
             noise = self.draw_noise()
         stats = self.engine.step(noise)
@@ -326,6 +361,8 @@ class BatchedLFTS:
         from scipy.io import savemat
         if len(paths) != self.R:
             raise ValueError("one path per replica")
+        if self.noise == "device":
+            self._download_streams()
         w_aux = self.fields()
         phi = self.engine.get_concentrations(self.S)
         noise_prev = self.engine.get_noise_prev()
@@ -373,6 +410,8 @@ class BatchedLFTS:
             raise ValueError("the checkpoints are at different Langevin steps")
         stats = self.start(fields)
         self.engine.set_noise_prev(noise_prev)
+        if self.noise == "device":
+            self._upload_streams()
         self.langevin_step = steps.pop()
         return stats
 
