@@ -379,6 +379,63 @@ def _reference_scft_child(n_iter, threads):
     return 0
 
 
+def run_learned(args):
+    """Ablation of the learned saddle-point start on the workload's system:
+    equilibrate, collect (w_-, w_+prev) -> w_+ pairs from the plain solver,
+    train the U-Net, then run the same Langevin steps (same state, same host
+    noise) with and without the learned start and compare saddle iterations."""
+    import torch
+    from langevinfts_b200 import langevinfts as L
+    from langevinfts_b200.lfts import BatchedLFTS
+    from langevinfts_b200.learned import generate_pairs, train
+    from langevinfts_b200.ensemble import replica_seeds
+    torch.cuda.init()
+    R = args.replicas
+    p = workload_params(args.workload, args.nx)
+    seeds = replica_seeds(0, R, base=WORKLOADS[args.workload]["seed"])
+    sim = BatchedLFTS(p, seeds, module=L)
+    sim.engine.autotune()
+    sim.start([initial_fields(s, sim.M) for s in seeds])
+    for _ in range(args.warmup):
+        sim.step()
+    t0 = time.time()
+    X, Y, it_gen = generate_pairs(sim, args.learned_steps)
+    t_gen = time.time() - t0
+    t0 = time.time()
+    start, hist = train(X, Y, seconds=args.learned_train)
+    t_train = time.time() - t0
+    w0, xi0 = sim.fields(), sim.engine.get_noise_prev()
+    rng0 = [g.bit_generator.state for g in sim.rngs]
+
+    def run(st):
+        sim.engine.set_fields(w0)
+        sim.engine.find_saddle_point()  # concentrations at w0 (a saddle point already)
+        sim.engine.set_noise_prev(xi0)
+        for g, s0 in zip(sim.rngs, rng0):
+            g.bit_generator.state = s0
+        iters, fails = [], 0
+        torch.cuda.synchronize()
+        t = time.time()
+        for _ in range(args.steps):
+            out = sim.step(start=st) if st is not None else sim.step()
+            iters += list(out["iterations"])
+            fails += int(sum(out["failed"]))
+        torch.cuda.synchronize()
+        return float(np.mean(iters)), R * args.steps / (time.time() - t), fails
+
+    plain, learned = run(None), run(start)
+    print(json.dumps({"metric": "mean saddle-point iterations per Langevin step (learned start ablation)",
+                      "workload": args.workload, "grid": [args.nx] * 3, "replicas": R,
+                      "plain": {"mean_iterations": plain[0], "replica_steps_per_s": plain[1], "failed": plain[2]},
+                      "learned": {"mean_iterations": learned[0], "replica_steps_per_s": learned[1], "failed": learned[2]},
+                      "steps": args.steps, "training_pairs": int(len(X)), "data_steps": args.learned_steps,
+                      "data_seconds": t_gen, "train_seconds": t_train, "epochs": len(hist),
+                      "loss_first_last": [hist[0][1], hist[-1][1]],
+                      "model": "3-level periodic 3D U-Net, 24 base channels, 3^3 kernels, BF16 autocast (torch conv3d)",
+                      "timing": "wall clock around the steps, host noise"}))
+    return 0
+
+
 def run_scft(args):
     """SCFT of config 2 with the device loop in FP64 and FP32, and the time per
     iteration of the host-driven loop; one JSON line."""
@@ -599,6 +656,10 @@ def main():
     ap.add_argument("--ref-statistics", default="", help=argparse.SUPPRESS)
     ap.add_argument("--ref-scft", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--scft", action="store_true", help="SCFT of the 64^3 asymmetric diblock (device loop, FP64 and FP32)")
+    ap.add_argument("--learned", action="store_true",
+                    help="ablation of the learned saddle-point start (U-Net) on the workload's system")
+    ap.add_argument("--learned-steps", type=int, default=20, help="plain Langevin steps that make the training pairs")
+    ap.add_argument("--learned-train", type=float, default=60.0, help="training time budget (s)")
     ap.add_argument("--statistics", action="store_true",
                     help="time compute_statistics of single systems (configs 1 and 3) on the GPU and the reference CPU")
     ap.add_argument("--threads", type=int, default=1, help=argparse.SUPPRESS)
@@ -619,6 +680,8 @@ def main():
         return run_statistics(args)
     if args.scft:
         return run_scft(args)
+    if args.learned:
+        return run_learned(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.kernel_only:

@@ -72,6 +72,14 @@ class BatchedLangevin {
     void get_noise_streams(unsigned long long *states) const;
     bool has_noise_streams() const { return pcg_.get() != nullptr; }
     SaddleStats step_device_rng(double sigma);
+    // The two halves of a step, for a caller that changes the imaginary fields
+    // in between (a learned saddle-point start): the Langevin update of the
+    // real fields (saving fields and concentrations for a restore), then
+    // find_saddle_point(true).  w_aux_device: the [R][S][M] fields, written on
+    // stream() only.
+    void langevin_update_device(const double *noise_dev);
+    void langevin_update_rng(double sigma);
+    double *w_aux_device() { return w_aux_.as<double>(); }
     // Structure function of every replica (examples/fts/lfts.py:753-767):
     //   sf[r][p] += mu_a conj(phi_b / M),  mu_a = sum_{q < S-1} F[w_aux_q] coef[q][a],
     // for the type pairs p = (pairs[2p], pairs[2p+1]); coef (host, (S-1) x S) =

@@ -354,6 +354,11 @@ SaddleStats BatchedLangevin::step(const double *noise) {
 }
 
 SaddleStats BatchedLangevin::step_device(const double *noise_dev) {
+    langevin_update_device(noise_dev);
+    return find_saddle_point(true);
+}
+
+void BatchedLangevin::langevin_update_device(const double *noise_dev) {
     const size_t SM = (size_t)S_ * M_;
     // keep the fields and concentrations to restore replicas whose saddle point fails
     check_rc(lfts_memcpy_d2d_async(ctx_, w_save_.get(), w_aux_.get(), w_aux_.size()));
@@ -372,7 +377,12 @@ SaddleStats BatchedLangevin::step_device(const double *noise_dev) {
                                     w_aux_.as<double>(), xi_[xi_cur_].as<double>(), cur.as<double>(), nullptr));
         xi_cur_ = 1 - xi_cur_;  // this step's draw is the next step's "previous" noise (lfts.py:708-709)
     }
-    return find_saddle_point(true);
+}
+
+void BatchedLangevin::langevin_update_rng(double sigma) {
+    if (!pcg_.get()) LFTS_THROW("no device noise streams (set_noise_streams first)");
+    check_rc(lfts_pcg64_normal(ctx_, pcg_.as<unsigned long long>(), R_, (long long)Rr_ * M_, sigma, noise_buf_.as<double>()));
+    langevin_update_device(noise_buf_.as<double>());
 }
 
 void BatchedLangevin::set_noise_streams(const unsigned long long *states) {

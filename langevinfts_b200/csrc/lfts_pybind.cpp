@@ -401,6 +401,23 @@ PYBIND11_MODULE(langevinfts, m) {
             return st;
         })
         .def("has_noise_streams", &BatchedLangevin::has_noise_streams)
+        .def("w_aux_ptr", [](BatchedLangevin &b) { return (std::uintptr_t)b.w_aux_device(); })
+        .def("langevin_update_device", [](BatchedLangevin &b, std::uintptr_t noise_dev) {
+            py::gil_scoped_release nogil;
+            b.langevin_update_device((const double *)noise_dev);
+        })
+        .def("langevin_update_rng", [](BatchedLangevin &b, double sigma) {
+            py::gil_scoped_release nogil;
+            b.langevin_update_rng(sigma);
+        }, py::arg("sigma"))
+        .def("finish_step", [](BatchedLangevin &b) {
+            SaddleStats s;
+            {
+                py::gil_scoped_release nogil;
+                s = b.find_saddle_point(true);
+            }
+            return stats_dict(s);
+        })
         .def("step_rng", [](BatchedLangevin &b, double sigma) {
             SaddleStats s;
             {

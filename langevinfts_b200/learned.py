@@ -1,0 +1,154 @@
+"""Learned saddle-point start for batched L-FTS.
+
+After the Langevin update of the real (exchange) fields w_-, the saddle-point
+search over the imaginary (pressure) fields w_+ normally starts from the
+previous step's saddle point.  Here a 3-level periodic 3D U-Net predicts the
+new saddle point from (new w_-, previous w_+) and the search starts there:
+
+    w_+start = w_+prev + s_out * UNet([w_- / s_in, w_+prev / s_out])
+
+The network adds a residual to the warm start; its last layer starts at zero,
+so an untrained model reproduces the plain warm start exactly.  The search
+itself (Anderson mixing to the same tolerance) is unchanged, so the learned
+start can only change how many iterations a step needs, not where it ends.
+
+Pieces:
+  UNet3D            3 levels (N, N/2, N/4), 24 base channels, 3^3 kernels with
+                    circular padding (the box is periodic), ReLU, average
+                    pooling down, nearest upsampling, skip concatenation; runs
+                    in BF16 with FP32 accumulation (torch autocast over cuDNN).
+  generate_pairs    training pairs from the plain solver: inputs (w_-, w_+prev)
+                    and target w_+ of every replica and step.
+  train             AdamW on the mean-squared error of the residual.
+  LearnedStart      the callable BatchedLFTS.step(start=...) uses: reads w_aux
+                    on the device (zero copy), writes the predicted w_+ in place
+                    on the engine's stream.
+
+The convolutions are torch's (cuDNN); the step kernels of the solver are this
+library's.  Grids must have extents divisible by 4.
+"""
+import time
+
+import numpy as np
+import torch
+import torch.nn as nn
+import torch.nn.functional as F
+
+
+class _DeviceArray:
+    """Zero-copy view of device memory for torch.as_tensor (__cuda_array_interface__)."""
+
+    def __init__(self, ptr, shape, typestr="<f8"):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+def _conv(cin, cout, k=3):
+    return nn.Conv3d(cin, cout, k, padding=k // 2, padding_mode="circular")
+
+
+def _block(cin, cout):
+    return nn.Sequential(_conv(cin, cout), nn.ReLU(inplace=True), _conv(cout, cout), nn.ReLU(inplace=True))
+
+
+class UNet3D(nn.Module):
+    """3-level periodic 3D U-Net (base channels b: b, 2b, 4b by level)."""
+
+    def __init__(self, cin=2, cout=1, base=24):
+        super().__init__()
+        b = base
+        self.e1, self.e2, self.e3 = _block(cin, b), _block(b, 2 * b), _block(2 * b, 4 * b)
+        self.d2, self.d1 = _block(6 * b, 2 * b), _block(3 * b, b)
+        self.out = nn.Conv3d(b, cout, 1)
+        nn.init.zeros_(self.out.weight)
+        nn.init.zeros_(self.out.bias)
+
+    def forward(self, x):
+        x1 = self.e1(x)
+        x2 = self.e2(F.avg_pool3d(x1, 2))
+        x3 = self.e3(F.avg_pool3d(x2, 2))
+        y2 = self.d2(torch.cat([F.interpolate(x3, scale_factor=2, mode="nearest"), x2], 1))
+        y1 = self.d1(torch.cat([F.interpolate(y2, scale_factor=2, mode="nearest"), x1], 1))
+        return self.out(y1)
+
+
+def generate_pairs(sim, nsteps):
+    """Run nsteps plain Langevin steps of a started BatchedLFTS and collect, per
+    replica and step that met the tolerance, the network inputs (w_- after the
+    update, w_+ before the search) and the target (w_+ at the saddle point).
+    Returns float32 arrays X [n, 2, nx, ny, nz], Y [n, 1, nx, ny, nz] and the
+    saddle iterations of the steps."""
+    shape = list(sim.cb.get_nx())
+    ri, ii = sim.mpt.aux_fields_real_idx, sim.mpt.aux_fields_imag_idx
+    if len(ri) != 1 or len(ii) != 1:
+        raise ValueError("the learned start handles one real and one imaginary auxiliary field")
+    X, Y, iters = [], [], []
+    w_prev = sim.fields()
+    for _ in range(nsteps):
+        st = sim.step()
+        w = sim.fields()
+        for r in range(sim.R):
+            if st["failed"][r]:
+                continue
+            X.append(np.stack([w[r, ri[0]], w_prev[r, ii[0]]]).reshape([2] + shape).astype(np.float32))
+            Y.append(w[r, ii[0]].reshape([1] + shape).astype(np.float32))
+        iters += list(st["iterations"])
+        w_prev = w
+    return np.array(X), np.array(Y), iters
+
+
+class LearnedStart:
+    """Callable for BatchedLFTS.step(start=...): predicts the imaginary field
+    of every replica from the fields on the device and writes it in place."""
+
+    def __init__(self, model, s_in, s_out, batch=8):
+        self.model, self.s_in, self.s_out, self.batch = model.eval(), float(s_in), float(s_out), batch
+
+    @torch.no_grad()
+    def __call__(self, sim):
+        shape = list(sim.cb.get_nx())
+        R, S, M = sim.R, sim.S, sim.M
+        ri, ii = sim.mpt.aux_fields_real_idx[0], sim.mpt.aux_fields_imag_idx[0]
+        stream = torch.cuda.ExternalStream(sim.engine.stream_ptr())
+        with torch.cuda.stream(stream):
+            w = torch.as_tensor(_DeviceArray(sim.engine.w_aux_ptr(), (R, S, M)), device="cuda")
+            for r0 in range(0, R, self.batch):
+                wr = w[r0:r0 + self.batch]
+                x = torch.stack([wr[:, ri] / self.s_in, wr[:, ii] / self.s_out], 1).float().reshape([-1, 2] + shape)
+                with torch.autocast("cuda", dtype=torch.bfloat16):
+                    d = self.model(x).float()
+                d = d.reshape(-1, M).double() * self.s_out
+                d -= d.mean(1, keepdim=True)  # the pressure field keeps zero mean
+                wr[:, ii] += d
+
+
+def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_decay=1e-4, seed=0, log=None):
+    """AdamW on MSE of the scaled residual target (Y - w_+prev) / s_out, BF16
+    autocast, until `seconds` or `epochs` run out.  Returns (LearnedStart,
+    history of (epoch, mean loss))."""
+    torch.manual_seed(seed)
+    s_in = float(np.std(X[:, 0])) or 1.0
+    s_out = float(np.std(X[:, 1])) or 1.0
+    xin = torch.from_numpy(np.concatenate([X[:, :1] / s_in, X[:, 1:] / s_out], 1)).cuda()
+    tgt = torch.from_numpy((Y - X[:, 1:]) / s_out).cuda()
+    model = UNet3D(cin=2, cout=1, base=base).cuda()
+    opt = torch.optim.AdamW(model.parameters(), lr=lr, weight_decay=weight_decay)
+    n = xin.shape[0]
+    hist, t0 = [], time.time()
+    for ep in range(epochs):
+        perm = torch.randperm(n, device="cuda")
+        tot = 0.0
+        for k in range(0, n, batch):
+            idx = perm[k:k + batch]
+            with torch.autocast("cuda", dtype=torch.bfloat16):
+                loss = F.mse_loss(model(xin[idx]).float(), tgt[idx])
+            opt.zero_grad(set_to_none=True)
+            loss.backward()
+            opt.step()
+            tot += float(loss.detach()) * len(idx)
+        hist.append((ep, tot / n))
+        if log:
+            log(f"epoch {ep} loss {tot / n:.4e}")
+        if time.time() - t0 > seconds:
+            break
+    return LearnedStart(model, s_in, s_out), hist

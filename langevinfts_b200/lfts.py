@@ -339,7 +339,27 @@ class BatchedLFTS:
         list(self._pool.map(one, range(self.R)))
         return out
 
-    def step(self, noise=None):
+    def step(self, noise=None, start=None):
+        """One Langevin step of every replica.  start (optional): a callable
+        (e.g. learned.LearnedStart) run after the Langevin update and before the
+        saddle-point search; it may change the imaginary fields on the device,
+        which the search then starts from."""
+        if start is not None:
+            import torch
+            keep = None
+            if self.noise == "device" and noise is None:
+                self.engine.langevin_update_rng(self.sigma)
+            else:
+                if noise is None:
+                    noise = self.draw_noise()
+                with torch.cuda.stream(torch.cuda.ExternalStream(self.engine.stream_ptr())):
+                    keep = torch.from_numpy(np.ascontiguousarray(noise)).cuda()
+                self.engine.langevin_update_device(keep.data_ptr())
+            start(self)
+            stats = self.engine.finish_step()
+            del keep
+            self.langevin_step += 1
+            return stats
         if noise is None and self.noise == "device":
             stats = self.engine.step_rng(self.sigma)
             self.langevin_step += 1

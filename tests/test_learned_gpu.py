@@ -1,0 +1,63 @@
+"""Learned saddle-point start (langevinfts_b200.learned): the U-Net respects
+the periodic box, an untrained network (zero last layer) leaves the batched
+L-FTS trajectory exactly as the plain warm start gives it, training pairs
+are the solver's own fields, and training lowers the loss."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_unet_is_shift_equivariant_on_the_periodic_grid():
+    import torch
+    from langevinfts_b200.learned import UNet3D
+    torch.manual_seed(0)
+    net = UNet3D(cin=2, cout=1, base=8).cuda().double()
+    for p in net.parameters():  # a non-trivial last layer
+        torch.nn.init.normal_(p, 0, 0.1)
+    x = torch.randn(1, 2, 16, 16, 16, device="cuda", dtype=torch.float64)
+    shift = (4, 8, 12)  # multiples of 4: both pooling levels commute with the shift
+    with torch.no_grad():
+        a = torch.roll(net(x), shift, dims=(2, 3, 4))
+        b = net(torch.roll(x, shift, dims=(2, 3, 4)))
+    assert float((a - b).abs().max()) < 1e-12 * float(a.abs().max())
+
+
+def test_untrained_start_reproduces_the_plain_step():
+    from langevinfts_b200.learned import LearnedStart, UNet3D
+    from langevinfts_b200.lfts import BatchedLFTS
+    from tests.test_checkpoint_gpu import params
+    sims = [BatchedLFTS(params(), random_seeds=[41, 42]) for _ in range(2)]
+    rng = np.random.Generator(np.random.PCG64(5))
+    init = [{"A": rng.normal(0, 1, sims[0].M), "B": rng.normal(0, 1, sims[0].M)} for _ in range(2)]
+    for s in sims:
+        s.start(init)
+    start = LearnedStart(UNet3D(base=8).cuda(), 1.0, 1.0)
+    for _ in range(2):
+        a = sims[0].step()
+        b = sims[1].step(start=start)
+        assert list(a["iterations"]) == list(b["iterations"])
+    assert np.array_equal(sims[0].fields(), sims[1].fields())
+
+
+def test_generate_pairs_and_training_lowers_the_loss():
+    from langevinfts_b200.learned import generate_pairs, train
+    from langevinfts_b200.lfts import BatchedLFTS
+    from tests.test_checkpoint_gpu import params
+    sim = BatchedLFTS(params(), random_seeds=[51, 52, 53, 54])
+    rng = np.random.Generator(np.random.PCG64(6))
+    sim.start([{"A": rng.normal(0, 1, sim.M), "B": rng.normal(0, 1, sim.M)} for _ in range(sim.R)])
+    w_before = sim.fields()
+    X, Y, iters = generate_pairs(sim, 3)
+    assert X.shape == (12, 2, 16, 16, 16) and Y.shape == (12, 1, 16, 16, 16) and len(iters) == 12
+    w_after = sim.fields()
+    ri, ii = sim.mpt.aux_fields_real_idx[0], sim.mpt.aux_fields_imag_idx[0]
+    # the last step's pairs: inputs (w_- now, w_+ of the step before), target w_+ now
+    last = X[-sim.R:], Y[-sim.R:]
+    np.testing.assert_allclose(last[0][:, 0].reshape(sim.R, -1), w_after[:, ri].astype(np.float32), rtol=0, atol=0)
+    np.testing.assert_allclose(last[1][:, 0].reshape(sim.R, -1), w_after[:, ii].astype(np.float32), rtol=0, atol=0)
+    first = X[:sim.R]
+    np.testing.assert_allclose(first[:, 1].reshape(sim.R, -1), w_before[:, ii].astype(np.float32), rtol=0, atol=0)
+    # the network can fit a handful of pairs: 150 AdamW steps on 4 of them
+    start, hist = train(X[:4], Y[:4], base=8, seconds=120, epochs=150, batch=4, lr=3e-3)
+    assert hist[-1][1] < 0.6 * hist[0][1], hist[:: max(1, len(hist) // 6)]
