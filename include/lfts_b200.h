@@ -335,6 +335,22 @@ int lfts_am_batch_solve(lfts_ctx ctx, int R, int L, const int *head, const int *
 int lfts_pcg64_raw(lfts_ctx ctx, unsigned long long *states, int nstreams, long long n, unsigned long long *out);
 int lfts_pcg64_normal(lfts_ctx ctx, unsigned long long *states, int nstreams, long long n, double sigma, double *out);
 
+/* ---- learned saddle-point start: U-Net convolution ---------------------- */
+
+/* Periodic 3D convolution of channels-last BF16 activations on the tensor
+ * cores (tcgen05 implicit GEMM, FP32 accumulation in tensor memory):
+ *   out[p][co] = act(bias[co] + sum_{tap, ci} w[tap][co][ci] in[(p + tap) mod box][ci])
+ * in: [B][D][H][W][cin], out: [B][D][H][W][cout] (BF16, 16-byte aligned),
+ * wpk: packed weights [taps][cin/8][cout][8] BF16 (tap = 9 kz + 3 ky + kx,
+ * offset (kz-1, ky-1, kx-1); taps = 27 for 3x3x3, 1 for 1x1x1), bias: cout
+ * FP32 (device).  cin, cout: multiples of 16, cin <= LFTS_CONV_MAX_CIN,
+ * cout <= LFTS_CONV_MAX_COUT; act = ReLU when relu != 0.  stream: cudaStream_t.
+ * No counterpart in the reference (it has no learned component). */
+#define LFTS_CONV_MAX_CIN 160
+#define LFTS_CONV_MAX_COUT 128
+int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, const float *bias, void *out, int B, int D, int H, int W,
+                     int cin, int cout, int taps, int relu);
+
 /* Adam field update of the SCFT driver (examples/scft/scft.py:42-54), on n
  * doubles: m = b1 m + (1-b1) d; v = b2 v + (1-b2) d^2;
  * w_new = w + lr (m / (1 - b1^count)) / (sqrt(v / (1 - b2^count)) + eps).

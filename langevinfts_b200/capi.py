@@ -98,6 +98,8 @@ _SIGS = {
     "lfts_autotune": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_size_t],
     "lfts_pcg64_raw": [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p],
     "lfts_pcg64_normal": [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_double, C.c_void_p],
+    "lfts_conv3d_bf16": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                         C.c_int, C.c_int, C.c_int, C.c_int],
 }
 
 _lib = None

@@ -1319,3 +1319,6 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
     }
     return rc;
 }
+
+// ---------------------------------------------------------------- U-Net convolution (tcgen05)
+#include "lfts_unet.cuh"

@@ -1,0 +1,216 @@
+// Periodic 3D convolution for the learned saddle-point start (U-Net), as an
+// implicit GEMM on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+//   out[p][co] = act(bias[co] + sum_{tap, ci} w[tap][co][ci] in[p + tap][ci])
+//
+// Activations are channels-last BF16 ([B][D][H][W][C], C a multiple of 16),
+// the box is periodic (p + tap wraps), accumulation is FP32 in tensor memory.
+// One CTA of 128 threads owns 128 consecutive output positions (the GEMM's M)
+// and all COUT channels (N).  Per tap the threads gather the shifted input
+// rows (K = CIN) and copy the tap's packed weights into one of two shared
+// stages, in the K-major no-swizzle layout of the MMA: 16-byte core-matrix
+// rows, chunk kc of row m at (kc * ROWS + m) * 16 bytes.  Thread 0 issues the
+// CIN/16 MMAs of the tap (M = 128, N = COUT, K = 16 each) and commits them to
+// the stage's mbarrier; a stage is refilled only after that commit arrived.
+// Waits are bounded (lfts_bulk.cuh): a wait that gives up sets the device
+// error word, waits once more for the tensor core, frees the tensor memory
+// and returns.  Included by lfts_engine.cu (one device error word).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "lfts_bulk.cuh"
+
+namespace lfts {
+namespace unet {
+
+constexpr int CONV_M = 128;  // output positions per CTA (MMA M)
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    // K-major, no swizzle: start, leading (K-chunk) and stride (8-row group)
+    // byte offsets in 16-byte units; version 1 (bits 46-47)
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+        "[%16];\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint16_t to_bf16(float f) {
+    // round to nearest even (finite values; NaN stays NaN)
+    uint32_t u = __float_as_uint(f);
+    if ((u & 0x7F800000u) == 0x7F800000u) return (uint16_t)((u >> 16) | ((u & 0xFFFF) ? 0x40 : 0));
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+// in: [npos][cin] BF16 (npos = B*D*H*W), wpk: [taps][cin/8][cout][8] BF16,
+// bias: [cout] FP32, out: [npos][cout] BF16.
+__global__ void __launch_bounds__(CONV_M) k_conv3d_umma(const uint4 *__restrict__ in, const uint4 *__restrict__ wpk,
+                                                        const float *__restrict__ bias, uint16_t *__restrict__ out, int B,
+                                                        int D, int H, int W, int cin, int cout, int taps, int relu,
+                                                        uint32_t tmem_cols) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int kc_n = cin / 8;                       // 16-byte chunks per row (K / 8)
+    const int a_units = kc_n * CONV_M, b_units = kc_n * cout;
+    uint4 *stage0 = (uint4 *)smem_raw;              // [2][a_units + b_units] 16-byte units
+    uint64_t *bar = (uint64_t *)(stage0 + 2 * (a_units + b_units));
+    uint32_t *tmem_slot = (uint32_t *)(bar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const long long npos = (long long)B * D * H * W;
+    const long long p = (long long)blockIdx.x * CONV_M + tid;
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    // this thread's output position
+    int n = 0, z = 0, y = 0, x = 0;
+    const bool valid = p < npos;
+    if (valid) {
+        long long q = p;
+        x = (int)(q % W);
+        q /= W;
+        y = (int)(q % H);
+        q /= H;
+        z = (int)(q % D);
+        n = (int)(q / D);
+    }
+    // instruction descriptor: FP32 accumulate, BF16 A and B, both K-major, N = cout, M = 128
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(cout >> 3) << 17) | ((uint32_t)(CONV_M >> 4) << 24);
+    bool ok = true;
+    for (int t = 0; t < taps; t++) {
+        const int st = t & 1;
+        // every thread takes the same branch: the wait results are combined
+        if (t >= 2 && !__syncthreads_and(mbar_wait(bar + st, ((t >> 1) - 1) & 1))) {
+            ok = false;
+            break;
+        }
+        uint4 *sa = stage0 + st * (a_units + b_units), *sb = sa + a_units;
+        // A: the input row at this position shifted by the tap (periodic)
+        {
+            uint4 *dst = sa + tid;
+            if (valid) {
+                int dz = 0, dy = 0, dx = 0;
+                if (taps == 27) {
+                    dz = t / 9 - 1;
+                    dy = (t / 3) % 3 - 1;
+                    dx = t % 3 - 1;
+                }
+                const int zz = (z + dz + D) % D, yy = (y + dy + H) % H, xx = (x + dx + W) % W;
+                const uint4 *src = in + ((((long long)n * D + zz) * H + yy) * W + xx) * kc_n;
+                for (int kc = 0; kc < kc_n; kc++) dst[kc * CONV_M] = src[kc];
+            } else {
+                for (int kc = 0; kc < kc_n; kc++) dst[kc * CONV_M] = make_uint4(0, 0, 0, 0);
+            }
+        }
+        // B: the tap's packed weights
+        {
+            const uint4 *src = wpk + (long long)t * b_units;
+            for (int i = tid; i < b_units; i += CONV_M) sb[i] = src[i];
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_addr(sa), b0 = smem_addr(sb);
+            for (int s = 0; s < kc_n / 2; s++) {
+                const uint64_t da = umma_desc(a0 + (uint32_t)(2 * s * CONV_M * 16), CONV_M * 16, 128);
+                const uint64_t db = umma_desc(b0 + (uint32_t)(2 * s * cout * 16), (uint32_t)cout * 16, 128);
+                umma_bf16(tmem, da, db, idesc, (t > 0 || s > 0) ? 1u : 0u);
+            }
+            umma_commit(bar + st);
+        }
+    }
+    {
+        const bool fin = ok ? mbar_wait(bar + ((taps - 1) & 1), ((taps - 1) >> 1) & 1) : false;
+        ok = __syncthreads_and(fin);
+    }
+    if (!ok) {
+        // give the tensor core a second bounded wait, then release and leave
+        mbar_wait(bar + ((taps - 1) & 1), ((taps - 1) >> 1) & 1);
+    } else {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // epilogue: warp w reads accumulator rows 32w..32w+31 (tensor-memory lanes)
+        for (int c0 = 0; c0 < cout; c0 += 16) {
+            uint32_t v[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+            if (valid) {
+                uint16_t h[16];
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    float f = __uint_as_float(v[i]) + bias[c0 + i];
+                    if (relu && f < 0.f) f = 0.f;
+                    h[i] = to_bf16(f);
+                }
+                uint4 *o = (uint4 *)(out + p * cout + c0);
+                o[0] = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
+                o[1] = make_uint4(h[8] | (h[9] << 16), h[10] | (h[11] << 16), h[12] | (h[13] << 16), h[14] | (h[15] << 16));
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+}
+}  // namespace unet
+}  // namespace lfts
+
+extern "C" int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, const float *bias, void *out, int B, int D,
+                                int H, int W, int cin, int cout, int taps, int relu) {
+    if (!in || !wpk || !bias || !out) return fail("null argument");
+    if (B < 1 || D < 1 || H < 1 || W < 1) return fail("conv3d: extents must be positive");
+    if (cin < 16 || cin % 16 || cin > LFTS_CONV_MAX_CIN)
+        return fail("conv3d: cin must be a multiple of 16 up to " + std::to_string(LFTS_CONV_MAX_CIN));
+    if (cout < 16 || cout % 16 || cout > LFTS_CONV_MAX_COUT)
+        return fail("conv3d: cout must be a multiple of 16 up to " + std::to_string(LFTS_CONV_MAX_COUT));
+    if (taps != 1 && taps != 27) return fail("conv3d: taps must be 1 (1x1x1) or 27 (3x3x3)");
+    if (((uintptr_t)in | (uintptr_t)wpk | (uintptr_t)out) & 15) return fail("conv3d: buffers must be 16-byte aligned");
+    const long long npos = (long long)B * D * H * W;
+    const long long blocks = (npos + lfts::unet::CONV_M - 1) / lfts::unet::CONV_M;
+    if (blocks > 0x7fffffffLL) return fail("conv3d: too many positions");
+    uint32_t cols = 32;
+    while ((int)cols < cout) cols <<= 1;
+    const size_t smem = (size_t)2 * 16 * ((size_t)(cin / 8) * (lfts::unet::CONV_M + cout)) + 2 * sizeof(uint64_t) + 16;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(lfts::unet::k_conv3d_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return fail(std::string("conv3d: ") + cudaGetErrorString(e));
+        attr_set = true;
+    }
+    lfts::unet::k_conv3d_umma<<<(unsigned)blocks, lfts::unet::CONV_M, smem, (cudaStream_t)stream>>>(
+        (const uint4 *)in, (const uint4 *)wpk, bias, (uint16_t *)out, B, D, H, W, cin, cout, taps, relu, cols);
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) return fail(std::string("conv3d launch: ") + cudaGetErrorString(e));
+    return 0;
+}

@@ -97,12 +97,95 @@ def generate_pairs(sim, nsteps):
     return np.array(X), np.array(Y), iters
 
 
+def _pad16(c):
+    return (c + 15) // 16 * 16
+
+
+def pack_conv(conv, in_map, cin_pad):
+    """Weights of an nn.Conv3d (kernel 3 or 1) in the layout lfts_conv3d_bf16
+    reads: [taps][cin_pad/8][cout_pad][8] BF16, tap = 9 kz + 3 ky + kx; real
+    input channel i sits at padded position in_map[i].  Returns (packed
+    weights, FP32 bias [cout_pad], cout_pad, taps)."""
+    w = conv.weight.detach().float().cpu()
+    co, ci, k = w.shape[0], w.shape[1], w.shape[2]
+    taps, cout_pad = k ** 3, _pad16(co)
+    full = torch.zeros(taps, cout_pad, cin_pad)
+    full[:, :co, torch.as_tensor(in_map)] = w.permute(2, 3, 4, 0, 1).reshape(taps, co, ci)
+    packed = full.reshape(taps, cout_pad, cin_pad // 8, 8).permute(0, 2, 1, 3).contiguous()
+    bias = torch.zeros(cout_pad)
+    if conv.bias is not None:
+        bias[:co] = conv.bias.detach().float().cpu()
+    return packed.to(torch.bfloat16).cuda(), bias.cuda(), cout_pad, taps
+
+
+def conv3d_tcgen05(x, layer, relu):
+    """Periodic convolution of a channels-last BF16 tensor [B, D, H, W, cin_pad]
+    with a packed layer, by lfts_conv3d_bf16 on torch's current stream."""
+    from langevinfts_b200.capi import check, lib
+    wpk, bias, cout_pad, taps = layer
+    B, D, H, W, cin = x.shape
+    out = torch.empty([B, D, H, W, cout_pad], dtype=torch.bfloat16, device=x.device)
+    check(lib().lfts_conv3d_bf16(torch.cuda.current_stream().cuda_stream, x.data_ptr(), wpk.data_ptr(), bias.data_ptr(),
+                                 out.data_ptr(), B, D, H, W, cin, cout_pad, taps, 1 if relu else 0))
+    return out
+
+
+class TcgenUNet:
+    """Inference of a trained UNet3D with every convolution on the tensor cores
+    (lfts_conv3d_bf16: tcgen05 implicit GEMM, BF16 operands, FP32 accumulate);
+    activations channels-last BF16 with channels padded to multiples of 16,
+    pooling / upsampling / concatenation as torch glue."""
+
+    def __init__(self, net):
+        b = net.e1[0].out_channels
+        pb, p2, p4 = _pad16(b), _pad16(2 * b), _pad16(4 * b)
+        cin = net.e1[0].in_channels
+        rng = lambda n: list(range(n))
+        self.cin_pad = _pad16(cin)
+        self.e1 = (pack_conv(net.e1[0], rng(cin), self.cin_pad), pack_conv(net.e1[2], rng(b), pb))
+        self.e2 = (pack_conv(net.e2[0], rng(b), pb), pack_conv(net.e2[2], rng(2 * b), p2))
+        self.e3 = (pack_conv(net.e3[0], rng(2 * b), p2), pack_conv(net.e3[2], rng(4 * b), p4))
+        # concatenations: upsampled part first, then the skip (each padded)
+        self.d2 = (pack_conv(net.d2[0], rng(4 * b) + [p4 + i for i in range(2 * b)], p4 + p2),
+                   pack_conv(net.d2[2], rng(2 * b), p2))
+        self.d1 = (pack_conv(net.d1[0], rng(2 * b) + [p2 + i for i in range(b)], p2 + pb), pack_conv(net.d1[2], rng(b), pb))
+        self.out = pack_conv(net.out, rng(b), pb)
+        self.cout = net.out.out_channels
+
+    @staticmethod
+    def _pool(x):
+        B, D, H, W, C = x.shape
+        return x.float().reshape(B, D // 2, 2, H // 2, 2, W // 2, 2, C).mean((2, 4, 6)).to(torch.bfloat16).contiguous()
+
+    @staticmethod
+    def _up(x):
+        return x.repeat_interleave(2, 1).repeat_interleave(2, 2).repeat_interleave(2, 3).contiguous()
+
+    def _block(self, x, pair):
+        return conv3d_tcgen05(conv3d_tcgen05(x, pair[0], True), pair[1], True)
+
+    @torch.no_grad()
+    def __call__(self, x):
+        """x: [B, cin, D, H, W] float -> [B, cout, D, H, W] float32."""
+        h = x.permute(0, 2, 3, 4, 1).to(torch.bfloat16)
+        h = torch.nn.functional.pad(h, (0, self.cin_pad - h.shape[-1])).contiguous()
+        x1 = self._block(h, self.e1)
+        x2 = self._block(self._pool(x1), self.e2)
+        x3 = self._block(self._pool(x2), self.e3)
+        y2 = self._block(torch.cat([self._up(x3), x2], -1).contiguous(), self.d2)
+        y1 = self._block(torch.cat([self._up(y2), x1], -1).contiguous(), self.d1)
+        o = conv3d_tcgen05(y1, self.out, False)[..., :self.cout]
+        return o.permute(0, 4, 1, 2, 3).float().contiguous()
+
+
 class LearnedStart:
     """Callable for BatchedLFTS.step(start=...): predicts the imaginary field
     of every replica from the fields on the device and writes it in place."""
 
-    def __init__(self, model, s_in, s_out, batch=8):
+    def __init__(self, model, s_in, s_out, batch=8, tcgen05=False):
         self.model, self.s_in, self.s_out, self.batch = model.eval(), float(s_in), float(s_out), batch
+        # tcgen05=True: the convolutions run on this library's tensor-core kernel
+        self.net = TcgenUNet(self.model) if tcgen05 else None
 
     @torch.no_grad()
     def __call__(self, sim):
@@ -115,8 +198,11 @@ class LearnedStart:
             for r0 in range(0, R, self.batch):
                 wr = w[r0:r0 + self.batch]
                 x = torch.stack([wr[:, ri] / self.s_in, wr[:, ii] / self.s_out], 1).float().reshape([-1, 2] + shape)
-                with torch.autocast("cuda", dtype=torch.bfloat16):
-                    d = self.model(x).float()
+                if self.net is not None:
+                    d = self.net(x)
+                else:
+                    with torch.autocast("cuda", dtype=torch.bfloat16):
+                        d = self.model(x).float()
                 d = d.reshape(-1, M).double() * self.s_out
                 d -= d.mean(1, keepdim=True)  # the pressure field keeps zero mean
                 wr[:, ii] += d

@@ -1,0 +1,67 @@
+"""The U-Net convolution on the tensor cores (lfts_conv3d_bf16: tcgen05
+implicit GEMM, BF16 operands, FP32 accumulation in tensor memory) against
+torch's FP32 periodic conv3d of the same BF16-rounded inputs and weights, for
+every layer shape of the 24-channel U-Net (channel padding, the padded skip
+concatenations, the 1x1x1 output layer, a partial 128-position tile); then the
+whole tensor-core U-Net against the FP32 torch model."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _reference(x, conv, relu):
+    import torch
+    import torch.nn.functional as F
+    w = conv.weight.detach().to(torch.bfloat16).float()
+    b = conv.bias.detach().float()
+    k = w.shape[-1]
+    xp = F.pad(x, (k // 2,) * 6, mode="circular") if k > 1 else x
+    y = F.conv3d(xp, w, b)
+    return F.relu(y) if relu else y
+
+
+@pytest.mark.parametrize("cin,cin_pad,cout,k,grid,batch", [
+    (2, 16, 24, 3, (8, 8, 8), 2),      # first layer (input channels padded 2 -> 16, outputs 24 -> 32)
+    (24, 32, 48, 3, (8, 8, 8), 2),
+    (48, 48, 96, 3, (4, 4, 4), 2),
+    (144, 144, 48, 3, (8, 8, 8), 1),   # decoder concat, largest K
+    (96, 96, 96, 3, (4, 6, 5), 1),     # non-cubic box, 120 positions: one partial tile
+    (24, 32, 1, 1, (8, 8, 8), 2),      # 1x1x1 output layer
+])
+@pytest.mark.parametrize("relu", [True, False])
+def test_conv_matches_torch(cin, cin_pad, cout, k, grid, batch, relu):
+    import torch
+    from langevinfts_b200.learned import conv3d_tcgen05, pack_conv
+    torch.manual_seed(cin * 31 + cout)
+    conv = torch.nn.Conv3d(cin, cout, k).cuda()
+    x = torch.randn(batch, cin, *grid, device="cuda").to(torch.bfloat16).float()
+    layer = pack_conv(conv, list(range(cin)), cin_pad)
+    h = x.permute(0, 2, 3, 4, 1)
+    h = torch.nn.functional.pad(h, (0, cin_pad - cin)).to(torch.bfloat16).contiguous()
+    got = conv3d_tcgen05(h, layer, relu).float()
+    torch.cuda.synchronize()
+    ref = _reference(x, conv, relu).permute(0, 2, 3, 4, 1)
+    scale = float(ref.abs().max())
+    # BF16 rounding of the output (2^-8 relative) plus FP32 accumulation order
+    assert float((got[..., :cout] - ref).abs().max()) <= 8e-3 * scale + 1e-6
+    assert float(got[..., cout:].abs().max() if got.shape[-1] > cout else 0) == 0.0  # padded channels stay zero
+
+
+def test_tcgen05_unet_matches_torch_model():
+    import torch
+    from langevinfts_b200.learned import TcgenUNet, UNet3D
+    torch.manual_seed(3)
+    net = UNet3D(cin=2, cout=1, base=24).cuda()
+    for p in net.parameters():  # non-zero last layer
+        if p.dim() == 1:
+            torch.nn.init.normal_(p, 0, 0.05)
+    torch.nn.init.normal_(net.out.weight, 0, 0.2)
+    x = torch.randn(2, 2, 16, 16, 16, device="cuda")
+    with torch.no_grad():
+        ref = net(x)
+    got = TcgenUNet(net)(x)
+    torch.cuda.synchronize()
+    rel = float((got - ref).abs().max() / ref.abs().max())
+    assert rel < 5e-2, rel  # BF16 activations through 11 layers
+    assert np.corrcoef(got.flatten().cpu().numpy(), ref.flatten().cpu().numpy())[0, 1] > 0.999
