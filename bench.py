@@ -424,15 +424,76 @@ def run_learned(args):
         return float(np.mean(iters)), R * args.steps / (time.time() - t), fails
 
     plain, learned = run(None), run(start)
+    from langevinfts_b200.learned import LearnedStart
+    learned_tc = run(LearnedStart(start.model, start.s_in, start.s_out, tcgen05=True))
     print(json.dumps({"metric": "mean saddle-point iterations per Langevin step (learned start ablation)",
                       "workload": args.workload, "grid": [args.nx] * 3, "replicas": R,
                       "plain": {"mean_iterations": plain[0], "replica_steps_per_s": plain[1], "failed": plain[2]},
                       "learned": {"mean_iterations": learned[0], "replica_steps_per_s": learned[1], "failed": learned[2]},
+                      "learned_tcgen05": {"mean_iterations": learned_tc[0], "replica_steps_per_s": learned_tc[1],
+                                          "failed": learned_tc[2], "inference": "lfts_conv3d_bf16 (tcgen05)"},
                       "steps": args.steps, "training_pairs": int(len(X)), "data_steps": args.learned_steps,
                       "data_seconds": t_gen, "train_seconds": t_train, "epochs": len(hist),
                       "loss_first_last": [hist[0][1], hist[-1][1]],
                       "model": "3-level periodic 3D U-Net, 24 base channels, 3^3 kernels, BF16 autocast (torch conv3d)",
                       "timing": "wall clock around the steps, host noise"}))
+    return 0
+
+
+def run_conv(args):
+    """The U-Net convolutions on the tensor cores (lfts_conv3d_bf16) against
+    torch's conv3d (cuDNN, BF16, channels-last) for every layer shape of the
+    24-channel U-Net at the workload grid, batch 8 (the learned start's batch):
+    CUDA-event time per launch, FLOP/s on the real channels, fraction of the
+    measured BF16 peak."""
+    import torch
+    import torch.nn.functional as F
+    from langevinfts_b200.learned import conv3d_tcgen05, pack_conv
+    torch.cuda.init()
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(pk)) if os.path.exists(pk) else {}
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    N, B, b = args.nx, 8, 24
+    # (name, cin real, cin padded, cout, kernel, level)
+    layers = [("e1a", 2, 16, b, 3, 0), ("e1b", b, 32, b, 3, 0), ("e2a", b, 32, 2 * b, 3, 1), ("e2b", 2 * b, 48, 2 * b, 3, 1),
+              ("e3a", 2 * b, 48, 4 * b, 3, 2), ("e3b", 4 * b, 96, 4 * b, 3, 2), ("d2a", 6 * b, 144, 2 * b, 3, 1),
+              ("d2b", 2 * b, 48, 2 * b, 3, 1), ("d1a", 3 * b, 80, b, 3, 0), ("d1b", b, 32, b, 3, 0), ("out", b, 32, 1, 1, 0)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    rows, tot_us, tot_us_ref, tot_flop = [], 0.0, 0.0, 0.0
+    for name, ci, cip, co, k, lev in layers:
+        n = N >> lev
+        conv = torch.nn.Conv3d(ci, co, k).cuda()
+        layer = pack_conv(conv, list(range(ci)), cip)
+        x = torch.randn(B, n, n, n, cip, device="cuda").to(torch.bfloat16)
+        xr = x[..., :ci].permute(0, 4, 1, 2, 3).contiguous(memory_format=torch.channels_last_3d)
+        convb = conv.to(torch.bfloat16).to(memory_format=torch.channels_last_3d)
+        flop = 2.0 * B * n ** 3 * ci * co * k ** 3
+
+        def ours():
+            conv3d_tcgen05(x, layer, True)
+
+        def ref():
+            F.relu(convb(F.pad(xr, (k // 2,) * 6, mode="circular") if k > 1 else xr))
+
+        res = []
+        for fn in (ours, ref):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            ev[0].record()
+            for _ in range(args.steps):
+                fn()
+            ev[1].record()
+            ev[1].synchronize()
+            res.append(ev[0].elapsed_time(ev[1]) * 1e3 / args.steps)
+        tot_us, tot_us_ref, tot_flop = tot_us + res[0], tot_us_ref + res[1], tot_flop + flop
+        rows.append({"layer": name, "grid": n, "cin": ci, "cout": co, "k": k, "tcgen05_us": res[0], "cudnn_us": res[1],
+                     "tcgen05_tflops": flop / res[0] / 1e6, "cudnn_tflops": flop / res[1] / 1e6})
+    print(json.dumps({"metric": "U-Net convolution time per forward (batch 8)", "grid": [N] * 3, "layers": rows,
+                      "total_tcgen05_us": tot_us, "total_cudnn_us": tot_us_ref,
+                      "tcgen05_tflops": tot_flop / tot_us / 1e6, "peak_bf16_tflops": peak,
+                      "frac_of_peak": tot_flop / tot_us / 1e6 / peak,
+                      "note": "FLOPs on the real channels; cuDNN timing includes its circular pad"}))
     return 0
 
 
@@ -656,6 +717,7 @@ def main():
     ap.add_argument("--ref-statistics", default="", help=argparse.SUPPRESS)
     ap.add_argument("--ref-scft", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--scft", action="store_true", help="SCFT of the 64^3 asymmetric diblock (device loop, FP64 and FP32)")
+    ap.add_argument("--conv", action="store_true", help="time the tensor-core U-Net convolutions against cuDNN")
     ap.add_argument("--learned", action="store_true",
                     help="ablation of the learned saddle-point start (U-Net) on the workload's system")
     ap.add_argument("--learned-steps", type=int, default=20, help="plain Langevin steps that make the training pairs")
@@ -682,6 +744,8 @@ def main():
         return run_scft(args)
     if args.learned:
         return run_learned(args)
+    if args.conv:
+        return run_conv(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.kernel_only:
