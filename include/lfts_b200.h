@@ -344,12 +344,20 @@ int lfts_pcg64_normal(lfts_ctx ctx, unsigned long long *states, int nstreams, lo
  * wpk: packed weights [taps][cin/8][cout][8] BF16 (tap = 9 kz + 3 ky + kx,
  * offset (kz-1, ky-1, kx-1); taps = 27 for 3x3x3, 1 for 1x1x1), bias: cout
  * FP32 (device).  cin, cout: multiples of 16, cin <= LFTS_CONV_MAX_CIN,
- * cout <= LFTS_CONV_MAX_COUT; act = ReLU when relu != 0.  stream: cudaStream_t.
+ * cout <= LFTS_CONV_MAX_COUT, and the two shared stages, 32 cin (128 + cout)
+ * bytes, within 200 KB; act = ReLU when relu != 0.  stream: cudaStream_t.
  * No counterpart in the reference (it has no learned component). */
 #define LFTS_CONV_MAX_CIN 160
-#define LFTS_CONV_MAX_COUT 128
+#define LFTS_CONV_MAX_COUT 256
 int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, const float *bias, void *out, int B, int D, int H, int W,
                      int cin, int cout, int taps, int relu);
+/* Its weight gradient, also on the tensor cores:
+ *   dw[tap][co][ci] += sum_p gy[p][co] x[(p + tap) mod box][ci]
+ * x: [B][D][H][W][cin], gy: [B][D][H][W][cout] BF16 channels-last; dw: FP32
+ * [taps][cout][ci], accumulated (zero it first); cout <= 128.  The input gradient is
+ * lfts_conv3d_bf16 of gy with the weights transposed and the taps mirrored. */
+int lfts_conv3d_wgrad_bf16(void *stream, const void *x, const void *gy, float *dw, int B, int D, int H, int W, int cin,
+                           int cout, int taps);
 
 /* Adam field update of the SCFT driver (examples/scft/scft.py:42-54), on n
  * doubles: m = b1 m + (1-b1) d; v = b2 v + (1-b2) d^2;

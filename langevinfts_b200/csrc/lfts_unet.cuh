@@ -183,8 +183,171 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_umma(const uint4 *__restrict_
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
 }
+
+// ------------------------------------------------------------------------
+// Weight gradient of the periodic convolution:
+//   dw[tap][co][ci] += sum_p gy[p][co] x[p + tap][ci]
+// per tap a GEMM with M = co (padded to 128 rows), N = cin, K = positions.
+// Both operands are MN-major in channels-last memory (16 bytes = 8 channels of
+// one position), so they are staged without transposition: chunk c of
+// position k at (c * WG_K + k) * 16 bytes; 8 consecutive positions form a core
+// matrix (LBO = 128 bytes), channel chunks are WG_K * 16 bytes apart (SBO).
+// A CTA takes one (kz, ky) row of taps (kx = 0..2; the single tap of a 1x1x1
+// kernel) over WG_CHUNK positions, keeps one accumulator per tap in tensor
+// memory, and adds them to dw (FP32, zeroed by the caller) with atomics.
+constexpr int WG_K = 64;        // positions per stage (4 MMA K-steps)
+constexpr int WG_CHUNK = 2048;  // positions per CTA
+
+__global__ void __launch_bounds__(CONV_M) k_conv3d_wgrad_umma(const uint4 *__restrict__ x, const uint4 *__restrict__ gy,
+                                                              float *__restrict__ dw, int B, int D, int H, int W, int cin,
+                                                              int cout, int taps, uint32_t tmem_cols) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int ntap = taps == 27 ? 3 : 1;
+    const int xc = cin / 8, gc = cout / 8;             // 16-byte chunks per position
+    const int a_units = 16 * WG_K, b_units = xc * WG_K; // A: 128 rows (16 chunks), B per tap
+    const int st_units = a_units + ntap * b_units;
+    uint4 *stage0 = (uint4 *)smem_raw;
+    uint64_t *bar = (uint64_t *)(stage0 + 2 * st_units);
+    uint32_t *tmem_slot = (uint32_t *)(bar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const long long npos = (long long)B * D * H * W;
+    const long long p0 = (long long)blockIdx.x * WG_CHUNK;
+    const int g = blockIdx.y;  // tap row: kz = g / 3, ky = g % 3
+    // rows of A beyond cout stay zero in both stages
+    for (int i = tid; i < 2 * st_units; i += CONV_M) stage0[i] = make_uint4(0, 0, 0, 0);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    // M = 128, N = cin, both operands MN-major, FP32 accumulate
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(cin >> 3) << 17) |
+                           ((uint32_t)(CONV_M >> 4) << 24);
+    const int k = tid & (WG_K - 1), half = tid / WG_K;  // two threads per staged position
+    const int nst = WG_CHUNK / WG_K;
+    bool ok = true;
+    for (int u = 0; u < nst; u++) {
+        const int st = u & 1;
+        if (u >= 2 && !__syncthreads_and(mbar_wait(bar + st, ((u >> 1) - 1) & 1))) {
+            ok = false;
+            break;
+        }
+        uint4 *sa = stage0 + st * st_units, *sb = sa + a_units;
+        const long long p = p0 + (long long)u * WG_K + k;
+        const bool valid = p < npos;
+        int n = 0, z = 0, y = 0, xx = 0;
+        if (valid) {
+            long long q = p;
+            xx = (int)(q % W);
+            q /= W;
+            y = (int)(q % H);
+            q /= H;
+            z = (int)(q % D);
+            n = (int)(q / D);
+        }
+        for (int c = half; c < gc; c += 2)
+            sa[c * WG_K + k] = valid ? gy[p * gc + c] : make_uint4(0, 0, 0, 0);
+        for (int j = 0; j < ntap; j++) {
+            uint4 *dst = sb + j * b_units + k;
+            if (valid) {
+                int dz = 0, dy = 0, dx = 0;
+                if (taps == 27) {
+                    dz = g / 3 - 1;
+                    dy = g % 3 - 1;
+                    dx = j - 1;
+                }
+                const int zz = (z + dz + D) % D, yy = (y + dy + H) % H, x2 = (xx + dx + W) % W;
+                const uint4 *src = x + ((((long long)n * D + zz) * H + yy) * W + x2) * xc;
+                for (int c = half; c < xc; c += 2) dst[c * WG_K] = src[c];
+            } else {
+                for (int c = half; c < xc; c += 2) dst[c * WG_K] = make_uint4(0, 0, 0, 0);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_addr(sa), b0 = smem_addr(sb);
+            for (int s = 0; s < WG_K / 16; s++) {
+                const uint64_t da = umma_desc(a0 + (uint32_t)(16 * s * 16), 128, WG_K * 16);
+                for (int j = 0; j < ntap; j++) {
+                    const uint64_t db = umma_desc(b0 + (uint32_t)((j * b_units + 16 * s) * 16), 128, WG_K * 16);
+                    umma_bf16(tmem + (uint32_t)(j * cin), da, db, idesc, (u > 0 || s > 0) ? 1u : 0u);
+                }
+            }
+            umma_commit(bar + st);
+        }
+    }
+    {
+        const bool fin = ok ? mbar_wait(bar + ((nst - 1) & 1), ((nst - 1) >> 1) & 1) : false;
+        ok = __syncthreads_and(fin);
+    }
+    if (!ok) {
+        mbar_wait(bar + ((nst - 1) & 1), ((nst - 1) >> 1) & 1);
+    } else {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int co = 32 * warp + (tid & 31);  // accumulator row of this thread
+        for (int j = 0; j < ntap; j++) {
+            const int tap = taps == 27 ? 3 * g + j : 0;
+            for (int c0 = 0; c0 < cin; c0 += 16) {
+                uint32_t v[16];
+                tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(j * cin + c0), v);
+                if (co < cout) {
+                    float *o = dw + ((long long)tap * cout + co) * cin + c0;
+#pragma unroll
+                    for (int i = 0; i < 16; i++) atomicAdd(o + i, __uint_as_float(v[i]));
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+}
 }  // namespace unet
 }  // namespace lfts
+
+extern "C" int lfts_conv3d_wgrad_bf16(void *stream, const void *x, const void *gy, float *dw, int B, int D, int H, int W,
+                                      int cin, int cout, int taps) {
+    if (!x || !gy || !dw) return fail("null argument");
+    if (B < 1 || D < 1 || H < 1 || W < 1) return fail("conv3d wgrad: extents must be positive");
+    if (cin < 16 || cin % 16 || cin > LFTS_CONV_MAX_CIN)
+        return fail("conv3d wgrad: cin must be a multiple of 16 up to " + std::to_string(LFTS_CONV_MAX_CIN));
+    if (cout < 16 || cout % 16 || cout > LFTS_CONV_MAX_COUT)
+        return fail("conv3d wgrad: cout must be a multiple of 16 up to " + std::to_string(LFTS_CONV_MAX_COUT));
+    if (taps != 1 && taps != 27) return fail("conv3d wgrad: taps must be 1 or 27");
+    if (((uintptr_t)x | (uintptr_t)gy) & 15) return fail("conv3d wgrad: buffers must be 16-byte aligned");
+    const long long npos = (long long)B * D * H * W;
+    const long long chunks = (npos + lfts::unet::WG_CHUNK - 1) / lfts::unet::WG_CHUNK;
+    if (chunks > 0x7fffffffLL) return fail("conv3d wgrad: too many positions");
+    const int ntap = taps == 27 ? 3 : 1;
+    uint32_t cols = 32;
+    while ((int)cols < ntap * cin) cols <<= 1;
+    const size_t st_units = (size_t)16 * lfts::unet::WG_K + (size_t)ntap * (cin / 8) * lfts::unet::WG_K;
+    const size_t smem = 2 * 16 * st_units + 2 * sizeof(uint64_t) + 16;
+    if (smem > 200 * 1024) return fail("conv3d wgrad: cin too large for the shared-memory stages");
+    if (cout > 128) return fail("conv3d wgrad: cout (the accumulator rows) must be <= 128");
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(lfts::unet::k_conv3d_wgrad_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return fail(std::string("conv3d wgrad: ") + cudaGetErrorString(e));
+        attr_set = true;
+    }
+    lfts::unet::k_conv3d_wgrad_umma<<<dim3((unsigned)chunks, taps == 27 ? 9 : 1), lfts::unet::CONV_M, smem,
+                                      (cudaStream_t)stream>>>((const uint4 *)x, (const uint4 *)gy, dw, B, D, H, W, cin, cout,
+                                                              taps, cols);
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) return fail(std::string("conv3d wgrad launch: ") + cudaGetErrorString(e));
+    return 0;
+}
 
 extern "C" int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, const float *bias, void *out, int B, int D,
                                 int H, int W, int cin, int cout, int taps, int relu) {
@@ -202,6 +365,7 @@ extern "C" int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, c
     uint32_t cols = 32;
     while ((int)cols < cout) cols <<= 1;
     const size_t smem = (size_t)2 * 16 * ((size_t)(cin / 8) * (lfts::unet::CONV_M + cout)) + 2 * sizeof(uint64_t) + 16;
+    if (smem > 200 * 1024) return fail("conv3d: cin x (128 + cout) too large for the shared-memory stages");
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(lfts::unet::k_conv3d_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

@@ -130,6 +130,104 @@ def conv3d_tcgen05(x, layer, relu):
     return out
 
 
+def _full_weights(w, in_map, cin_pad, cout_pad):
+    """[taps, cout_pad, cin_pad] FP32 from a torch conv weight [co, ci, k, k, k]."""
+    co, ci, k = w.shape[0], w.shape[1], w.shape[2]
+    full = torch.zeros(k ** 3, cout_pad, cin_pad, device=w.device)
+    full[:, :co, torch.as_tensor(in_map, device=w.device)] = w.detach().float().permute(2, 3, 4, 0, 1).reshape(k ** 3, co, ci)
+    return full
+
+
+def _pack_full(full):
+    taps, cout_pad, cin_pad = full.shape
+    return full.reshape(taps, cout_pad, cin_pad // 8, 8).permute(0, 2, 1, 3).contiguous().to(torch.bfloat16)
+
+
+class _ConvFn(torch.autograd.Function):
+    """Periodic conv (+ ReLU) on the tensor cores with its backward: the input
+    gradient by lfts_conv3d_bf16 with transposed, tap-mirrored weights, the
+    weight gradient by lfts_conv3d_wgrad_bf16."""
+
+    @staticmethod
+    def forward(ctx, x, w, b, in_map, cin_pad, relu):
+        from langevinfts_b200.capi import check, lib
+        co, k = w.shape[0], w.shape[2]
+        cout_pad, taps = _pad16(co), k ** 3
+        full = _full_weights(w, in_map, cin_pad, cout_pad)
+        bias = torch.zeros(cout_pad, device=w.device)
+        bias[:co] = b.detach().float()
+        y = conv3d_tcgen05(x, (_pack_full(full), bias, cout_pad, taps), relu)
+        ctx.save_for_backward(x, y, full)
+        ctx.meta = (co, w.shape[1], k, in_map, cin_pad, cout_pad, taps, relu)
+        return y
+
+    @staticmethod
+    def backward(ctx, gy):
+        from langevinfts_b200.capi import check, lib
+        x, y, full = ctx.saved_tensors
+        co, ci, k, in_map, cin_pad, cout_pad, taps, relu = ctx.meta
+        g = gy * (y > 0) if relu else gy
+        g = g.to(torch.bfloat16).contiguous()
+        # input gradient: the same convolution of g, weights transposed, taps mirrored
+        back = full.flip(0).transpose(1, 2).contiguous()  # [taps, cin_pad, cout_pad]
+        dx = conv3d_tcgen05(g, (_pack_full(back), torch.zeros(cin_pad, device=g.device), cin_pad, taps), False)
+        dwp = torch.zeros(taps, cout_pad, cin_pad, device=g.device)
+        B, D, H, W, _ = x.shape
+        check(lib().lfts_conv3d_wgrad_bf16(torch.cuda.current_stream().cuda_stream, x.data_ptr(), g.data_ptr(), dwp.data_ptr(),
+                                           B, D, H, W, cin_pad, cout_pad, taps))
+        dw = dwp[:, :co, torch.as_tensor(in_map, device=g.device)].reshape(k, k, k, co, ci).permute(3, 4, 0, 1, 2).contiguous()
+        db = g[..., :co].float().sum((0, 1, 2, 3))
+        return dx, dw, db, None, None, None
+
+
+class TcgenUNetTrain(torch.nn.Module):
+    """Training form of a UNet3D with every convolution, forward and backward,
+    on the tensor cores (_ConvFn); the UNet3D's parameters receive the
+    gradients, so torch's AdamW steps them and TcgenUNet / the torch model
+    both run the result."""
+
+    def __init__(self, net):
+        super().__init__()
+        self.net = net
+        b = net.e1[0].out_channels
+        self.pb, self.p2, self.p4 = _pad16(b), _pad16(2 * b), _pad16(4 * b)
+        self.cin = net.e1[0].in_channels
+        self.cin_pad = _pad16(self.cin)
+        r = lambda n: list(range(n))
+        pb, p2, p4 = self.pb, self.p2, self.p4
+        self.maps = {"e1": (r(self.cin), self.cin_pad, r(b), pb), "e2": (r(b), pb, r(2 * b), p2),
+                     "e3": (r(2 * b), p2, r(4 * b), p4),
+                     "d2": (r(4 * b) + [p4 + i for i in range(2 * b)], p4 + p2, r(2 * b), p2),
+                     "d1": (r(2 * b) + [p2 + i for i in range(b)], p2 + pb, r(b), pb)}
+
+    def _block(self, h, name):
+        blk = getattr(self.net, name)
+        m0, c0, m1, c1 = self.maps[name]
+        h = _ConvFn.apply(h, blk[0].weight, blk[0].bias, m0, c0, True)
+        return _ConvFn.apply(h, blk[2].weight, blk[2].bias, m1, c1, True)
+
+    @staticmethod
+    def _pool(x):
+        B, D, H, W, C = x.shape
+        return x.float().reshape(B, D // 2, 2, H // 2, 2, W // 2, 2, C).mean((2, 4, 6)).to(torch.bfloat16).contiguous()
+
+    @staticmethod
+    def _up(x):
+        return x.repeat_interleave(2, 1).repeat_interleave(2, 2).repeat_interleave(2, 3).contiguous()
+
+    def forward(self, x):
+        h = x.permute(0, 2, 3, 4, 1).to(torch.bfloat16)
+        h = torch.nn.functional.pad(h, (0, self.cin_pad - h.shape[-1])).contiguous()
+        x1 = self._block(h, "e1")
+        x2 = self._block(self._pool(x1), "e2")
+        x3 = self._block(self._pool(x2), "e3")
+        y2 = self._block(torch.cat([self._up(x3), x2], -1).contiguous(), "d2")
+        y1 = self._block(torch.cat([self._up(y2), x1], -1).contiguous(), "d1")
+        o = _ConvFn.apply(y1, self.net.out.weight, self.net.out.bias, list(range(self.net.out.in_channels)),
+                          self.pb, False)[..., :self.net.out.out_channels]
+        return o.permute(0, 4, 1, 2, 3).float()
+
+
 class TcgenUNet:
     """Inference of a trained UNet3D with every convolution on the tensor cores
     (lfts_conv3d_bf16: tcgen05 implicit GEMM, BF16 operands, FP32 accumulate);
@@ -208,16 +306,18 @@ class LearnedStart:
                 wr[:, ii] += d
 
 
-def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_decay=1e-4, seed=0, log=None):
-    """AdamW on MSE of the scaled residual target (Y - w_+prev) / s_out, BF16
-    autocast, until `seconds` or `epochs` run out.  Returns (LearnedStart,
-    history of (epoch, mean loss))."""
+def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_decay=1e-4, seed=0, log=None, tcgen05=False):
+    """AdamW on MSE of the scaled residual target (Y - w_+prev) / s_out until
+    `seconds` or `epochs` run out; BF16 autocast over torch's convolutions, or
+    (tcgen05=True) every convolution's forward and backward on this library's
+    tensor-core kernels.  Returns (LearnedStart, history of (epoch, mean loss))."""
     torch.manual_seed(seed)
     s_in = float(np.std(X[:, 0])) or 1.0
     s_out = float(np.std(X[:, 1])) or 1.0
     xin = torch.from_numpy(np.concatenate([X[:, :1] / s_in, X[:, 1:] / s_out], 1)).cuda()
     tgt = torch.from_numpy((Y - X[:, 1:]) / s_out).cuda()
     model = UNet3D(cin=2, cout=1, base=base).cuda()
+    fwd = TcgenUNetTrain(model) if tcgen05 else None
     opt = torch.optim.AdamW(model.parameters(), lr=lr, weight_decay=weight_decay)
     n = xin.shape[0]
     hist, t0 = [], time.time()
@@ -226,8 +326,11 @@ def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_dec
         tot = 0.0
         for k in range(0, n, batch):
             idx = perm[k:k + batch]
-            with torch.autocast("cuda", dtype=torch.bfloat16):
-                loss = F.mse_loss(model(xin[idx]).float(), tgt[idx])
+            if fwd is not None:
+                loss = F.mse_loss(fwd(xin[idx]), tgt[idx])
+            else:
+                with torch.autocast("cuda", dtype=torch.bfloat16):
+                    loss = F.mse_loss(model(xin[idx]).float(), tgt[idx])
             opt.zero_grad(set_to_none=True)
             loss.backward()
             opt.step()
@@ -237,4 +340,4 @@ def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_dec
             log(f"epoch {ep} loss {tot / n:.4e}")
         if time.time() - t0 > seconds:
             break
-    return LearnedStart(model, s_in, s_out), hist
+    return LearnedStart(model, s_in, s_out, tcgen05=tcgen05), hist
