@@ -402,8 +402,11 @@ def run_learned(args):
     X, Y, it_gen = generate_pairs(sim, args.learned_steps)
     t_gen = time.time() - t0
     t0 = time.time()
-    start, hist = train(X, Y, seconds=args.learned_train)
+    start, hist = train(X, Y, seconds=args.learned_train)  # torch autograd over cuDNN
     t_train = time.time() - t0
+    t0 = time.time()
+    start_tc, hist_tc = train(X, Y, seconds=args.learned_train, tcgen05=True)  # every convolution on tcgen05
+    t_train_tc = time.time() - t0
     w0, xi0 = sim.fields(), sim.engine.get_noise_prev()
     rng0 = [g.bit_generator.state for g in sim.rngs]
 
@@ -423,19 +426,19 @@ def run_learned(args):
         torch.cuda.synchronize()
         return float(np.mean(iters)), R * args.steps / (time.time() - t), fails
 
-    plain, learned = run(None), run(start)
-    from langevinfts_b200.learned import LearnedStart
-    learned_tc = run(LearnedStart(start.model, start.s_in, start.s_out, tcgen05=True))
+    plain, learned, learned_tc = run(None), run(start), run(start_tc)
     print(json.dumps({"metric": "mean saddle-point iterations per Langevin step (learned start ablation)",
                       "workload": args.workload, "grid": [args.nx] * 3, "replicas": R,
                       "plain": {"mean_iterations": plain[0], "replica_steps_per_s": plain[1], "failed": plain[2]},
                       "learned": {"mean_iterations": learned[0], "replica_steps_per_s": learned[1], "failed": learned[2]},
                       "learned_tcgen05": {"mean_iterations": learned_tc[0], "replica_steps_per_s": learned_tc[1],
-                                          "failed": learned_tc[2], "inference": "lfts_conv3d_bf16 (tcgen05)"},
+                                          "failed": learned_tc[2], "train_seconds": t_train_tc, "epochs": len(hist_tc),
+                                          "loss_first_last": [hist_tc[0][1], hist_tc[-1][1]],
+                                          "network": "trained and run on lfts_conv3d_bf16 / lfts_conv3d_wgrad_bf16 (tcgen05)"},
                       "steps": args.steps, "training_pairs": int(len(X)), "data_steps": args.learned_steps,
                       "data_seconds": t_gen, "train_seconds": t_train, "epochs": len(hist),
                       "loss_first_last": [hist[0][1], hist[-1][1]],
-                      "model": "3-level periodic 3D U-Net, 24 base channels, 3^3 kernels, BF16 autocast (torch conv3d)",
+                      "model": "3-level periodic 3D U-Net, 24 base channels, 3^3 kernels; 'learned': torch conv3d with BF16 autocast",
                       "timing": "wall clock around the steps, host noise"}))
     return 0
 

@@ -73,7 +73,8 @@ def _rel(a, b):
 
 @pytest.mark.parametrize("cin,cin_pad,cout,k,grid,batch", [
     (2, 16, 24, 3, (8, 8, 8), 2), (24, 32, 48, 3, (8, 8, 8), 1), (144, 144, 48, 3, (4, 4, 4), 2),
-    (96, 96, 96, 3, (4, 6, 5), 1), (24, 32, 1, 1, (8, 8, 8), 2)])
+    (96, 96, 96, 3, (4, 6, 5), 1), (24, 32, 1, 1, (8, 8, 8), 2),
+    (48, 48, 96, 3, (32, 32, 32), 2)])  # 65536 positions: 32 weight-gradient chunks
 def test_conv_backward_matches_torch(cin, cin_pad, cout, k, grid, batch):
     """Input gradient (the forward kernel with transposed, mirrored weights)
     and weight gradient (lfts_conv3d_wgrad_bf16) against torch autograd on the
@@ -105,28 +106,32 @@ def test_conv_backward_matches_torch(cin, cin_pad, cout, k, grid, batch):
 
 
 def test_tcgen05_unet_gradients_match_torch_model():
+    """Gradients of the whole 24-channel network (32^3, batch 2: the weight
+    gradients reduce over many position chunks) against the FP32 torch model:
+    as close as torch's own BF16 autocast gets, parameter by parameter."""
     import torch
     import torch.nn.functional as F
     from langevinfts_b200.learned import TcgenUNetTrain, UNet3D
-    torch.manual_seed(5)
-    net = UNet3D(cin=2, cout=1, base=8).cuda()
-    torch.nn.init.normal_(net.out.weight, 0, 0.2)
-    x = torch.randn(2, 2, 16, 16, 16, device="cuda")
-    t = torch.randn(2, 1, 16, 16, 16, device="cuda")
-    F.mse_loss(TcgenUNetTrain(net)(x), t).backward()
-    got = {n: p.grad.clone() for n, p in net.named_parameters()}
-    net.zero_grad()
-    F.mse_loss(net(x), t).backward()
-    # BF16 activations against the FP32 model flip some ReLU masks, so each
-    # parameter's gradient agrees in direction only roughly; the layer-level
-    # tests above are the tight ones, this one checks the network's plumbing
-    # (channel maps of the padded concatenations, pooling, upsampling)
-    for n, p in net.named_parameters():
-        cos = float((got[n] * p.grad).sum() / (got[n].norm() * p.grad.norm() + 1e-30))
-        assert cos > 0.95, (n, cos, _rel(got[n], p.grad))
-    a = torch.cat([got[n].flatten() for n, _ in net.named_parameters()])
-    b = torch.cat([p.grad.flatten() for _, p in net.named_parameters()])
-    assert float((a * b).sum() / (a.norm() * b.norm())) > 0.99 and _rel(a, b) < 0.15
+    torch.manual_seed(0)
+    net = UNet3D(cin=2, cout=1, base=24).cuda()
+    torch.nn.init.normal_(net.out.weight, 0, 0.05)
+    x = torch.randn(2, 2, 32, 32, 32, device="cuda")
+    t = 0.1 * torch.randn(2, 1, 32, 32, 32, device="cuda")
+
+    def grads(fn):
+        net.zero_grad()
+        F.mse_loss(fn(x), t).backward()
+        return {n: p.grad.clone() for n, p in net.named_parameters()}
+
+    def autocast(z):
+        with torch.autocast("cuda", dtype=torch.bfloat16):
+            return net(z).float()
+
+    g32, gac, gtc = grads(net), grads(autocast), grads(TcgenUNetTrain(net))
+    for n in g32:
+        cos = float((gtc[n] * g32[n]).sum() / (gtc[n].norm() * g32[n].norm()))
+        assert cos > 0.98 and _rel(gtc[n], g32[n]) <= max(2 * _rel(gac[n], g32[n]), 0.03), (n, cos, _rel(gtc[n], g32[n]),
+                                                                                          _rel(gac[n], g32[n]))
 
 
 def test_training_on_the_tensor_cores_lowers_the_loss():
