@@ -185,6 +185,106 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_umma(const uint4 *__restrict_
 }
 
 // ------------------------------------------------------------------------
+// 3x3x3 convolution with the input of a tile staged once: the tile is 1 x 16
+// x 8 output positions (z, y, x) and its halo 3 x 18 x 10 positions sits in
+// shared memory as planes [kc][zh][yh][xh] of 16-byte units.  For tap (dz, dy,
+// dx) the A operand of the MMA is read in place: the 8 output positions of a
+// y row map to 8 consecutive halo rows (one core matrix), the 16 y rows are
+// HX units apart (SBO), the channel chunks a plane apart (LBO); only the
+// tap's weights are copied per tap.  Needs H % 16 == 0 and W % 8 == 0.
+constexpr int HT_Y = 16, HT_X = 8, HZ = 3, HY = HT_Y + 2, HX = HT_X + 2, HPLANE = HZ * HY * HX;
+
+__global__ void __launch_bounds__(CONV_M) k_conv3d_halo_umma(const uint4 *__restrict__ in, const uint4 *__restrict__ wpk,
+                                                             const float *__restrict__ bias, uint16_t *__restrict__ out,
+                                                             int B, int D, int H, int W, int cin, int cout, int relu,
+                                                             uint32_t tmem_cols) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int kc_n = cin / 8, b_units = kc_n * cout;
+    uint4 *halo = (uint4 *)smem_raw;                 // kc_n * HPLANE units
+    uint4 *wst = halo + kc_n * HPLANE;               // two weight stages
+    uint64_t *bar = (uint64_t *)(wst + 2 * b_units);
+    uint32_t *tmem_slot = (uint32_t *)(bar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int x0 = blockIdx.x * HT_X, y0 = blockIdx.y * HT_Y, z = blockIdx.z % D, n = blockIdx.z / D;
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    // the halo, periodic
+    for (int i = tid; i < kc_n * HPLANE; i += CONV_M) {
+        const int kc = i / HPLANE, r = i - kc * HPLANE;
+        const int zh = r / (HY * HX), yh = (r / HX) % HY, xh = r % HX;
+        const int zz = (z + zh - 1 + D) % D, yy = (y0 + yh - 1 + H) % H, xx = (x0 + xh - 1 + W) % W;
+        halo[i] = in[((((long long)n * D + zz) * H + yy) * W + xx) * kc_n + kc];
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(cout >> 3) << 17) | ((uint32_t)(CONV_M >> 4) << 24);
+    const uint32_t halo0 = smem_addr(halo);
+    bool ok = true;
+    for (int t = 0; t < 27; t++) {
+        const int st = t & 1;
+        if (t >= 2 && !__syncthreads_and(mbar_wait(bar + st, ((t >> 1) - 1) & 1))) {
+            ok = false;
+            break;
+        }
+        uint4 *sb = wst + st * b_units;
+        const uint4 *src = wpk + (long long)t * b_units;
+        for (int i = tid; i < b_units; i += CONV_M) sb[i] = src[i];
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;  // halo offsets of the tap (0..2)
+            const uint32_t a_tap = halo0 + (uint32_t)(((dz * HY + dy) * HX + dx) * 16);
+            const uint32_t b0 = smem_addr(sb);
+            for (int s = 0; s < kc_n / 2; s++) {
+                const uint64_t da = umma_desc(a_tap + (uint32_t)(2 * s * HPLANE * 16), HPLANE * 16, HX * 16);
+                const uint64_t db = umma_desc(b0 + (uint32_t)(2 * s * cout * 16), (uint32_t)cout * 16, 128);
+                umma_bf16(tmem, da, db, idesc, (t > 0 || s > 0) ? 1u : 0u);
+            }
+            umma_commit(bar + st);
+        }
+    }
+    {
+        const bool fin = ok ? mbar_wait(bar + (26 & 1), (26 >> 1) & 1) : false;
+        ok = __syncthreads_and(fin);
+    }
+    if (!ok) {
+        mbar_wait(bar + (26 & 1), (26 >> 1) & 1);
+    } else {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int m = tid;  // accumulator row = 8 j + l: position (y0 + j, x0 + l)
+        const long long p = (((long long)n * D + z) * H + (y0 + m / 8)) * W + (x0 + m % 8);
+        for (int c0 = 0; c0 < cout; c0 += 16) {
+            uint32_t v[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+            uint16_t h[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                float f = __uint_as_float(v[i]) + bias[c0 + i];
+                if (relu && f < 0.f) f = 0.f;
+                h[i] = to_bf16(f);
+            }
+            uint4 *o = (uint4 *)(out + p * cout + c0);
+            o[0] = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
+            o[1] = make_uint4(h[8] | (h[9] << 16), h[10] | (h[11] << 16), h[12] | (h[13] << 16), h[14] | (h[15] << 16));
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+}
+
+// ------------------------------------------------------------------------
 // Weight gradient of the periodic convolution:
 //   dw[tap][co][ci] += sum_p gy[p][co] x[p + tap][ci]
 // per tap a GEMM with M = co (padded to 128 rows), N = cin, K = positions.
@@ -364,6 +464,26 @@ extern "C" int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, c
     if (blocks > 0x7fffffffLL) return fail("conv3d: too many positions");
     uint32_t cols = 32;
     while ((int)cols < cout) cols <<= 1;
+    {
+        // halo-staged kernel: 3x3x3, H % 16 == 0, W % 8 == 0, halo + weight stages within 200 KB
+        using namespace lfts::unet;
+        const size_t hsmem = (size_t)16 * ((size_t)(cin / 8) * HPLANE + 2 * (size_t)(cin / 8) * cout) + 2 * sizeof(uint64_t) + 16;
+        if (taps == 27 && H % HT_Y == 0 && W % HT_X == 0 && hsmem <= 200 * 1024 && (long long)B * D <= 65535 &&
+            !std::getenv("LFTS_CONV_NO_HALO")) {
+            static bool hattr = false;
+            if (!hattr) {
+                cudaError_t e = cudaFuncSetAttribute(k_conv3d_halo_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+                if (e != cudaSuccess) return fail(std::string("conv3d: ") + cudaGetErrorString(e));
+                hattr = true;
+            }
+            k_conv3d_halo_umma<<<dim3((unsigned)(W / HT_X), (unsigned)(H / HT_Y), (unsigned)(B * D)), CONV_M, hsmem,
+                                 (cudaStream_t)stream>>>((const uint4 *)in, (const uint4 *)wpk, bias, (uint16_t *)out, B, D, H,
+                                                         W, cin, cout, relu, cols);
+            cudaError_t e = cudaPeekAtLastError();
+            if (e != cudaSuccess) return fail(std::string("conv3d launch: ") + cudaGetErrorString(e));
+            return 0;
+        }
+    }
     const size_t smem = (size_t)2 * 16 * ((size_t)(cin / 8) * (lfts::unet::CONV_M + cout)) + 2 * sizeof(uint64_t) + 16;
     if (smem > 200 * 1024) return fail("conv3d: cin x (128 + cout) too large for the shared-memory stages");
     static bool attr_set = false;

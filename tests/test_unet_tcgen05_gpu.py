@@ -28,6 +28,9 @@ def _reference(x, conv, relu):
     (144, 144, 48, 3, (8, 8, 8), 1),   # decoder concat, largest K
     (96, 96, 96, 3, (4, 6, 5), 1),     # non-cubic box, 120 positions: one partial tile
     (24, 32, 1, 1, (8, 8, 8), 2),      # 1x1x1 output layer
+    # grids with H % 16 == 0 and W % 8 == 0 take the halo-staged kernel
+    (2, 16, 24, 3, (16, 16, 16), 2), (24, 32, 48, 3, (16, 16, 16), 1), (144, 144, 48, 3, (8, 16, 8), 2),
+    (96, 96, 96, 3, (6, 32, 24), 1),
 ])
 @pytest.mark.parametrize("relu", [True, False])
 def test_conv_matches_torch(cin, cin_pad, cout, k, grid, batch, relu):
@@ -74,7 +77,8 @@ def _rel(a, b):
 @pytest.mark.parametrize("cin,cin_pad,cout,k,grid,batch", [
     (2, 16, 24, 3, (8, 8, 8), 2), (24, 32, 48, 3, (8, 8, 8), 1), (144, 144, 48, 3, (4, 4, 4), 2),
     (96, 96, 96, 3, (4, 6, 5), 1), (24, 32, 1, 1, (8, 8, 8), 2),
-    (48, 48, 96, 3, (32, 32, 32), 2)])  # 65536 positions: 32 weight-gradient chunks
+    (48, 48, 96, 3, (32, 32, 32), 2),  # 65536 positions: 32 weight-gradient chunks (input gradient: halo kernel)
+    (24, 32, 24, 3, (16, 16, 16), 2)])
 def test_conv_backward_matches_torch(cin, cin_pad, cout, k, grid, batch):
     """Input gradient (the forward kernel with transposed, mirrored weights)
     and weight gradient (lfts_conv3d_wgrad_bf16) against torch autograd on the
