@@ -58,6 +58,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// 16-byte global -> shared copy that does not wait for the data (cp.async,
+// completed by cp_async_wait_all), so a thread keeps many loads in flight
+__device__ __forceinline__ void cp_async16(void *dst_smem, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst_smem)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 __device__ __forceinline__ uint16_t to_bf16(float f) {
     // round to nearest even (finite values; NaN stays NaN)
     uint32_t u = __float_as_uint(f);
@@ -194,21 +203,28 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_umma(const uint4 *__restrict_
 // tap's weights are copied per tap.  Needs H % 16 == 0 and W % 8 == 0.
 constexpr int HT_Y = 16, HT_X = 8, HZ = 3, HY = HT_Y + 2, HX = HT_X + 2, HPLANE = HZ * HY * HX;
 
+// Warp roles after the halo is staged: warps 1-3 copy the tap weights into a
+// ring of NS stages (full[st]: 96 producer arrivals), lane 0 of warp 0 issues
+// each tap's MMAs once its stage is full and commits them to empty[st], which
+// frees the stage; a last commit to bar_done releases the epilogue.
 __global__ void __launch_bounds__(CONV_M) k_conv3d_halo_umma(const uint4 *__restrict__ in, const uint4 *__restrict__ wpk,
                                                              const float *__restrict__ bias, uint16_t *__restrict__ out,
                                                              int B, int D, int H, int W, int cin, int cout, int relu,
-                                                             uint32_t tmem_cols) {
+                                                             uint32_t tmem_cols, int NS) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int kc_n = cin / 8, b_units = kc_n * cout;
     uint4 *halo = (uint4 *)smem_raw;                 // kc_n * HPLANE units
-    uint4 *wst = halo + kc_n * HPLANE;               // two weight stages
-    uint64_t *bar = (uint64_t *)(wst + 2 * b_units);
-    uint32_t *tmem_slot = (uint32_t *)(bar + 2);
+    uint4 *wst = halo + kc_n * HPLANE;               // NS weight stages
+    uint64_t *full = (uint64_t *)(wst + (size_t)NS * b_units), *empty = full + NS, *done = empty + NS;
+    uint32_t *tmem_slot = (uint32_t *)(done + 1);
     const int tid = threadIdx.x, warp = tid >> 5;
     const int x0 = blockIdx.x * HT_X, y0 = blockIdx.y * HT_Y, z = blockIdx.z % D, n = blockIdx.z / D;
     if (tid == 0) {
-        mbar_init(bar, 1);
-        mbar_init(bar + 1, 1);
+        for (int i = 0; i < NS; i++) {
+            mbar_init(full + i, CONV_M - 32);
+            mbar_init(empty + i, 1);
+        }
+        mbar_init(done, 1);
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
@@ -220,46 +236,60 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_halo_umma(const uint4 *__rest
         const int kc = i / HPLANE, r = i - kc * HPLANE;
         const int zh = r / (HY * HX), yh = (r / HX) % HY, xh = r % HX;
         const int zz = (z + zh - 1 + D) % D, yy = (y0 + yh - 1 + H) % H, xx = (x0 + xh - 1 + W) % W;
-        halo[i] = in[((((long long)n * D + zz) * H + yy) * W + xx) * kc_n + kc];
+        cp_async16(halo + i, in + ((((long long)n * D + zz) * H + yy) * W + xx) * kc_n + kc);
     }
+    cp_async_wait_all();
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
-    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(cout >> 3) << 17) | ((uint32_t)(CONV_M >> 4) << 24);
-    const uint32_t halo0 = smem_addr(halo);
     bool ok = true;
-    for (int t = 0; t < 27; t++) {
-        const int st = t & 1;
-        if (t >= 2 && !__syncthreads_and(mbar_wait(bar + st, ((t >> 1) - 1) & 1))) {
-            ok = false;
-            break;
+    if (warp > 0) {
+        // producers: tap t into stage t % NS once the MMAs of tap t - NS freed it
+        const int pt = tid - 32;
+        for (int t = 0; t < 27 && ok; t++) {
+            const int st = t % NS, u = t / NS;
+            if (u > 0 && !mbar_wait(empty + st, (u - 1) & 1)) {
+                ok = false;
+                break;
+            }
+            uint4 *sb = wst + (size_t)st * b_units;
+            const uint4 *src = wpk + (long long)t * b_units;
+            for (int i = pt; i < b_units; i += CONV_M - 32) cp_async16(sb + i, src + i);
+            cp_async_wait_all();
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(full + st)) : "memory");
         }
-        uint4 *sb = wst + st * b_units;
-        const uint4 *src = wpk + (long long)t * b_units;
-        for (int i = tid; i < b_units; i += CONV_M) sb[i] = src[i];
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+    } else if (tid == 0) {
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(cout >> 3) << 17) | ((uint32_t)(CONV_M >> 4) << 24);
+        const uint32_t halo0 = smem_addr(halo);
+        for (int t = 0; t < 27; t++) {
+            const int st = t % NS, u = t / NS;
+            if (!mbar_wait(full + st, u & 1)) {
+                ok = false;
+                break;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;  // halo offsets of the tap (0..2)
             const uint32_t a_tap = halo0 + (uint32_t)(((dz * HY + dy) * HX + dx) * 16);
-            const uint32_t b0 = smem_addr(sb);
+            const uint32_t b0 = smem_addr(wst + (size_t)st * b_units);
             for (int s = 0; s < kc_n / 2; s++) {
                 const uint64_t da = umma_desc(a_tap + (uint32_t)(2 * s * HPLANE * 16), HPLANE * 16, HX * 16);
                 const uint64_t db = umma_desc(b0 + (uint32_t)(2 * s * cout * 16), (uint32_t)cout * 16, 128);
                 umma_bf16(tmem, da, db, idesc, (t > 0 || s > 0) ? 1u : 0u);
             }
-            umma_commit(bar + st);
+            umma_commit(empty + st);
         }
+        if (ok) umma_commit(done);
     }
     {
-        const bool fin = ok ? mbar_wait(bar + (26 & 1), (26 >> 1) & 1) : false;
+        // every thread: the accumulator is complete (or some wait gave up)
+        const bool fin = __syncthreads_and(ok) ? mbar_wait(done, 0) : false;
         ok = __syncthreads_and(fin);
     }
     if (!ok) {
-        mbar_wait(bar + (26 & 1), (26 >> 1) & 1);
+        mbar_wait(done, 0);  // a second bounded wait for MMAs still in flight
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int m = tid;  // accumulator row = 8 j + l: position (y0 + j, x0 + l)
@@ -467,7 +497,13 @@ extern "C" int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, c
     {
         // halo-staged kernel: 3x3x3, H % 16 == 0, W % 8 == 0, halo + weight stages within 200 KB
         using namespace lfts::unet;
-        const size_t hsmem = (size_t)16 * ((size_t)(cin / 8) * HPLANE + 2 * (size_t)(cin / 8) * cout) + 2 * sizeof(uint64_t) + 16;
+        // weight stages: as many (2..4) as fit beside the halo in 200 KB
+        auto hs = [&](int ns) {
+            return (size_t)16 * ((size_t)(cin / 8) * HPLANE + (size_t)ns * (cin / 8) * cout) + (2 * (size_t)ns + 1) * sizeof(uint64_t) + 16;
+        };
+        int NS = 4;
+        while (NS > 2 && hs(NS) > 200 * 1024) NS--;
+        const size_t hsmem = hs(NS);
         if (taps == 27 && H % HT_Y == 0 && W % HT_X == 0 && hsmem <= 200 * 1024 && (long long)B * D <= 65535 &&
             !std::getenv("LFTS_CONV_NO_HALO")) {
             static bool hattr = false;
@@ -478,7 +514,7 @@ extern "C" int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, c
             }
             k_conv3d_halo_umma<<<dim3((unsigned)(W / HT_X), (unsigned)(H / HT_Y), (unsigned)(B * D)), CONV_M, hsmem,
                                  (cudaStream_t)stream>>>((const uint4 *)in, (const uint4 *)wpk, bias, (uint16_t *)out, B, D, H,
-                                                         W, cin, cout, relu, cols);
+                                                         W, cin, cout, relu, cols, NS);
             cudaError_t e = cudaPeekAtLastError();
             if (e != cudaSuccess) return fail(std::string("conv3d launch: ") + cudaGetErrorString(e));
             return 0;
