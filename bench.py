@@ -489,11 +489,38 @@ def run_conv(args):
             ev[1].record()
             ev[1].synchronize()
             res.append(ev[0].elapsed_time(ev[1]) * 1e3 / args.steps)
+        # forward + backward (input and weight gradients) of the layer
+        from langevinfts_b200.learned import _ConvFn
+        xg = x.detach().clone().requires_grad_(True)
+        xrg = xr.detach().clone().requires_grad_(True)
+        gy = torch.randn(B, n, n, n, layer[2], device="cuda").to(torch.bfloat16)
+        gyr = gy[..., :co].permute(0, 4, 1, 2, 3).contiguous(memory_format=torch.channels_last_3d)
+        convb.weight.requires_grad_(True)
+
+        def ours_b():
+            _ConvFn.apply(xg, conv.weight, conv.bias, list(range(ci)), cip, True).backward(gy)
+
+        def ref_b():
+            F.relu(convb(F.pad(xrg, (k // 2,) * 6, mode="circular") if k > 1 else xrg)).backward(gyr)
+
+        for fn in (ours_b, ref_b):
+            for _ in range(2):
+                fn()
+            torch.cuda.synchronize()
+            ev[0].record()
+            for _ in range(args.steps):
+                fn()
+            ev[1].record()
+            ev[1].synchronize()
+            res.append(ev[0].elapsed_time(ev[1]) * 1e3 / args.steps)
         tot_us, tot_us_ref, tot_flop = tot_us + res[0], tot_us_ref + res[1], tot_flop + flop
         rows.append({"layer": name, "grid": n, "cin": ci, "cout": co, "k": k, "tcgen05_us": res[0], "cudnn_us": res[1],
-                     "tcgen05_tflops": flop / res[0] / 1e6, "cudnn_tflops": flop / res[1] / 1e6})
+                     "tcgen05_tflops": flop / res[0] / 1e6, "cudnn_tflops": flop / res[1] / 1e6,
+                     "fwd_bwd_tcgen05_us": res[2], "fwd_bwd_cudnn_us": res[3]})
     print(json.dumps({"metric": "U-Net convolution time per forward (batch 8)", "grid": [N] * 3, "layers": rows,
                       "total_tcgen05_us": tot_us, "total_cudnn_us": tot_us_ref,
+                      "total_fwd_bwd_tcgen05_us": sum(r["fwd_bwd_tcgen05_us"] for r in rows),
+                      "total_fwd_bwd_cudnn_us": sum(r["fwd_bwd_cudnn_us"] for r in rows),
                       "tcgen05_tflops": tot_flop / tot_us / 1e6, "peak_bf16_tflops": peak,
                       "frac_of_peak": tot_flop / tot_us / 1e6 / peak,
                       "note": "FLOPs on the real channels; cuDNN timing includes its circular pad"}))

@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_umma(const uint4 *__restrict_
                 }
                 const int zz = (z + dz + D) % D, yy = (y + dy + H) % H, xx = (x + dx + W) % W;
                 const uint4 *src = in + ((((long long)n * D + zz) * H + yy) * W + xx) * kc_n;
-                for (int kc = 0; kc < kc_n; kc++) dst[kc * CONV_M] = src[kc];
+                for (int kc = 0; kc < kc_n; kc++) cp_async16(dst + kc * CONV_M, src + kc);
             } else {
                 for (int kc = 0; kc < kc_n; kc++) dst[kc * CONV_M] = make_uint4(0, 0, 0, 0);
             }
@@ -146,8 +146,9 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_umma(const uint4 *__restrict_
         // B: the tap's packed weights
         {
             const uint4 *src = wpk + (long long)t * b_units;
-            for (int i = tid; i < b_units; i += CONV_M) sb[i] = src[i];
+            for (int i = tid; i < b_units; i += CONV_M) cp_async16(sb + i, src + i);
         }
+        cp_async_wait_all();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
@@ -383,8 +384,10 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_wgrad_umma(const uint4 *__res
             z = (int)(q % D);
             n = (int)(q / D);
         }
-        for (int c = half; c < gc; c += 2)
-            sa[c * WG_K + k] = valid ? gy[p * gc + c] : make_uint4(0, 0, 0, 0);
+        for (int c = half; c < gc; c += 2) {
+            if (valid) cp_async16(sa + c * WG_K + k, gy + p * gc + c);
+            else sa[c * WG_K + k] = make_uint4(0, 0, 0, 0);
+        }
         for (int j = 0; j < ntap; j++) {
             uint4 *dst = sb + j * b_units + k;
             if (valid) {
@@ -396,11 +399,12 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_wgrad_umma(const uint4 *__res
                 }
                 const int zz = (z + dz + D) % D, yy = (y + dy + H) % H, x2 = (xx + dx + W) % W;
                 const uint4 *src = x + ((((long long)n * D + zz) * H + yy) * W + x2) * xc;
-                for (int c = half; c < xc; c += 2) dst[c * WG_K] = src[c];
+                for (int c = half; c < xc; c += 2) cp_async16(dst + c * WG_K, src + c);
             } else {
                 for (int c = half; c < xc; c += 2) dst[c * WG_K] = make_uint4(0, 0, 0, 0);
             }
         }
+        cp_async_wait_all();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
