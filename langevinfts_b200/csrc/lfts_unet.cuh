@@ -469,11 +469,9 @@ extern "C" int lfts_conv3d_wgrad_bf16(void *stream, const void *x, const void *g
     const size_t smem = 2 * 16 * st_units + 2 * sizeof(uint64_t) + 16;
     if (smem > 200 * 1024) return fail("conv3d wgrad: cin too large for the shared-memory stages");
     if (cout > 128) return fail("conv3d wgrad: cout (the accumulator rows) must be <= 128");
-    static bool attr_set = false;
-    if (!attr_set) {
+    {
         cudaError_t e = cudaFuncSetAttribute(lfts::unet::k_conv3d_wgrad_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return fail(std::string("conv3d wgrad: ") + cudaGetErrorString(e));
-        attr_set = true;
     }
     lfts::unet::k_conv3d_wgrad_umma<<<dim3((unsigned)chunks, taps == 27 ? 9 : 1), lfts::unet::CONV_M, smem,
                                       (cudaStream_t)stream>>>((const uint4 *)x, (const uint4 *)gy, dw, B, D, H, W, cin, cout,
@@ -508,29 +506,23 @@ extern "C" int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, c
         int NS = 4;
         while (NS > 2 && hs(NS) > 200 * 1024) NS--;
         const size_t hsmem = hs(NS);
-        if (taps == 27 && H % HT_Y == 0 && W % HT_X == 0 && hsmem <= 200 * 1024 && (long long)B * D <= 65535 &&
-            !std::getenv("LFTS_CONV_NO_HALO")) {
-            static bool hattr = false;
-            if (!hattr) {
-                cudaError_t e = cudaFuncSetAttribute(k_conv3d_halo_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-                if (e != cudaSuccess) return fail(std::string("conv3d: ") + cudaGetErrorString(e));
-                hattr = true;
-            }
+        if (taps == 27 && H % HT_Y == 0 && W % HT_X == 0 && hsmem <= 200 * 1024 && (long long)B * D <= 65535) {
+            // per device (the attribute belongs to the current device), so set on every call
+            cudaError_t e = cudaFuncSetAttribute(k_conv3d_halo_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            if (e != cudaSuccess) return fail(std::string("conv3d: ") + cudaGetErrorString(e));
             k_conv3d_halo_umma<<<dim3((unsigned)(W / HT_X), (unsigned)(H / HT_Y), (unsigned)(B * D)), CONV_M, hsmem,
                                  (cudaStream_t)stream>>>((const uint4 *)in, (const uint4 *)wpk, bias, (uint16_t *)out, B, D, H,
                                                          W, cin, cout, relu, cols, NS);
-            cudaError_t e = cudaPeekAtLastError();
+            e = cudaPeekAtLastError();
             if (e != cudaSuccess) return fail(std::string("conv3d launch: ") + cudaGetErrorString(e));
             return 0;
         }
     }
     const size_t smem = (size_t)2 * 16 * ((size_t)(cin / 8) * (lfts::unet::CONV_M + cout)) + 2 * sizeof(uint64_t) + 16;
     if (smem > 200 * 1024) return fail("conv3d: cin x (128 + cout) too large for the shared-memory stages");
-    static bool attr_set = false;
-    if (!attr_set) {
+    {
         cudaError_t e = cudaFuncSetAttribute(lfts::unet::k_conv3d_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return fail(std::string("conv3d: ") + cudaGetErrorString(e));
-        attr_set = true;
     }
     lfts::unet::k_conv3d_umma<<<(unsigned)blocks, lfts::unet::CONV_M, smem, (cudaStream_t)stream>>>(
         (const uint4 *)in, (const uint4 *)wpk, bias, (uint16_t *)out, B, D, H, W, cin, cout, taps, relu, cols);
