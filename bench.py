@@ -393,7 +393,7 @@ def run_learned(args):
     R = args.replicas
     p = workload_params(args.workload, args.nx)
     seeds = replica_seeds(0, R, base=WORKLOADS[args.workload]["seed"])
-    sim = BatchedLFTS(p, seeds, module=L)
+    sim = BatchedLFTS(p, seeds, module=L, platform="cuda" if args.precision == "fp64" else "cuda-fp32")
     sim.engine.autotune()
     sim.start([initial_fields(s, sim.M) for s in seeds])
     for _ in range(args.warmup):
@@ -428,7 +428,7 @@ def run_learned(args):
 
     plain, learned, learned_tc = run(None), run(start), run(start_tc)
     print(json.dumps({"metric": "mean saddle-point iterations per Langevin step (learned start ablation)",
-                      "workload": args.workload, "grid": [args.nx] * 3, "replicas": R,
+                      "workload": args.workload, "grid": [args.nx] * 3, "replicas": R, "precision": args.precision,
                       "plain": {"mean_iterations": plain[0], "replica_steps_per_s": plain[1], "failed": plain[2]},
                       "learned": {"mean_iterations": learned[0], "replica_steps_per_s": learned[1], "failed": learned[2]},
                       "learned_tcgen05": {"mean_iterations": learned_tc[0], "replica_steps_per_s": learned_tc[1],
