@@ -15,17 +15,25 @@ start can only change how many iterations a step needs, not where it ends.
 Pieces:
   UNet3D            3 levels (N, N/2, N/4), 24 base channels, 3^3 kernels with
                     circular padding (the box is periodic), ReLU, average
-                    pooling down, nearest upsampling, skip concatenation; runs
-                    in BF16 with FP32 accumulation (torch autocast over cuDNN).
+                    pooling down, nearest upsampling, skip concatenation; the
+                    parameter holder, and the torch form (BF16 autocast).
+  TcgenUNet         inference with every convolution on this library's
+                    tensor-core kernel (lfts_conv3d_bf16: tcgen05 implicit
+                    GEMM, BF16 operands, FP32 accumulation in tensor memory).
+  TcgenUNetTrain    training form: forward and backward of every convolution
+                    on the tensor cores (_ConvFn: input gradient by the forward
+                    kernel with mirrored taps, weight gradient by
+                    lfts_conv3d_wgrad_bf16).
   generate_pairs    training pairs from the plain solver: inputs (w_-, w_+prev)
                     and target w_+ of every replica and step.
-  train             AdamW on the mean-squared error of the residual.
+  train             AdamW on the mean-squared error of the residual, over
+                    torch's convolutions or (tcgen05=True) the tensor-core ones.
   LearnedStart      the callable BatchedLFTS.step(start=...) uses: reads w_aux
                     on the device (zero copy), writes the predicted w_+ in place
                     on the engine's stream.
 
-The convolutions are torch's (cuDNN); the step kernels of the solver are this
-library's.  Grids must have extents divisible by 4.
+Pooling, upsampling, concatenation and AdamW are torch's.  Grids must have
+extents divisible by 4.
 """
 import time
 
