@@ -37,19 +37,13 @@ sys.path.insert(0, ROOT)
 METRIC = "Langevin steps/s @ saddle err 1e-4 (batched L-FTS, plain FP64)"
 METRIC_FP32 = "Langevin steps/s @ saddle err 1e-4 (batched L-FTS, FP32 propagators, FP64 reductions)"
 UNIT = "replica-steps/s"
-# mean saddle-point iterations per Langevin step of this workload, measured by
-# the GPU arm on B200 (the algorithm and inputs are the reference's, so the
-# reference arm uses it to convert its timed saddle iterations into steps/s)
-ITERS_PER_STEP = 44.0
 
 
 # The batched L-FTS workloads: config4 is the headline (64^3, 64 replicas);
 # config5 is the system of the learned-start study run with the plain solver.
 WORKLOADS = {
-    "config4": {"nx": 64, "lx": 7.3, "f": 0.5, "chin": 17.0, "nbar": 100, "replicas": 64, "seed": 1000,
-                "iters_per_step": ITERS_PER_STEP},
-    "config5": {"nx": 96, "lx": 8.0, "f": 0.4, "chin": 18.0, "nbar": 200, "replicas": 16, "seed": 2000,
-                "iters_per_step": 54.3},  # measured by the GPU arm on this workload
+    "config4": {"nx": 64, "lx": 7.3, "f": 0.5, "chin": 17.0, "nbar": 100, "replicas": 64, "seed": 1000},
+    "config5": {"nx": 96, "lx": 8.0, "f": 0.4, "chin": 18.0, "nbar": 200, "replicas": 16, "seed": 2000},
 }
 
 
@@ -189,33 +183,74 @@ def _reference_sample_child(n_iter, threads, workload="config4"):
     return 0
 
 
+def _reference_steps_child(k_max, budget_s, workload="config4"):
+    """The reference CPU platform through the driver: the initial saddle-point
+    search of one replica (untimed, its warm-up), then Langevin steps until
+    k_max are done or the next one would pass budget_s of timed work (at
+    least one).  Prints [seconds per step, saddle iterations per step, steps,
+    initial iterations, failed steps, threads]."""
+    ref = load_reference()
+    if ref is None:
+        return 1
+    from langevinfts_b200.lfts import LFTS
+    p = workload_params(workload)
+    seed = WORKLOADS[workload]["seed"]
+    sim = LFTS(p, random_seed=seed, module=ref, platform="cpu-mkl")
+    it0, _ = sim.start(initial_fields(seed, sim.M))
+    ts, its, fails = [], [], 0
+    while len(ts) < max(k_max, 1):
+        if ts and sum(ts) + ts[-1] > budget_s:
+            break
+        t0 = time.perf_counter()
+        it, _, _, failed = sim.step()
+        ts.append(time.perf_counter() - t0)
+        its.append(it)
+        fails += int(failed)
+    print(json.dumps([float(np.mean(ts)), float(np.mean(its)), len(ts), int(it0), fails,
+                      int(os.environ.get("OMP_NUM_THREADS", "1"))]))
+    return 0
+
+
+REFERENCE_STEP_BUDGET_S = 150.0
+
+
 def run_reference(args):
-    """--impl reference: the reference's CPU implementation on this host."""
+    """--impl reference: the reference's CPU implementation on this host, one
+    replica at a time, real Langevin steps (each with its own saddle-point
+    search) after the initial search; its own iteration counts."""
+    import resource
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    ref = load_reference()
-    if ref is None:
+    if load_reference() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) is missing"}))
         return 0
-    r = reference_sample(args.steps, threads, workload=args.workload)
-    if r is None:
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_STACKSIZE="1G")
+    t_run = time.perf_counter()
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-steps", str(args.steps), "--ref-budget",
+                        str(REFERENCE_STEP_BUDGET_S), "--workload", args.workload], env=env, capture_output=True, text=True,
+                       timeout=3000, preexec_fn=lambda: resource.setrlimit(
+                           resource.RLIMIT_STACK, (resource.RLIM_INFINITY, resource.RLIM_INFINITY)))
+    t_run = time.perf_counter() - t_run
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout[-2000:] + r.stderr[-2000:])
         print(json.dumps({"impl": "reference", "unavailable": "the reference CPU platform failed on this host (see stderr)"}))
         return 0
-    t_iter = r[0]
-    ips = WORKLOADS[args.workload]["iters_per_step"]
-    v = 1.0 / (t_iter * ips)
-    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+    t_step, ips, n, it0, fails, thr = json.loads(r.stdout.strip().splitlines()[-1])
+    v = 1.0 / t_step
+    sample = (f"initial saddle-point search of 1 replica ({it0} iterations, untimed), then {n} timed Langevin step(s) "
+              f"of that replica ({ips:.1f} saddle iterations per step, its own count; {fails} failed), {args.nx}^3, N=90; "
+              f"reference CPU platform (project FFT in place of MKL), {thr} OpenMP threads; steps stop after "
+              f"{REFERENCE_STEP_BUDGET_S:.0f} s of timed work")
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": n,
+           "steps_requested": args.steps, "warmup": 0, "ms_per_step": 1000.0 * t_step, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": dict(workload_config(args.replicas, args.nx, args.workload), parallelism="reference CPU platform, OpenMP threads",
-                          reference_sample="one replica at a time; replica-steps/s = 1 / (seconds per saddle iteration "
-                                           "x saddle iterations per Langevin step)"),
-           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                            "sample": f"{args.steps} timed saddle-point iterations (after 1 untimed) of 1 replica, {args.nx}^3, N=90, "
-                                      f"x {ips} iterations per Langevin step; reference CPU platform, project FFT "
-                                      "in place of MKL"},
+                          reference_sample="one replica; replica-steps/s = 1 / (seconds per Langevin step)",
+                          mean_saddle_iterations=ips, initial_saddle_iterations=it0, failed_steps=fails,
+                          run_seconds=t_run),
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": thr, "kind": "reference", "sample": sample},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
@@ -703,7 +738,7 @@ def run_ours(args):
         r = reference_sample(1, threads, workload=args.workload)
         sys.stderr.write(f"[bench] reference CPU sample: {r}\n")
         if r is not None:
-            mean_iters = float(np.mean(iters)) if iters else ITERS_PER_STEP
+            mean_iters = float(np.mean(iters))
             cpu = {"value": 1.0 / (r[0] * mean_iters), "unit": UNIT, "cores": r[1], "kind": "reference",
                    "sample": f"2 saddle-point iterations of 1 replica ({args.nx}^3, N=90) on the reference CPU platform "
                              f"(first discarded), {r[0]:.2f} s/iteration x {mean_iters:.1f} iterations per step measured above"}
@@ -744,6 +779,8 @@ def main():
                     help="fp64 (the headline) or fp32 propagators with FP64 reductions (platform cuda-fp32)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--ref-steps", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--ref-budget", type=float, default=REFERENCE_STEP_BUDGET_S, help=argparse.SUPPRESS)
     ap.add_argument("--ref-statistics", default="", help=argparse.SUPPRESS)
     ap.add_argument("--ref-scft", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--scft", action="store_true", help="SCFT of the 64^3 asymmetric diblock (device loop, FP64 and FP32)")
@@ -764,6 +801,8 @@ def main():
         args.nx = WORKLOADS[args.workload]["nx"]
     if args.ref_sample:
         return _reference_sample_child(args.ref_sample, args.threads, args.workload)
+    if args.ref_steps:
+        return _reference_steps_child(args.ref_steps, args.ref_budget, args.workload)
     if args.ref_statistics:
         return _reference_statistics_child(args.ref_statistics, args.threads)
     if args.ref_scft:

@@ -74,6 +74,16 @@ int lfts_graph_begin(lfts_ctx ctx);
 int lfts_graph_end(lfts_ctx ctx, lfts_graph *out);
 int lfts_graph_launch(lfts_ctx ctx, lfts_graph g);
 int lfts_graph_destroy(lfts_graph g);
+/* A device-controlled loop inside a capture (no counterpart in the reference,
+ * whose saddle loop runs on the host): between lfts_graph_begin and
+ * lfts_graph_end, lfts_graph_while_begin appends a conditional WHILE node after
+ * the work captured so far and sends the context stream's work into the node's
+ * body until lfts_graph_while_end; work captured afterwards follows the loop.
+ * The body repeats while the condition *handle is non-zero.  The condition is 1
+ * when each graph launch reaches the node (the body runs at least once), and
+ * device code in the body sets it (lfts_saddle_next).  Loops do not nest. */
+int lfts_graph_while_begin(lfts_ctx ctx, unsigned long long *handle);
+int lfts_graph_while_end(lfts_ctx ctx);
 
 /* ---- tables ------------------------------------------------------------ */
 
@@ -131,6 +141,10 @@ int lfts_step_continuous(lfts_ctx ctx, const lfts_step_job *jobs, int njobs, int
  * allocates and frees its own buffers, synchronises, and must not run inside a
  * graph capture.  report (may be NULL) receives the timings and the choice. */
 int lfts_autotune(lfts_ctx ctx, int njobs, int reps, char *report, size_t report_cap);
+/* Name of the context's current step implementation ("register-64",
+ * "register-64 xcap2", "register-96", "cubic", "generic"): the default chosen
+ * at creation, or lfts_autotune's choice.  No counterpart in the reference. */
+int lfts_step_impl(lfts_ctx ctx, char *name, size_t cap);
 /* Discrete chain: out = [fac *] F^-1[ b * F[in] ] with b = bond (half=0) or
  * bond_half (half=1), multiplied by fac when with_fac=1.  (half=0, with_fac=1)
  * replaces advance_propagator_discrete (CudaSolverPseudo.cu:413-450);
@@ -302,9 +316,34 @@ int lfts_am_batch_update(lfts_ctx ctx, int R, long long n, int L, const int *hea
 typedef struct {
     int *active, *n_anderson, *head_raw, *iter, *head, *flag, *ndots, *mode, *nh, *any_active;
     double *err, *err_old, *mix;
+    int *loop_iter;  /* device iteration counter of a graph loop; read when it <= 0 (may be NULL otherwise) */
 } lfts_saddle_state;
 int lfts_saddle_control(lfts_ctx ctx, int R, int I, int it, const double *var, const double *scale, double tolerance,
                         double am_start_error, int am_max_hist, double am_mix_min, const lfts_saddle_state *st);
+/* The saddle-point loop of one Langevin step as device work (for one graph per
+ * step; no counterpart in the reference, whose loop runs on the host):
+ * lfts_saddle_begin resets every replica to the start of a search (active,
+ * no Anderson history, err = err_old = 1e20, iter = 0, mix = mix_init) and
+ * sets *st->loop_iter = 1.  lfts_saddle_next, the last work of the loop body,
+ * sets the WHILE condition handle to (*any_active && *loop_iter < max_iter)
+ * and advances *loop_iter, so a loop runs at most max_iter times. */
+int lfts_saddle_begin(lfts_ctx ctx, int R, double mix_init, const lfts_saddle_state *st);
+int lfts_saddle_next(lfts_ctx ctx, unsigned long long handle, const lfts_saddle_state *st, int max_iter);
+/* After the saddle-point loop of a step, per replica r (examples/fts/lfts.py:
+ * 219-235, 711-730, 866): failed = isnan(err) || err >= tolerance; the
+ * Hamiltonian from the field moments mean/msq ([R][S], of the fields before the
+ * pressure shift) and Q ([R][P]):
+ *   H = (sum_p -poly[p] ln Q[r][p]) + (-mean[S-1] + sum_{i<S-1} h2[i] msq[i]
+ *       + h1[i] mean[i]) + h_const,   poly[p] = volume fraction / alpha;
+ * the pressure field w_aux[r][S-1] loses its mean; when restore != 0 a failed
+ * replica gets w_save and phi_save ([R][S][M]) back into w_aux and phi[s][r];
+ * active[r] = 1.  stats (device doubles) receives, for a host read in one copy:
+ *   [iter (R) | err (R) | H (R) | failed (R) | Q (R*P) | mean (R*S) | msq (R*S)].
+ * S <= LFTS_MAX_MONOMERS, P <= 8. */
+int lfts_lfts_step_finish(lfts_ctx ctx, int R, int S, int P, long long M, const lfts_saddle_state *st, double tolerance,
+                          const double *mean, const double *msq, const double *Q, const double *h1, const double *h2,
+                          double h_const, const double *poly, int restore, double *w_aux, const double *w_save,
+                          double *const *phi, const double *phi_save, double *scratch, double *stats);
 /* Anderson-mixing coefficients of every replica on the device
  * (src/common/AndersonMixing.cpp:19-47 and CpuAndersonMixing.cpp:122-146):
  * where ndots[r] > 0 the new dot row dots[r*L + i] (i < ndots[r]) enters the
@@ -404,9 +443,11 @@ int lfts_sf_accumulate(lfts_ctx ctx, int R, int S, int I, const void *spec, cons
  * that overlap in time (two streams, or two host threads, on one device) race
  * and must be serialised by the caller.  Each call writes every scratch entry
  * it reads, so nothing needs clearing between calls.
- * The first call on each device looks up the array's address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. */
+ * The first call in each device context looks up the array's address
+ * (cudaGetSymbolAddress) with that device current and caches it with the
+ * context's id; make that first call before any stream capture.  A new
+ * context on the device (after cudaDeviceReset) gets a fresh lookup on its
+ * first call, which must likewise precede any capture. */
 #define LFTS_DOTS_STATIC_MAX_JOBS 256
 int lfts_dots_static(int precision, long long M, const lfts_dot_job *jobs, int njobs, double *out, void *stream);
 

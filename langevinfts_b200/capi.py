@@ -96,6 +96,14 @@ _SIGS = {
     "lfts_status_post": [C.c_void_p, C.c_void_p, C.c_int],
     "lfts_status_wait": [C.c_void_p, C.c_int, C.c_void_p],
     "lfts_autotune": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_size_t],
+    "lfts_step_impl": [C.c_void_p, C.c_char_p, C.c_size_t],
+    "lfts_graph_while_begin": [C.c_void_p, C.POINTER(C.c_ulonglong)],
+    "lfts_graph_while_end": [C.c_void_p],
+    "lfts_saddle_begin": [C.c_void_p, C.c_int, C.c_double, C.c_void_p],
+    "lfts_saddle_next": [C.c_void_p, C.c_ulonglong, C.c_void_p, C.c_int],
+    "lfts_lfts_step_finish": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_longlong, C.c_void_p, C.c_double, C.c_void_p,
+                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_void_p,
+                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "lfts_pcg64_raw": [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p],
     "lfts_pcg64_normal": [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_double, C.c_void_p],
     "lfts_conv3d_bf16": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,

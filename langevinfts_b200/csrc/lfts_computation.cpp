@@ -539,9 +539,9 @@ std::string GpuComputation::autotune(int reps) {
     return std::string(buf);
 }
 
-void GpuComputation::enqueue_statistics() {
+void GpuComputation::enqueue_statistics(bool use_graph) {
     if (mol_->get_n_solvent_types() > 0) LFTS_THROW("batched statistics do not support solvents");
-    if (use_graph_) {
+    if (use_graph_ && use_graph) {
         if (!stats_graph_) {
             const long long before = lfts_ctx_launches(ctx_);
             check_rc(lfts_graph_begin(ctx_));

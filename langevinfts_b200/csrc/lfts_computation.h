@@ -86,7 +86,9 @@ class GpuComputation {
     int *active_device() { return active_.as<int>(); }
     // Enqueue field factors, propagators, partition functions, block and
     // per-type concentrations for every active replica (graph-capturable).
-    void enqueue_statistics();
+    void enqueue_statistics(bool use_graph = true);
+    // kernels run by an outside graph replay, for kernel_launches()
+    void count_replayed(long long n) { graph_kernels_replayed_ += n; }
     // Copy the partition functions of every replica to the host.
     std::vector<double> partitions_host();
     // kernels launched so far: direct launches + kernels replayed in graphs

@@ -1,6 +1,7 @@
 // liblfts_b200: C-ABI implementation of the B200 chain-propagator engine.
 // Declarations and the reference interfaces each entry replaces are in
 // include/lfts_b200.h.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -59,6 +60,9 @@ struct lfts_ctx_s {
     int *status_host = nullptr;           // pinned words read by lfts_status_wait
     cudaEvent_t status_ev[LFTS_STATUS_SLOTS] = {};
     long long launches = 0;  // kernels enqueued through this context (graph replays excluded)
+    // device-controlled loops inside a graph capture (lfts_graph_while_begin/end):
+    // the body is captured on body_stream while the outer capture waits on outer_stream
+    cudaStream_t body_stream = nullptr, outer_stream = nullptr;
 };
 
 struct lfts_graph_s {
@@ -328,6 +332,7 @@ extern "C" int lfts_ctx_destroy(lfts_ctx c) {
     for (int i = 0; i < LFTS_STATUS_SLOTS; i++)
         if (c->status_ev[i]) cudaEventDestroy(c->status_ev[i]);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    if (c->body_stream) cudaStreamDestroy(c->body_stream);
     delete c;
     return 0;
 }
@@ -424,6 +429,47 @@ extern "C" int lfts_graph_end(lfts_ctx c, lfts_graph *out) {
         return fail(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
     }
     *out = gr;
+    return 0;
+}
+// A conditional WHILE node after the work captured so far on the context
+// stream; the context stream then points at a private stream that captures
+// into the node's body graph until lfts_graph_while_end.  The handle starts at
+// 1 on every launch of the graph (cudaGraphCondAssignDefault), so the body
+// runs at least once; device code in the body sets it (lfts_saddle_next).
+extern "C" int lfts_graph_while_begin(lfts_ctx c, unsigned long long *handle) {
+    if (!c || !handle) return fail("null argument");
+    if (c->outer_stream) return fail("lfts_graph_while_begin: loops do not nest");
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    CK(cudaStreamGetCaptureInfo(c->stream, &status, nullptr, &g, &deps, &ndeps));
+    if (status != cudaStreamCaptureStatusActive || !g) return fail("lfts_graph_while_begin: the context stream is not capturing");
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};  // the rest zero-initialised
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, ndeps, &np));
+    CK(cudaStreamUpdateCaptureDependencies(c->stream, &node, 1, cudaStreamSetCaptureDependencies));
+    if (!c->body_stream) CK(cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCaptureToGraph(c->body_stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    c->outer_stream = c->stream;
+    c->stream = c->body_stream;
+    *handle = (unsigned long long)h;
+    return 0;
+}
+extern "C" int lfts_graph_while_end(lfts_ctx c) {
+    if (!c) return fail("null context");
+    if (!c->outer_stream) return fail("lfts_graph_while_end without lfts_graph_while_begin");
+    cudaGraph_t body = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->body_stream, &body);
+    c->stream = c->outer_stream;
+    c->outer_stream = nullptr;
+    if (e != cudaSuccess) return fail(std::string("lfts_graph_while_end: cudaStreamEndCapture: ") + cudaGetErrorString(e));
     return 0;
 }
 extern "C" int lfts_graph_launch(lfts_ctx c, lfts_graph g) {
@@ -732,30 +778,82 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
     return v;
 }
 
+// Compensated (error-free transform) summation for the FP32 propagator form:
+// sums of FP32 products are accumulated in FP64 as a pair (s, c) where s is
+// the running sum and c the running sum of the rounding errors of every
+// addition (Knuth's two-sum; Neumaier's improvement of Kahan's method), and
+// reduced across threads with the same transform.  The FP64 form keeps the
+// plain FP64 sums.
+__device__ __forceinline__ void comp_add(double &s, double &c, double x) {
+    const double t = s + x;
+    const double bp = t - s;
+    c += (s - (t - bp)) + (x - bp);
+    s = t;
+}
+// block sum of compensated pairs (block of NTHR threads, sh holds 2 * NWARP
+// doubles); s + c of the block is valid in thread 0
+__device__ __forceinline__ double block_sum_comp(double s, double c, double *sh) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const double so = __shfl_down_sync(0xffffffffu, s, o), co = __shfl_down_sync(0xffffffffu, c, o);
+        comp_add(s, c, so);
+        c += co;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) { sh[w] = s; sh[NWARP + w] = c; }
+    __syncthreads();
+    s = 0.0;
+    c = 0.0;
+    if (w == 0) {
+        s = lane < NWARP ? sh[lane] : 0.0;
+        c = lane < NWARP ? sh[NWARP + lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double so = __shfl_down_sync(0xffffffffu, s, o), co = __shfl_down_sync(0xffffffffu, c, o);
+            comp_add(s, c, so);
+            c += co;
+        }
+    }
+    return s + c;
+}
+template <typename T>
+struct Acc {  // plain FP64 sum for T = double, compensated FP64 sum for T = float
+    double s = 0.0, c = 0.0;
+    __device__ __forceinline__ void add(double x) {
+        if (sizeof(T) == 4) comp_add(s, c, x);
+        else s += x;
+    }
+    __device__ __forceinline__ double value() const { return s + c; }
+    __device__ __forceinline__ double block(double *sh) const {
+        return sizeof(T) == 4 ? block_sum_comp(s, c, sh) : block_sum(s, sh);
+    }
+};
+
 constexpr int DOT_CHUNKS = 128;
 
 template <typename T>
 __global__ void __launch_bounds__(NTHR) k_dots(const lfts_dot_job *__restrict__ jobs, long long M, double *partials) {
-    __shared__ double sh[NWARP];
+    __shared__ double sh[2 * NWARP];
     const lfts_dot_job jb = jobs[blockIdx.y];
     const T *a = (const T *)jb.a, *b = (const T *)jb.b, *w = (const T *)jb.w;
-    double acc = 0.0;
+    Acc<T> acc;
     for (long long i = blockIdx.x * (long long)NTHR + threadIdx.x; i < M; i += (long long)gridDim.x * NTHR) {
-        double v = (double)a[i] * (double)b[i];
+        double v = (double)a[i] * (double)b[i];  // exact for FP32 operands
         if (w) v /= (double)w[i];
-        acc += v;
+        acc.add(v);
     }
-    acc = block_sum(acc, sh);
-    if (threadIdx.x == 0) partials[(long long)blockIdx.y * gridDim.x + blockIdx.x] = acc;
+    const double v = acc.block(sh);
+    if (threadIdx.x == 0) partials[(long long)blockIdx.y * gridDim.x + blockIdx.x] = v;
 }
+// T selects the summation of the partials as in Acc<T> (compensated for float)
+template <typename T = double>
 __global__ void __launch_bounds__(NTHR) k_finish(const double *__restrict__ partials, int nparts, const double *scale_src,
                                                  int scale_stride, double mult, double *out, int out_stride, int ncomp) {
     // job = blockIdx.x; component = blockIdx.y; partials[(job*nparts + p)*ncomp + comp]
-    __shared__ double sh[NWARP];
+    __shared__ double sh[2 * NWARP];
     const int j = blockIdx.x, d = blockIdx.y;
-    double acc = 0.0;
-    for (int p = threadIdx.x; p < nparts; p += NTHR) acc += partials[((long long)j * nparts + p) * ncomp + d];
-    acc = block_sum(acc, sh);
+    Acc<T> a;
+    for (int p = threadIdx.x; p < nparts; p += NTHR) a.add(partials[((long long)j * nparts + p) * ncomp + d]);
+    const double acc = a.block(sh);
     if (threadIdx.x == 0) {
         const double sc = scale_src ? *(const double *)((const char *)scale_src + (long long)j * scale_stride) : 1.0;
         out[(long long)j * out_stride + d] = acc * sc * mult;
@@ -766,10 +864,15 @@ extern "C" int lfts_dots(lfts_ctx c, const lfts_dot_job *jobs, int nj, double *o
     for (int j0 = 0; j0 < nj; j0 += 4096) {
         const int n = nj - j0 < 4096 ? nj - j0 : 4096;
         const dim3 grid(DOT_CHUNKS, n);
-        if (c->prec == 8) k_dots<double><<<grid, NTHR, 0, c->stream>>>(jobs + j0, c->g.M, c->partials);
-        else k_dots<float><<<grid, NTHR, 0, c->stream>>>(jobs + j0, c->g.M, c->partials);
-        k_finish<<<dim3(n, 1), NTHR, 0, c->stream>>>(c->partials, DOT_CHUNKS, (const double *)&jobs[j0].scale,
-                                                    (int)sizeof(lfts_dot_job), 1.0, out + j0, 1, 1);
+        if (c->prec == 8) {
+            k_dots<double><<<grid, NTHR, 0, c->stream>>>(jobs + j0, c->g.M, c->partials);
+            k_finish<double><<<dim3(n, 1), NTHR, 0, c->stream>>>(c->partials, DOT_CHUNKS, (const double *)&jobs[j0].scale,
+                                                                (int)sizeof(lfts_dot_job), 1.0, out + j0, 1, 1);
+        } else {
+            k_dots<float><<<grid, NTHR, 0, c->stream>>>(jobs + j0, c->g.M, c->partials);
+            k_finish<float><<<dim3(n, 1), NTHR, 0, c->stream>>>(c->partials, DOT_CHUNKS, (const double *)&jobs[j0].scale,
+                                                               (int)sizeof(lfts_dot_job), 1.0, out + j0, 1, 1);
+        }
         c->launches += 2;
     }
     CKLAUNCH();
@@ -784,14 +887,16 @@ __global__ void __launch_bounds__(NTHR) k_phi(const lfts_phi_job *__restrict__ j
     const T *ql = (const T *)jb.q_left, *qr = (const T *)jb.q_right;
     const double norm = jb.q_div ? jb.norm / *jb.q_div : jb.norm;
     for (long long i = blockIdx.x * (long long)NTHR + threadIdx.x; i < M; i += (long long)gridDim.x * NTHR) {
-        double acc = 0.0;
+        Acc<T> a;
+        double acc;
         if (MODEL == 0) {
             for (int n = 0; n <= jb.n_right; n++)
-                acc += coefs[jb.coef_offset + n] * (double)ql[(long long)(jb.n_left - n) * M + i] * (double)qr[(long long)n * M + i];
+                a.add(coefs[jb.coef_offset + n] * (double)ql[(long long)(jb.n_left - n) * M + i] * (double)qr[(long long)n * M + i]);
+            acc = a.value();
         } else {
             for (int n = 1; n <= jb.n_right; n++)
-                acc += (double)ql[(long long)(jb.n_left - n + 1) * M + i] * (double)qr[(long long)n * M + i];
-            acc /= (double)((const T *)jb.fac)[i];
+                a.add((double)ql[(long long)(jb.n_left - n + 1) * M + i] * (double)qr[(long long)n * M + i]);
+            acc = a.value() / (double)((const T *)jb.fac)[i];
         }
         jb.phi[i] = acc * norm;
     }
@@ -821,7 +926,7 @@ __global__ void __launch_bounds__(NTHR) k_xstress(GridPlan g, const lfts_step_jo
                                                   int TJ, double *partials) {
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double sh[NWARP];
+    __shared__ double sh[2 * NWARP];
     const int n0 = g.n0;
     C *tile = (C *)smem_raw;
     C *twx = tile + 2 * n0 * TJ;
@@ -845,7 +950,7 @@ __global__ void __launch_bounds__(NTHR) k_xstress(GridPlan g, const lfts_step_jo
     __syncthreads();
     const LineMap lmx = {2 * TJ, TJ, n0 * TJ, TJ};
     dit_lines<C, true, GEN>(tile, lmx, g.ax[0], twx, -1, tid, NTHR);
-    double acc[3] = {0, 0, 0};
+    Acc<T> acc[3];
     for (int i = tid; i < n0 * TJ; i += NTHR) {
         const int jj = i % TJ, x = i / TJ;
         if (j0 + jj < plane) {
@@ -853,13 +958,13 @@ __global__ void __launch_bounds__(NTHR) k_xstress(GridPlan g, const lfts_step_jo
             const C A = tile[x * TJ + jj], B = tile[(n0 + x) * TJ + jj];
             double co = (double)A.x * (double)B.x + (double)A.y * (double)B.y;
             if (bond) co *= (double)bond[k] * (double)g.M;  // tables carry 1/M
-            acc[0] += co * basis[k];
-            acc[1] += co * basis[g.Mc + k];
-            acc[2] += co * basis[2 * g.Mc + k];
+            acc[0].add(co * basis[k]);
+            acc[1].add(co * basis[g.Mc + k]);
+            acc[2].add(co * basis[2 * g.Mc + k]);
         }
     }
     for (int d = 0; d < 3; d++) {
-        const double v = block_sum(acc[d], sh);
+        const double v = acc[d].block(sh);
         if (tid == 0) partials[((long long)job * gridDim.x + blockIdx.x) * 3 + d] = v;
     }
 }
@@ -890,8 +995,8 @@ static int stress_t(lfts_ctx c, const lfts_stress_job *jobs, int nj, const doubl
         k_stress_prep<T><<<(n + 127) / 128, 128, 0, st>>>(jobs + j0, n, spec, g.Mc, c->sjobs);
         k_plane_forward<T, 1, GEN><<<dim3(g.n0, 2 * n), NTHR, c->sm_pf1, st>>>(g, c->sjobs, 0, FM_NONE, 0, 0, c->zb);
         k_xstress<T, GEN><<<dim3(c->ntiles, n), NTHR, smx, st>>>(g, c->sjobs, jobs + j0, basis, c->TJ, c->partials);
-        k_finish<<<dim3(n, 3), NTHR, 0, st>>>(c->partials, c->ntiles, (const double *)&jobs[j0].weight,
-                                             (int)sizeof(lfts_stress_job), 1.0, out + 3 * (long long)j0, 3, 3);
+        k_finish<T><<<dim3(n, 3), NTHR, 0, st>>>(c->partials, c->ntiles, (const double *)&jobs[j0].weight,
+                                                (int)sizeof(lfts_stress_job), 1.0, out + 3 * (long long)j0, 3, 3);
     }
     CKLAUNCH();
     return 0;
@@ -997,15 +1102,15 @@ extern "C" int lfts_lincomb(lfts_ctx c, double *out, int nsrc, const double *con
 
 template <typename T>
 __global__ void __launch_bounds__(NTHR) k_pow_sum(const T *__restrict__ fac, int power, long long M, double *partials) {
-    __shared__ double sh[NWARP];
-    double acc = 0.0;
+    __shared__ double sh[2 * NWARP];
+    Acc<T> acc;
     for (long long i = blockIdx.x * (long long)NTHR + threadIdx.x; i < M; i += (long long)gridDim.x * NTHR) {
         double f = (double)fac[i], v = f;
         for (int p = 1; p < power; p++) v *= f;
-        acc += v;
+        acc.add(v);
     }
-    acc = block_sum(acc, sh);
-    if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+    const double v = acc.block(sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = v;
 }
 template <typename T>
 __global__ void k_solvent_phi(const T *__restrict__ fac, int power, double vf, const double *__restrict__ Q,
@@ -1024,7 +1129,8 @@ extern "C" int lfts_solvent(lfts_ctx c, const void *fac, int power, double vf, d
     const long long M = c->g.M;
     if (c->prec == 8) k_pow_sum<double><<<DOT_CHUNKS, NTHR, 0, c->stream>>>((const double *)fac, power, M, c->partials);
     else k_pow_sum<float><<<DOT_CHUNKS, NTHR, 0, c->stream>>>((const float *)fac, power, M, c->partials);
-    k_finish<<<dim3(1, 1), NTHR, 0, c->stream>>>(c->partials, DOT_CHUNKS, nullptr, 0, dv_over_V, Q_out, 1, 1);
+    if (c->prec == 8) k_finish<double><<<dim3(1, 1), NTHR, 0, c->stream>>>(c->partials, DOT_CHUNKS, nullptr, 0, dv_over_V, Q_out, 1, 1);
+    else k_finish<float><<<dim3(1, 1), NTHR, 0, c->stream>>>(c->partials, DOT_CHUNKS, nullptr, 0, dv_over_V, Q_out, 1, 1);
     if (c->prec == 8) k_solvent_phi<double><<<grid_for(M), NTHR, 0, c->stream>>>((const double *)fac, power, vf, Q_out, phi_out, M);
     else k_solvent_phi<float><<<grid_for(M), NTHR, 0, c->stream>>>((const float *)fac, power, vf, Q_out, phi_out, M);
     CKLAUNCH();
@@ -1158,19 +1264,51 @@ constexpr int DOTS_STATIC_MAX_DEVICES = 64;
 static std::mutex g_dots_static_mu;
 static double *g_dots_static_ptr[DOTS_STATIC_MAX_DEVICES];
 
-// Address of the scratch array on the current device, looked up once per
-// device (with that device current) and cached.
+// The current context's unique id (cuCtxGetId, never reused within a
+// process), through the driver entry points the runtime exposes, so the
+// library needs no link to the driver library.  0 when no context is current.
+typedef CUresult (*lfts_pfn_ctx_get_current)(CUcontext *);
+typedef CUresult (*lfts_pfn_ctx_get_id)(CUcontext, unsigned long long *);
+static int current_context_id(unsigned long long *id) {
+    static lfts_pfn_ctx_get_current get_current = nullptr;
+    static lfts_pfn_ctx_get_id get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        CK(cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa));
+        CK(cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb));
+        if (!a || !b || qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess)
+            return fail("lfts_dots_static: the driver offers no cuCtxGetCurrent / cuCtxGetId");
+        get_current = (lfts_pfn_ctx_get_current)a;
+        get_id = (lfts_pfn_ctx_get_id)b;
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS) return fail("lfts_dots_static: cuCtxGetCurrent failed");
+    *id = 0;
+    if (ctx && get_id(ctx, id) != CUDA_SUCCESS) return fail("lfts_dots_static: cuCtxGetId failed");
+    return 0;
+}
+
+// Address of the scratch array in the current device's context, looked up
+// (with that device current) the first time a context is seen and cached with
+// the context's id: a new context on the device (after cudaDeviceReset, which
+// reloads the module, possibly at another address) gets a new lookup.
+static unsigned long long g_dots_static_ctx[DOTS_STATIC_MAX_DEVICES];
 static int dots_static_scratch(double **out) {
     int dev = -1;
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= DOTS_STATIC_MAX_DEVICES)
         return fail("lfts_dots_static: device ordinal " + std::to_string(dev) + " out of range");
     std::lock_guard<std::mutex> lock(g_dots_static_mu);
-    if (!g_dots_static_ptr[dev]) {
+    unsigned long long id = 0;
+    if (current_context_id(&id)) return -1;
+    if (!g_dots_static_ptr[dev] || id == 0 || id != g_dots_static_ctx[dev]) {
         double *p = nullptr;
-        CK(cudaGetSymbolAddress((void **)&p, g_dots_static_scratch));
+        CK(cudaGetSymbolAddress((void **)&p, g_dots_static_scratch));  // makes the primary context current if none is
         if (!p) return fail("lfts_dots_static: cudaGetSymbolAddress returned a null address");
+        if (current_context_id(&id)) return -1;
         g_dots_static_ptr[dev] = p;
+        g_dots_static_ctx[dev] = id;
     }
     *out = g_dots_static_ptr[dev];
     return 0;
@@ -1188,10 +1326,15 @@ extern "C" int lfts_dots_static(int precision, long long M, const lfts_dot_job *
     if (dots_static_scratch(&scratch)) return -1;
     cudaStream_t st = (cudaStream_t)stream;
     const dim3 grid(DOT_CHUNKS, nj);
-    if (precision == 8) k_dots<double><<<grid, NTHR, 0, st>>>(jobs, M, scratch);
-    else k_dots<float><<<grid, NTHR, 0, st>>>(jobs, M, scratch);
-    k_finish<<<dim3(nj, 1), NTHR, 0, st>>>(scratch, DOT_CHUNKS, (const double *)&jobs[0].scale, (int)sizeof(lfts_dot_job),
-                                           1.0, out, 1, 1);
+    if (precision == 8) {
+        k_dots<double><<<grid, NTHR, 0, st>>>(jobs, M, scratch);
+        k_finish<double><<<dim3(nj, 1), NTHR, 0, st>>>(scratch, DOT_CHUNKS, (const double *)&jobs[0].scale,
+                                                       (int)sizeof(lfts_dot_job), 1.0, out, 1, 1);
+    } else {
+        k_dots<float><<<grid, NTHR, 0, st>>>(jobs, M, scratch);
+        k_finish<float><<<dim3(nj, 1), NTHR, 0, st>>>(scratch, DOT_CHUNKS, (const double *)&jobs[0].scale,
+                                                      (int)sizeof(lfts_dot_job), 1.0, out, 1, 1);
+    }
     CKLAUNCH();
     return 0;
 }
@@ -1318,6 +1461,16 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
         report[report_cap - 1] = 0;
     }
     return rc;
+}
+
+extern "C" int lfts_step_impl(lfts_ctx c, char *name, size_t cap) {
+    if (!c || !name || cap == 0) return fail("null argument");
+    std::string n = c->r8 ? (c->xcap ? "register-64 xcap" + std::to_string(c->xcap) : std::string("register-64"))
+                  : c->r12 ? (c->xcap ? "register-96 xcap" + std::to_string(c->xcap) : std::string("register-96"))
+                  : c->fastN ? std::string("cubic") : std::string("generic");
+    std::strncpy(name, n.c_str(), cap - 1);
+    name[cap - 1] = 0;
+    return 0;
 }
 
 // ---------------------------------------------------------------- U-Net convolution (tcgen05)

@@ -242,6 +242,7 @@ __global__ void k_saddle_control(SaddleArgs a, const double *__restrict__ var) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.R) return;
     const lfts_saddle_state &s = a.st;
+    const int it = a.it > 0 ? a.it : *s.loop_iter;  // a graph loop keeps its iteration number on the device
     s.flag[r] = 0;
     s.ndots[r] = 0;
     s.mode[r] = 0;
@@ -256,7 +257,7 @@ __global__ void k_saddle_control(SaddleArgs a, const double *__restrict__ var) {
         const double eo = s.err[r];
         s.err_old[r] = eo;
         s.err[r] = e;
-        s.iter[r] = a.it;
+        s.iter[r] = it;
         if (e < a.tol) {
             s.active[r] = 0;  // converged: fields and statistics stay as they are
         } else {
@@ -281,6 +282,84 @@ __global__ void k_saddle_control(SaddleArgs a, const double *__restrict__ var) {
         }
     }
     s.head[r] = s.head_raw[r] > 0 ? s.head_raw[r] : 0;
+}
+
+// start of a saddle-point search of every replica (the state am_reset and the
+// host loop start from); thread 0 also starts the graph loop's counter
+__global__ void k_saddle_begin(lfts_saddle_state s, int R, double mix_init) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r == 0) {
+        *s.loop_iter = 1;
+        *s.any_active = 1;
+    }
+    if (r >= R) return;
+    s.active[r] = 1;
+    s.n_anderson[r] = -1;
+    s.head_raw[r] = -1;
+    s.iter[r] = 0;
+    s.err[r] = 1e20;
+    s.err_old[r] = 1e20;
+    s.mix[r] = mix_init;
+}
+// last work of a loop body: continue while a replica is active and fewer than
+// max_iter iterations have run; the counter bounds the loop by itself
+__global__ void k_saddle_next(lfts_saddle_state s, cudaGraphConditionalHandle h, int max_iter) {
+    const int it = *s.loop_iter;
+    const unsigned go = (*s.any_active != 0 && it < max_iter && it < 1000000) ? 1u : 0u;
+    *s.loop_iter = it + 1;
+    cudaGraphSetConditional(h, go);
+}
+
+constexpr int FINISH_MAX_POLY = 8;
+struct FinishArgs {
+    lfts_saddle_state st;
+    int R, S, P;
+    double tol, h_const;
+    double h1[LFTS_MAX_MONOMERS], h2[LFTS_MAX_MONOMERS], poly[FINISH_MAX_POLY];
+};
+// per replica: failure flag, Hamiltonian, the pressure mean, the packed statistics
+__global__ void k_step_finish(FinishArgs a, const double *__restrict__ mean, const double *__restrict__ msq,
+                              const double *__restrict__ Q, double *__restrict__ pm, double *__restrict__ stats) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.R) return;
+    const int R = a.R, S = a.S, P = a.P;
+    const double e = a.st.err[r];
+    const double *mr = mean + (long long)r * S, *qr = msq + (long long)r * S;
+    double h = -mr[S - 1];
+    for (int i = 0; i < S - 1; i++) {
+        h += a.h2[i] * qr[i];
+        h += a.h1[i] * mr[i];
+    }
+    double hp = 0.0;
+    for (int p = 0; p < P; p++) hp -= a.poly[p] * log(Q[(long long)r * P + p]);
+    stats[r] = (double)a.st.iter[r];
+    stats[R + r] = e;
+    stats[2 * R + r] = hp + h + a.h_const;
+    stats[3 * R + r] = (isnan(e) || e >= a.tol) ? 1.0 : 0.0;
+    double *o = stats + 4 * (long long)R;
+    for (int p = 0; p < P; p++) o[(long long)r * P + p] = Q[(long long)r * P + p];
+    o += (long long)R * P;
+    for (int i = 0; i < S; i++) {
+        o[(long long)r * S + i] = mr[i];
+        o[(long long)R * S + (long long)r * S + i] = qr[i];
+    }
+    pm[r] = mr[S - 1];
+    a.st.active[r] = 1;
+}
+struct PhiPtrs {
+    double *phi[LFTS_MAX_MONOMERS];
+};
+// a replica whose saddle point failed gets its fields and concentrations back
+__global__ void k_restore_failed(int R, int S, long long M, const double *__restrict__ failed, double *__restrict__ w_aux,
+                                 const double *__restrict__ w_save, PhiPtrs phi, const double *__restrict__ phi_save) {
+    const int r = blockIdx.y;
+    if (failed[r] == 0.0) return;
+    const long long n = (long long)S * M, base = (long long)r * n;
+    for (long long t = blockIdx.x * (long long)NT + threadIdx.x; t < n; t += (long long)gridDim.x * NT) {
+        w_aux[base + t] = w_save[base + t];
+        const int sidx = (int)(t / M);
+        phi.phi[sidx][(long long)r * M + (t - (long long)sidx * M)] = phi_save[base + t];
+    }
 }
 
 // Largest Anderson history the device solve holds (shared memory of one block).
@@ -550,6 +629,61 @@ extern "C" int lfts_saddle_control(lfts_ctx ctx, int R, int I, int it, const dou
     LCK(cudaMemsetAsync(st->any_active, 0, sizeof(int), s));
     k_saddle_control<<<(R + 63) / 64, 64, 0, s>>>(a, var);
     lfts_internal_count(ctx, 1);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_saddle_begin(lfts_ctx ctx, int R, double mix_init, const lfts_saddle_state *st) {
+    if (!ctx || !st || !st->loop_iter || !st->any_active) return lfts_internal_fail("null argument");
+    if (R < 1) return lfts_internal_fail("saddle begin: R must be positive");
+    k_saddle_begin<<<(R + 63) / 64, 64, 0, (cudaStream_t)lfts_ctx_stream(ctx)>>>(*st, R, mix_init);
+    lfts_internal_count(ctx, 1);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_saddle_next(lfts_ctx ctx, unsigned long long handle, const lfts_saddle_state *st, int max_iter) {
+    if (!ctx || !st || !st->loop_iter || !st->any_active) return lfts_internal_fail("null argument");
+    if (max_iter < 1) return lfts_internal_fail("saddle next: max_iter must be positive");
+    k_saddle_next<<<1, 1, 0, (cudaStream_t)lfts_ctx_stream(ctx)>>>(*st, (cudaGraphConditionalHandle)handle, max_iter);
+    lfts_internal_count(ctx, 1);
+    LCK(cudaPeekAtLastError());
+    return 0;
+}
+
+extern "C" int lfts_lfts_step_finish(lfts_ctx ctx, int R, int S, int P, long long M, const lfts_saddle_state *st,
+                                     double tolerance, const double *mean, const double *msq, const double *Q, const double *h1,
+                                     const double *h2, double h_const, const double *poly, int restore, double *w_aux,
+                                     const double *w_save, double *const *phi, const double *phi_save, double *scratch,
+                                     double *stats) {
+    if (!ctx || !st || !mean || !msq || !Q || !poly || !w_aux || !scratch || !stats) return lfts_internal_fail("null argument");
+    if (R < 1 || S < 1 || S > LFTS_MAX_MONOMERS || P < 1 || P > FINISH_MAX_POLY)
+        return lfts_internal_fail("step finish: R, S (<= " + std::to_string(LFTS_MAX_MONOMERS) + ") or P (<= 8) out of range");
+    if (restore && (!w_save || !phi || !phi_save)) return lfts_internal_fail("step finish: restore needs the saved state");
+    FinishArgs a;
+    a.st = *st;
+    a.R = R;
+    a.S = S;
+    a.P = P;
+    a.tol = tolerance;
+    a.h_const = h_const;
+    for (int i = 0; i < LFTS_MAX_MONOMERS; i++) {
+        a.h1[i] = (h1 && i < S - 1) ? h1[i] : 0.0;
+        a.h2[i] = (h2 && i < S - 1) ? h2[i] : 0.0;
+    }
+    for (int p = 0; p < FINISH_MAX_POLY; p++) a.poly[p] = p < P ? poly[p] : 0.0;
+    cudaStream_t s = (cudaStream_t)lfts_ctx_stream(ctx);
+    k_step_finish<<<(R + 63) / 64, 64, 0, s>>>(a, mean, msq, Q, scratch, stats);
+    k_subtract_mean<<<dim3(grid1(M, 1024), R), NT, 0, s>>>(w_aux, S, S - 1, M, scratch, nullptr);
+    int n = 2;
+    if (restore) {
+        PhiPtrs pp;
+        for (int i = 0; i < LFTS_MAX_MONOMERS; i++) pp.phi[i] = i < S ? phi[i] : nullptr;
+        k_restore_failed<<<dim3(grid1((long long)S * M, 1024), R), NT, 0, s>>>(R, S, M, stats + 3 * (long long)R, w_aux, w_save,
+                                                                               pp, phi_save);
+        n++;
+    }
+    lfts_internal_count(ctx, n);
     LCK(cudaPeekAtLastError());
     return 0;
 }

@@ -92,10 +92,25 @@ class BatchedLangevin {
     long long n_complex_grid() const;
     GpuComputation &computation() { return *comp_; }
 
+    // One CUDA graph per Langevin step (default; set_step_graph(false) or the
+    // host control or more than LFTS_AM_SOLVE_MAX_HIST histories fall back to
+    // the loop driven from the host): the update of the real fields, then the
+    // saddle loop as a conditional WHILE node controlled on the device, then
+    // the Hamiltonian, pressure shift and restore-on-failure on the device.
+    void set_step_graph(bool on) { step_graph_on_ = on; }
+    bool step_graph() const { return graph_mode(); }
+
    private:
     void am_reset();
     void saddle_loop_host(SaddleStats &st);
     void saddle_loop_device(SaddleStats &st);
+    lfts_saddle_state saddle_state();
+    bool graph_mode() const;
+    void enqueue_update(int parity);
+    void enqueue_search_body(const lfts_saddle_state &ss);
+    void enqueue_search(bool restore);
+    SaddleStats read_stats();
+    void put_noise(const double *noise_dev);
     double hamiltonian(int r, const std::vector<double> &mean, const std::vector<double> &msq, const std::vector<double> &Q) const;
 
     LangevinConfig cfg_;
@@ -121,6 +136,12 @@ class BatchedLangevin {
     DevBuf sf_spec_, sf_jobs_, sf_acc_, sf_coef_, sf_pairs_;
     int sf_np_ = 0;
     std::vector<int> sf_pairs_host_;
+    // per-step graphs: update[parity of the noise buffers], search (loop + finish), and both in one
+    bool step_graph_on_ = true;
+    lfts_graph g_update_[2] = {nullptr, nullptr}, g_step_[2] = {nullptr, nullptr}, g_search_ = nullptr;
+    long long k_update_ = 0, k_search_fixed_ = 0, k_body_ = 0;
+    DevBuf fin_stats_, fin_scratch_;
+    std::vector<double> poly_coef_;
 };
 
 }  // namespace lfts

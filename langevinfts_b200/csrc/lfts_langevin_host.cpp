@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace lfts {
@@ -66,7 +67,7 @@ BatchedLangevin::BatchedLangevin(ComputationBox *cb, Molecules *mol, PropagatorA
     am_d_.alloc(ctx_, sizeof(double) * (size_t)R_ * L_ * I_ * M_);
     am_dots_.alloc(ctx_, sizeof(double) * (size_t)R_ * L_);
     am_a_.alloc(ctx_, sizeof(double) * (size_t)R_ * (L_ + 1));
-    sint_.alloc(ctx_, sizeof(int) * ((size_t)3 * R_ + 1));
+    sint_.alloc(ctx_, sizeof(int) * ((size_t)3 * R_ + 2));
     sdbl_.alloc(ctx_, sizeof(double) * (size_t)2 * R_);
     dot_ring_.alloc(ctx_, sizeof(double) * (size_t)R_ * L_ * L_);
     for (const auto &t : cfg.monomer_types) {
@@ -75,11 +76,25 @@ BatchedLangevin::BatchedLangevin(ComputationBox *cb, Molecules *mol, PropagatorA
     }
     check_rc(lfts_memset_async(ctx_, w_aux_.get(), 0, w_aux_.size()));
     for (auto p : phi_ptrs_) check_rc(lfts_memset_async(ctx_, p, 0, sizeof(double) * (size_t)R_ * M_));
+    const int P = mol->get_n_polymer_types();
+    for (int p = 0; p < P; p++) {
+        Polymer &pc = mol->get_polymer(p);
+        poly_coef_.push_back(pc.get_volume_fraction() / pc.get_alpha());
+    }
+    fin_stats_.alloc(ctx_, sizeof(double) * ((size_t)4 * R_ + (size_t)R_ * P + (size_t)2 * R_ * S_));
+    fin_scratch_.alloc(ctx_, sizeof(double) * (size_t)R_);
+    if (const char *e = std::getenv("LFTS_NO_GRAPH")) step_graph_on_ = std::string(e) != "1";
     check_rc(lfts_synchronize(ctx_));
     am_reset();
 }
 
 BatchedLangevin::~BatchedLangevin() {
+    for (int k = 0; k < 2; k++) {
+        if (g_update_[k]) lfts_graph_destroy(g_update_[k]);
+        if (g_step_[k]) lfts_graph_destroy(g_step_[k]);
+    }
+    if (g_search_) lfts_graph_destroy(g_search_);
+    fin_stats_.release(); fin_scratch_.release();
     w_aux_.release(); w_save_.release(); phi_save_.release(); d_cur_.release(); xi_[0].release(); xi_[1].release();
     partials_.release(); stats_.release(); ctl_.release(); am_w_.release(); am_d_.release(); am_dots_.release(); am_a_.release();
     sint_.release(); sdbl_.release(); dot_ring_.release(); pcg_.release(); noise_buf_.release();
@@ -121,6 +136,15 @@ double BatchedLangevin::hamiltonian(int r, const std::vector<double> &mean, cons
 }
 
 SaddleStats BatchedLangevin::find_saddle_point(bool restore_on_failure) {
+    if (restore_on_failure && graph_mode()) {  // the search half of a step (after langevin_update_*)
+        if (!g_search_) {
+            check_rc(lfts_graph_begin(ctx_));
+            enqueue_search(true);
+            check_rc(lfts_graph_end(ctx_, &g_search_));
+        }
+        check_rc(lfts_graph_launch(ctx_, g_search_));
+        return read_stats();
+    }
     SaddleStats st;
     st.iterations.assign(R_, 0);
     st.error.assign(R_, 1e20);
@@ -273,6 +297,27 @@ void BatchedLangevin::saddle_loop_host(SaddleStats &st) {
 // polls the "any replica active" word of iteration it - 1 while iteration it
 // is queued; an iteration queued after the last replica converged changes
 // nothing (every kernel skips inactive replicas or recomputes the same values).
+lfts_saddle_state BatchedLangevin::saddle_state() {
+    lfts_saddle_state ss;
+    int *si = sint_.as<int>();
+    int *d_head = ctl_.as<int>();
+    ss.active = comp_->active_device();
+    ss.n_anderson = si;
+    ss.head_raw = si + R_;
+    ss.iter = si + 2 * R_;
+    ss.any_active = si + 3 * R_;
+    ss.loop_iter = si + 3 * R_ + 1;
+    ss.head = d_head;
+    ss.flag = d_head + R_;
+    ss.ndots = d_head + 2 * R_;
+    ss.mode = d_head + 3 * R_;
+    ss.nh = d_head + 4 * R_;
+    ss.err = sdbl_.as<double>();
+    ss.err_old = ss.err + R_;
+    ss.mix = am_a_.as<double>();
+    return ss;
+}
+
 void BatchedLangevin::saddle_loop_device(SaddleStats &st) {
     const long long nI = (long long)I_ * M_;
     int *d_active = comp_->active_device();
@@ -282,21 +327,8 @@ void BatchedLangevin::saddle_loop_device(SaddleStats &st) {
     double *w_imag = w_aux_.as<double>() + (size_t)(S_ - I_) * M_;
     std::vector<double> scale(I_);
     for (int c = 0; c < I_; c++) scale[c] = cfg_.dt_scaling[cfg_.imag_idx[c]];
-    lfts_saddle_state ss;
+    lfts_saddle_state ss = saddle_state();
     int *si = sint_.as<int>();
-    ss.active = d_active;
-    ss.n_anderson = si;
-    ss.head_raw = si + R_;
-    ss.iter = si + 2 * R_;
-    ss.any_active = si + 3 * R_;
-    ss.head = d_head;
-    ss.flag = d_flag;
-    ss.ndots = d_ndots;
-    ss.mode = d_mode;
-    ss.nh = d_nh;
-    ss.err = sdbl_.as<double>();
-    ss.err_old = ss.err + R_;
-    ss.mix = d_mix;
     // initial state of every replica: active, no Anderson history (am_reset)
     {
         std::vector<int> ints((size_t)3 * R_);
@@ -345,6 +377,114 @@ void BatchedLangevin::saddle_loop_device(SaddleStats &st) {
     check_rc(lfts_memcpy_h2d(ctx_, d_active, ones.data(), sizeof(int) * R_));
 }
 
+bool BatchedLangevin::graph_mode() const {
+    return step_graph_on_ && !host_control_ && cfg_.am_max_hist <= LFTS_AM_SOLVE_MAX_HIST && poly_coef_.size() <= 8;
+}
+
+// this step's noise into the buffer the update reads as "current"
+void BatchedLangevin::put_noise(const double *noise_dev) {
+    if (Rr_ > 0 && noise_dev)
+        check_rc(lfts_memcpy_d2d_async(ctx_, xi_[1 - xi_cur_].get(), noise_dev, sizeof(double) * (size_t)R_ * Rr_ * M_));
+}
+
+// Leimkuhler-Matthews update of the real fields with xi_[parity] as the
+// previous noise and xi_[1 - parity] as this step's; fields and concentrations
+// are kept first for a restore
+void BatchedLangevin::enqueue_update(int parity) {
+    const size_t SM = (size_t)S_ * M_;
+    check_rc(lfts_memcpy_d2d_async(ctx_, w_save_.get(), w_aux_.get(), w_aux_.size()));
+    for (int r = 0; r < R_; r++)
+        for (int s = 0; s < S_; s++)
+            check_rc(lfts_memcpy_d2d_async(ctx_, phi_save_.as<double>() + r * SM + (size_t)s * M_, phi_ptrs_[s] + (size_t)r * M_,
+                                           sizeof(double) * M_));
+    if (Rr_ > 0) {
+        std::vector<double> sc(Rr_);
+        for (int c = 0; c < Rr_; c++) sc[c] = cfg_.dt_scaling[cfg_.real_idx[c]];
+        check_rc(lfts_lfts_langevin(ctx_, R_, S_, M_, Rr_, cfg_.real_idx.data(), cfg_.A.data(), cfg_.h_coef_mu1.data(),
+                                    cfg_.h_coef_mu2.data(), (const double *const *)phi_ptrs_.data(), cfg_.dt, sc.data(),
+                                    w_aux_.as<double>(), xi_[parity].as<double>(), xi_[1 - parity].as<double>(), nullptr));
+    }
+}
+
+// one saddle-point iteration of every active replica, control on the device
+void BatchedLangevin::enqueue_search_body(const lfts_saddle_state &ss) {
+    const long long nI = (long long)I_ * M_;
+    double *d_a = am_a_.as<double>() + R_;
+    double *d_mean = stats_.as<double>(), *d_var = d_mean + (size_t)R_ * S_;
+    double *w_imag = w_aux_.as<double>() + (size_t)(S_ - I_) * M_;
+    std::vector<double> scale(I_);
+    for (int c = 0; c < I_; c++) scale[c] = cfg_.dt_scaling[cfg_.imag_idx[c]];
+    check_rc(lfts_lfts_monomer_fields(ctx_, R_, S_, M_, cfg_.A.data(), w_aux_.as<double>(), w_mono_ptrs_.data()));
+    comp_->enqueue_statistics(false);
+    check_rc(lfts_lfts_field_deriv(ctx_, R_, S_, M_, I_, cfg_.imag_idx.data(), scale.data(), cfg_.A.data(),
+                                   cfg_.h_coef_mu1.data(), cfg_.h_coef_mu2.data(), w_aux_.as<double>(),
+                                   (const double *const *)phi_ptrs_.data(), d_cur_.as<double>(), ss.active));
+    check_rc(lfts_lfts_row_moments(ctx_, d_cur_.as<double>(), R_, I_, M_, M_, nI, nullptr, partials_.as<double>(), d_mean, d_var));
+    check_rc(lfts_lfts_row_moments(ctx_, d_cur_.as<double>(), R_, I_, M_, M_, nI, d_mean, partials_.as<double>(),
+                                   stats_.as<double>() + 2 * (size_t)R_ * S_, d_var));
+    check_rc(lfts_saddle_control(ctx_, R_, I_, 0, d_var, scale.data(), cfg_.tolerance, cfg_.am_start_error, cfg_.am_max_hist,
+                                 cfg_.am_mix_min, &ss));
+    check_rc(lfts_am_batch_insert(ctx_, R_, nI, L_, ss.head, ss.flag, w_imag, (long long)S_ * M_, d_cur_.as<double>(), nI,
+                                  am_w_.as<double>(), am_d_.as<double>()));
+    check_rc(lfts_am_batch_dots(ctx_, R_, nI, L_, ss.head, ss.ndots, am_d_.as<double>(), partials_.as<double>(),
+                                am_dots_.as<double>()));
+    check_rc(lfts_am_batch_solve(ctx_, R_, L_, ss.head, ss.ndots, ss.mode, ss.nh, am_dots_.as<double>(), dot_ring_.as<double>(),
+                                 d_a));
+    check_rc(lfts_am_batch_update(ctx_, R_, nI, L_, ss.head, ss.mode, ss.nh, ss.mix, d_a, w_imag, (long long)S_ * M_,
+                                  d_cur_.as<double>(), nI, am_w_.as<double>(), am_d_.as<double>(), w_imag, (long long)S_ * M_));
+}
+
+// the saddle-point search of a step as device work: reset, WHILE loop of
+// iterations, moments, Hamiltonian, pressure shift, restore of failed replicas
+void BatchedLangevin::enqueue_search(bool restore) {
+    const lfts_saddle_state ss = saddle_state();
+    const long long k0 = lfts_ctx_launches(ctx_);
+    check_rc(lfts_saddle_begin(ctx_, R_, cfg_.am_mix_init, &ss));
+    unsigned long long handle = 0;
+    check_rc(lfts_graph_while_begin(ctx_, &handle));
+    const long long k1 = lfts_ctx_launches(ctx_);
+    enqueue_search_body(ss);
+    check_rc(lfts_saddle_next(ctx_, handle, &ss, cfg_.max_iter));
+    const long long k2 = lfts_ctx_launches(ctx_);
+    check_rc(lfts_graph_while_end(ctx_));
+    double *d_mean = stats_.as<double>(), *d_var = d_mean + (size_t)R_ * S_;
+    check_rc(lfts_lfts_row_moments(ctx_, w_aux_.as<double>(), R_, S_, M_, M_, (long long)S_ * M_, nullptr, partials_.as<double>(),
+                                   d_mean, d_var));
+    check_rc(lfts_lfts_step_finish(ctx_, R_, S_, (int)poly_coef_.size(), M_, &ss, cfg_.tolerance, d_mean, d_var,
+                                   comp_->partition_device(), cfg_.h_coef_mu1.data(), cfg_.h_coef_mu2.data(), cfg_.h_const,
+                                   poly_coef_.data(), restore ? 1 : 0, w_aux_.as<double>(), w_save_.as<double>(),
+                                   phi_ptrs_.data(), phi_save_.as<double>(), fin_scratch_.as<double>(), fin_stats_.as<double>()));
+    k_body_ = k2 - k1;
+    k_search_fixed_ = (lfts_ctx_launches(ctx_) - k0) - k_body_;
+}
+
+// the packed statistics of lfts_lfts_step_finish (one copy, which also waits for the step)
+SaddleStats BatchedLangevin::read_stats() {
+    const int P = (int)poly_coef_.size();
+    std::vector<double> h((size_t)4 * R_ + (size_t)R_ * P + (size_t)2 * R_ * S_);
+    check_rc(lfts_memcpy_d2h(ctx_, h.data(), fin_stats_.get(), sizeof(double) * h.size()));
+    SaddleStats st;
+    st.iterations.resize(R_);
+    st.error.resize(R_);
+    st.hamiltonian.resize(R_);
+    st.failed.resize(R_);
+    int it_max = 0;
+    for (int r = 0; r < R_; r++) {
+        st.iterations[r] = (int)h[r];
+        st.error[r] = h[R_ + r];
+        st.hamiltonian[r] = h[2 * R_ + r];
+        st.failed[r] = h[3 * R_ + r] != 0.0 ? 1 : 0;
+        it_max = std::max(it_max, st.iterations[r]);
+    }
+    const double *o = h.data() + 4 * (size_t)R_;
+    st.partitions.assign(o, o + (size_t)R_ * P);
+    o += (size_t)R_ * P;
+    st.aux_mean.assign(o, o + (size_t)R_ * S_);
+    st.aux_msq.assign(o + (size_t)R_ * S_, o + (size_t)2 * R_ * S_);
+    comp_->count_replayed(k_search_fixed_ + k_body_ * (long long)std::max(it_max, 1));
+    return st;
+}
+
 SaddleStats BatchedLangevin::step(const double *noise) {
     if (Rr_ > 0) {
         DevBuf &cur = xi_[1 - xi_cur_];
@@ -354,11 +494,42 @@ SaddleStats BatchedLangevin::step(const double *noise) {
 }
 
 SaddleStats BatchedLangevin::step_device(const double *noise_dev) {
-    langevin_update_device(noise_dev);
-    return find_saddle_point(true);
+    if (!graph_mode()) {
+        langevin_update_device(noise_dev);
+        return find_saddle_point(true);
+    }
+    put_noise(noise_dev);
+    const int par = xi_cur_;
+    if (!g_step_[par]) {
+        const long long k0 = lfts_ctx_launches(ctx_);
+        check_rc(lfts_graph_begin(ctx_));
+        enqueue_update(par);
+        k_update_ = lfts_ctx_launches(ctx_) - k0;
+        enqueue_search(true);
+        check_rc(lfts_graph_end(ctx_, &g_step_[par]));
+    }
+    check_rc(lfts_graph_launch(ctx_, g_step_[par]));
+    if (Rr_ > 0) xi_cur_ = 1 - xi_cur_;  // this step's draw is the next step's "previous" noise (lfts.py:708-709)
+    comp_->count_replayed(k_update_);
+    return read_stats();
 }
 
 void BatchedLangevin::langevin_update_device(const double *noise_dev) {
+    if (graph_mode()) {
+        put_noise(noise_dev);
+        const int par = xi_cur_;
+        if (!g_update_[par]) {
+            const long long k0 = lfts_ctx_launches(ctx_);
+            check_rc(lfts_graph_begin(ctx_));
+            enqueue_update(par);
+            check_rc(lfts_graph_end(ctx_, &g_update_[par]));
+            k_update_ = lfts_ctx_launches(ctx_) - k0;
+        }
+        check_rc(lfts_graph_launch(ctx_, g_update_[par]));
+        comp_->count_replayed(k_update_);
+        if (Rr_ > 0) xi_cur_ = 1 - xi_cur_;
+        return;
+    }
     const size_t SM = (size_t)S_ * M_;
     // keep the fields and concentrations to restore replicas whose saddle point fails
     check_rc(lfts_memcpy_d2d_async(ctx_, w_save_.get(), w_aux_.get(), w_aux_.size()));

@@ -390,6 +390,8 @@ PYBIND11_MODULE(langevinfts, m) {
         }), py::keep_alive<1, 3>(), py::keep_alive<1, 4>(), py::keep_alive<1, 5>())
         .def("n_replicas", &BatchedLangevin::n_replicas)
         .def("set_host_control", &BatchedLangevin::set_host_control)
+        .def("set_step_graph", &BatchedLangevin::set_step_graph)
+        .def("step_graph", &BatchedLangevin::step_graph)
         .def("set_noise_streams", [](BatchedLangevin &b, py::array_t<unsigned long long, py::array::c_style | py::array::forcecast> st) {
             py::buffer_info bi = st.request();
             if (bi.size != 4LL * b.n_replicas()) throw std::runtime_error("noise streams must be an n_replicas x 4 uint64 array");
@@ -430,6 +432,11 @@ PYBIND11_MODULE(langevinfts, m) {
             py::gil_scoped_release nogil;
             return b.computation().autotune(reps);
         }, py::arg("reps") = 5)
+        .def("step_implementation", [](BatchedLangevin &b) {
+            char buf[64];
+            check_rc(lfts_step_impl(b.computation().context(), buf, sizeof buf));
+            return std::string(buf);
+        })
         .def("host_control", &BatchedLangevin::host_control)
         .def("stream_ptr", [](BatchedLangevin &b) { return (std::uintptr_t)b.stream(); })
         .def("kernel_launches", [](BatchedLangevin &b) { return b.computation().kernel_launches(); })

@@ -8,7 +8,8 @@
                         schedule produced by the reference's own host code
                         (oracle/_ref/ref_schedule_dump) for a set of molecules
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py /path/to/reference
+        (or set LFTS_REFERENCE to the reference checkout)
 Needs the oracle build (make -C oracle).
 """
 import json
@@ -19,7 +20,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LFTS_REFERENCE", "")
+if not REF:
+    raise SystemExit("usage: make_golden.py <reference checkout> (or set LFTS_REFERENCE)")
 DUMP = os.path.join(ROOT, "oracle", "_ref", "ref_schedule_dump")
 
 NUM = r"[-+]?\d*\.?\d+(?:[eE][-+]?\d+)?"

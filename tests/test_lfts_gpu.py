@@ -86,31 +86,62 @@ def test_device_saddle_control_matches_host_control(seeds):
     """The saddle loop with its per-replica control and Anderson solve on the
     device (lfts_saddle_control, lfts_am_batch_solve; no host round trip inside
     an iteration) gives the iterates of the same loop controlled from the host:
-    equal iteration counts, fields and errors to 1e-12.  One replica exercises
-    the step launches without an active mask."""
+    equal iteration counts, fields and errors to 1e-12.  The device control runs
+    twice: polled by the host once per iteration, and as one CUDA graph per
+    Langevin step (a conditional WHILE node; Hamiltonian, pressure shift and
+    restore on the device).  One replica exercises the step launches without an
+    active mask."""
     from langevinfts_b200 import langevinfts as L
     from langevinfts_b200.lfts import BatchedLFTS
     p = small_params()
     runs = []
-    for host in (True, False):
+    for host, graph in ((True, False), (False, False), (False, True)):
         sim = BatchedLFTS(p, seeds, module=L)
         sim.engine.set_host_control(host)
-        assert sim.engine.host_control() == host
+        sim.engine.set_step_graph(graph)
+        assert sim.engine.host_control() == host and sim.engine.step_graph() == graph
         st = sim.start([init(s, sim.M) for s in seeds])
-        hist = [(list(st["iterations"]), np.array(st["error"]), sim.fields())]
+        hist = [(list(st["iterations"]), np.array(st["error"]), sim.fields(), None, None)]
         for _ in range(3):
             st = sim.step()
             assert not any(st["failed"])
-            hist.append((list(st["iterations"]), np.array(st["error"]), sim.fields()))
+            hist.append((list(st["iterations"]), np.array(st["error"]), sim.fields(), np.array(st["hamiltonian"]),
+                         np.array(st["partitions"])))
         runs.append(hist)
-    for (ih, eh, wh), (idv, ed, wd) in zip(*runs):
-        assert ih == idv
-        np.testing.assert_allclose(ed, eh, rtol=1e-12)
-        assert np.max(np.abs(wd - wh)) <= 1e-12 * np.max(np.abs(wh))
+    for other in runs[1:]:
+        for (ih, eh, wh, hh, qh), (idv, ed, wd, hd, qd) in zip(runs[0], other):
+            assert ih == idv
+            np.testing.assert_allclose(ed, eh, rtol=1e-12)
+            assert np.max(np.abs(wd - wh)) <= 1e-12 * np.max(np.abs(wh))
+            if hh is not None:
+                np.testing.assert_allclose(hd, hh, rtol=1e-12)
+                np.testing.assert_allclose(qd, qh, rtol=1e-12)
 
 
-def test_failed_saddle_point_restores_fields():
-    """max_iter too small: the step fails and the fields go back (lfts.py:713-730)."""
+def test_step_graph_split_update_and_search():
+    """The two halves of a step (langevin_update_device, then finish_step, the
+    route of a learned start) as two graphs give the one-graph step's result."""
+    from langevinfts_b200 import langevinfts as L
+    from langevinfts_b200.lfts import BatchedLFTS
+    p = small_params()
+    seeds = [41, 42]
+    out = []
+    for split in (False, True):
+        sim = BatchedLFTS(p, seeds, module=L)
+        assert sim.engine.step_graph()
+        sim.start([init(s, sim.M) for s in seeds])
+        for _ in range(2):
+            st = sim.step(start=(lambda s: None) if split else None)
+        out.append((list(st["iterations"]), sim.fields(), np.array(st["hamiltonian"])))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_failed_saddle_point_restores_fields(graph):
+    """max_iter too small: the step fails and the fields go back (lfts.py:713-730),
+    with the step as one graph (restore on the device) and driven from the host."""
     from langevinfts_b200 import langevinfts as L
     from langevinfts_b200.lfts import BatchedLFTS, LFTS
     p = small_params()
@@ -121,10 +152,13 @@ def test_failed_saddle_point_restores_fields():
     # a new engine with max_iter=2 from the converged fields
     p2 = small_params(max_iter=2)
     sim2 = BatchedLFTS(p2, seeds, module=L)
+    sim2.engine.set_step_graph(graph)
     sim2.engine.set_fields(before)
+    phi2 = sim2.engine.get_concentrations(sim2.S)
     st = sim2.step()
     assert all(st["failed"]) and all(i == 2 for i in st["iterations"])
     assert np.array_equal(sim2.fields(), before)
+    assert np.array_equal(sim2.engine.get_concentrations(sim2.S), phi2)
     # the drop-in driver agrees on the failure
     one = LFTS(p2, random_seed=21, module=L)
     one.w_aux = before[0].copy()
