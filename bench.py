@@ -596,7 +596,7 @@ def run_scft(args):
     return 0
 
 
-def roofline_step_kernel(nx, njobs, reps=20, prec=8):
+def roofline_step_kernel(nx, njobs, reps=20, prec=8, impl=None):
     """Time lfts_step_continuous at the batch shape of the workload (njobs =
     replicas x propagators per schedule slot) with CUDA events on its stream.
     Every job has its own field factors, as the two keys of a slot of each
@@ -605,6 +605,10 @@ def roofline_step_kernel(nx, njobs, reps=20, prec=8):
     import torch
     from langevinfts_b200.capi import Context, StepJob, check
     ctx = Context([nx] * 3, precision=prec)
+    if impl:
+        check(ctx.lib.lfts_set_step_impl(ctx.h, impl.encode()))
+    name = C.create_string_buffer(64)
+    check(ctx.lib.lfts_step_impl(ctx.h, name, 64))
     M, Mc = ctx.M, ctx.Mc
     sb = prec  # bytes per real
     lx = (C.c_double * 3)(7.3, 7.3, 7.3)
@@ -634,6 +638,7 @@ def roofline_step_kernel(nx, njobs, reps=20, prec=8):
     ev[1].synchronize()
     ms = ev[0].elapsed_time(ev[1]) / reps
     ctx.close()
+    roofline_step_kernel.impl = name.value.decode()
     return ms, M, Mc
 
 
@@ -792,6 +797,8 @@ def main():
     ap.add_argument("--statistics", action="store_true",
                     help="time compute_statistics of single systems (configs 1 and 3) on the GPU and the reference CPU")
     ap.add_argument("--threads", type=int, default=1, help=argparse.SUPPRESS)
+    ap.add_argument("--step-impl", default=None,
+                    help="with --kernel-only: the step implementation to time (default: the context's own choice)")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only time the fused continuous step at 2*replicas jobs (for profiling)")
     args = ap.parse_args()
@@ -821,9 +828,10 @@ def main():
         import torch
         torch.cuda.init()
         sb = 8 if args.precision == "fp64" else 4
-        ms, M, Mc = roofline_step_kernel(args.nx, 2 * args.replicas, reps=args.steps, prec=sb)
+        ms, M, Mc = roofline_step_kernel(args.nx, 2 * args.replicas, reps=args.steps, prec=sb, impl=args.step_impl)
         unit = sb * (12 * M + 24 * Mc)
-        print(json.dumps({"kernel": "lfts_step_continuous", "jobs": 2 * args.replicas, "nx": args.nx, "launch_ms": ms,
+        print(json.dumps({"kernel": "lfts_step_continuous", "impl": roofline_step_kernel.impl, "precision": args.precision,
+                          "jobs": 2 * args.replicas, "nx": args.nx, "launch_ms": ms,
                           "pass_model_GBps": 2 * args.replicas * unit / (ms * 1e-3) / 1e9}))
         return 0
     if args.impl == "reference":

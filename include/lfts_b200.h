@@ -145,6 +145,10 @@ int lfts_autotune(lfts_ctx ctx, int njobs, int reps, char *report, size_t report
  * "register-64 xcap2", "register-96", "cubic", "generic"): the default chosen
  * at creation, or lfts_autotune's choice.  No counterpart in the reference. */
 int lfts_step_impl(lfts_ctx ctx, char *name, size_t cap);
+/* Make name the context's step implementation ("register-64", "register-96",
+ * "cubic", "generic"); an error when the context has no such implementation.
+ * Not during a graph capture.  No counterpart in the reference. */
+int lfts_set_step_impl(lfts_ctx ctx, const char *name);
 /* Discrete chain: out = [fac *] F^-1[ b * F[in] ] with b = bond (half=0) or
  * bond_half (half=1), multiplied by fac when with_fac=1.  (half=0, with_fac=1)
  * replaces advance_propagator_discrete (CudaSolverPseudo.cu:413-450);

@@ -97,6 +97,7 @@ _SIGS = {
     "lfts_status_wait": [C.c_void_p, C.c_int, C.c_void_p],
     "lfts_autotune": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_size_t],
     "lfts_step_impl": [C.c_void_p, C.c_char_p, C.c_size_t],
+    "lfts_set_step_impl": [C.c_void_p, C.c_char_p],
     "lfts_graph_while_begin": [C.c_void_p, C.POINTER(C.c_ulonglong)],
     "lfts_graph_while_end": [C.c_void_p],
     "lfts_saddle_begin": [C.c_void_p, C.c_int, C.c_double, C.c_void_p],

@@ -47,6 +47,7 @@ struct lfts_ctx_s {
     int TJ = 16, ntiles = 1, zb = 1;
     int fastN = 0;            // cubic grid handled by the compile-time specialised kernels (0: generic)
     int r8 = 0;               // 64^3: register-resident 8x8 line transforms (lfts_step_r8.cuh)
+    int fast_ok = 0, r8_ok = 0, r12_ok = 0;  // families set up at creation (lfts_set_step_impl)
     int r12 = 0;              // 96^3: register-resident 12x8 plane kernels (lfts_step_r12.cuh)
     int nsm = 0;              // streaming multiprocessors of the device
     int xcap = 0;             // CTAs per SM of the persistent x-passes (0: the kernel's own residency)
@@ -268,6 +269,9 @@ template <typename T> static int setup_plan(lfts_ctx c) {
             c->fastN = N;
             if (N == 64 && !std::getenv("LFTS_NO_R8")) c->r8 = r8_setup<T>(max_smem);
             if (N == 96 && !std::getenv("LFTS_NO_R12")) c->r12 = r12_setup<T>(max_smem);
+            c->fast_ok = N;
+            c->r8_ok = c->r8;
+            c->r12_ok = c->r12;
         }
     }
     return 0;
@@ -1461,6 +1465,24 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
         report[report_cap - 1] = 0;
     }
     return rc;
+}
+
+extern "C" int lfts_set_step_impl(lfts_ctx c, const char *name) {
+    if (!c || !name) return fail("null argument");
+    const std::string n(name);
+    const int fastN = c->fast_ok;
+    auto set = [&](int f, int r8, int r12) {
+        c->fastN = f;
+        c->r8 = r8;
+        c->r12 = r12;
+        c->xcap = 0;
+        return 0;
+    };
+    if (n == "register-64" && c->r8_ok) return set(fastN, 1, 0);
+    if (n == "register-96" && c->r12_ok) return set(fastN, 0, 1);
+    if (n == "cubic" && fastN) return set(fastN, 0, 0);
+    if (n == "generic") return set(0, 0, 0);
+    return fail("step implementation \"" + n + "\" is not available for this context");
 }
 
 extern "C" int lfts_step_impl(lfts_ctx c, char *name, size_t cap) {

@@ -9,11 +9,11 @@
 // stage, which is what bounded the staged kernels (their shared-memory pipe
 // ran at ~70 % while DRAM ran at ~1/3).
 //
-// Plane kernels keep one x-plane in shared memory, rows of PR = 73 complex
-// (element e of a row at e + e/8, so row reads of eight consecutive elements
-// and column reads of eight rows 73 apart are both free of bank conflicts).
-// Exchanges run in place: a z-line in its own row, a y-column task in its own
-// columns (kz and 64 - kz), with a skewed slot order down the column.
+// Plane kernels keep one x-plane in shared memory, 64 rows of 64 complex
+// elements, in a layout chosen per element size (PlaneLayout) so that the
+// row and column accesses of a warp are free of bank conflicts.  Exchanges
+// run in place: a z-line in its own row, a y-column task in its own columns
+// (kz and 64 - kz), with a skewed slot order down the column.
 //
 // Pairings used to halve the real transforms:
 //   * two branches of one row (continuous K1/K5): z = q (f0 + i f1);
@@ -35,14 +35,33 @@ namespace lfts {
 namespace r8 {
 
 constexpr int N = 64, NZC = N / 2 + 1, PLANE = N * NZC;
-constexpr int PR = 73;  // plane row stride (complex elements)
 constexpr int GROUPS = NTHR / 8;
 static_assert(GROUPS == 32, "one lane group of 8 per 64-point line, 32 lines per CTA");
 static_assert(PLANE % GROUPS == 0, "x-pass tiles cover the plane exactly");
 
-template <typename C> constexpr size_t plane_smem() { return sizeof(C) * (size_t)N * PR; }
-
-__device__ __forceinline__ int xpad(int e) { return e + (e >> 3); }
+// Slot of element e (0..63) of row r of the plane in shared memory.  The
+// accesses to serve: a row's lanes j write 8k + j and read 8j + k (fixed k;
+// the four groups of a warp take four consecutive rows), and a column's lanes
+// read rows j + 8m or 8k + ((j + k) & 7) (the four groups of a warp take four
+// consecutive columns).
+//   16-byte complex (FP64): a wavefront serves one lane group; rows of 73
+//     with e at e + e/8 keep each group's eight slots in distinct banks.
+//   8-byte complex (FP32): a wavefront serves two lane groups, so the two
+//     must also avoid each other: rows of 64, e XOR 8 (row parity) XOR
+//     (e / 8 mod 8) XOR (r AND 6).  Every pattern above then costs the
+//     minimum two wavefronts per warp access (column kc of a y-task: 1.25x),
+//     against 1.5-2x in the padded layout.
+template <typename C> struct PlaneLayout;
+template <> struct PlaneLayout<double2> {
+    static constexpr int RS = 73;
+    __device__ __forceinline__ static int at(int r, int e) { return r * RS + e + (e >> 3); }
+};
+template <> struct PlaneLayout<float2> {
+    static constexpr int RS = 64;
+    __device__ __forceinline__ static int at(int r, int e) { return r * RS + (e ^ ((r & 1) << 3) ^ ((e >> 3) & 7) ^ (r & 6)); }
+};
+template <typename C> __device__ __forceinline__ int at(int r, int e) { return PlaneLayout<C>::at(r, e); }
+template <typename C> constexpr size_t plane_smem() { return sizeof(C) * (size_t)N * PlaneLayout<C>::RS; }
 
 // w64^j = exp(sign * 2 pi i j / 64)
 template <typename C>
@@ -55,19 +74,20 @@ __device__ __forceinline__ C tw_base(int j, int sign) {
     return w;
 }
 
-// exchange slots along a row: element (k, j) at b + 9k + j
+// exchange slots along row r of plane P: (k, j) at element 8k + j
 template <typename C> struct RowX {
-    C *b;
-    __device__ __forceinline__ C &ref(int k, int j) const { return b[9 * k + j]; }
+    C *P;
+    int r;
+    __device__ __forceinline__ C &ref(int k, int j) const { return P[at<C>(r, 8 * k + j)]; }
 };
-// exchange slots down a column of a buffer with row stride S, skewed:
-// (k, j) at row 8k + ((j + k) & 7), so both the writes (fixed k) and the reads
-// (fixed j) of a lane group touch eight different banks
-template <typename C, int S> struct ColX {
-    C *b;
-    __device__ __forceinline__ C &ref(int k, int j) const { return b[(8 * k + ((j + k) & 7)) * S]; }
+// exchange slots down column e of plane P, skewed: (k, j) at row
+// 8k + ((j + k) & 7), so both the writes (fixed k) and the reads (fixed j) of
+// a lane group touch eight different banks
+template <typename C> struct ColS {
+    C *P;
+    int e;
+    __device__ __forceinline__ C &ref(int k, int j) const { return P[at<C>(8 * k + ((j + k) & 7), e)]; }
 };
-template <typename C> using ColS = ColX<C, PR>;
 
 // One 64-point transform held by the 8 lanes of a group (mask = the group's
 // lanes).  On entry lane j holds x[j + 8m] in a[m]; on exit lane t holds
@@ -168,23 +188,23 @@ __device__ __forceinline__ void get_columns(const C *st, int kz, C (&c)[8], int 
     }
 }
 
-// y-phase forward on rows paired (u, u + 32): z-lines u = 0..31 of P (row
-// stride S) hold Z_u = F_z[row u] + i F_z[row u + 32].  Task kz splits them,
-// transforms over y and leaves the column(s) in c (lane j: ky = j + 8k).
-template <typename C, int S>
+// y-phase forward on rows paired (u, u + 32): z-lines u = 0..31 of P hold
+// Z_u = F_z[row u] + i F_z[row u + 32].  Task kz splits them, transforms over
+// y and leaves the column(s) in c (lane j: ky = j + 8k).
+template <typename C>
 __device__ __forceinline__ void yfwd_paired_task(C *P, int kz, int j, C wf, unsigned mask, C (&c)[8]) {
     if (kz != 0) {
         const int kc = N - kz;
 #pragma unroll
         for (int m = 0; m < 4; m++) {
             const int u = j + 8 * m;
-            split_pair(P[u * S + xpad(kz)], cconj(P[u * S + xpad(kc)]), c[m], c[m + 4]);
+            split_pair(P[at<C>(u, kz)], cconj(P[at<C>(u, kc)]), c[m], c[m + 4]);
         }
     } else {
 #pragma unroll
         for (int m = 0; m < 4; m++) {
             const int u = j + 8 * m;
-            const C z0 = P[u * S], z32 = P[u * S + xpad(N / 2)];
+            const C z0 = P[at<C>(u, 0)], z32 = P[at<C>(u, N / 2)];
             c[m].x = z0.x;  // row u: DC + i Nyquist
             c[m].y = z32.x;
             c[m + 4].x = z0.y;  // row u + 32
@@ -192,13 +212,13 @@ __device__ __forceinline__ void yfwd_paired_task(C *P, int kz, int j, C wf, unsi
         }
     }
     __syncwarp(mask);
-    fft64<-1>(c, ColX<C, S>{P + xpad(kz)}, j, wf, mask);
+    fft64<-1>(c, ColS<C>{P, kz}, j, wf, mask);
 }
 
 // Pack rows u, u + 32 (lane j holds rows j + 8k, k < 8) of the inverse
 // y-transformed column(s) of task kz into the z-lines u of P (imaginary parts
 // of DC and Nyquist dropped, Hermitian extension at 64 - kz).
-template <typename C, int S>
+template <typename C>
 __device__ __forceinline__ void put_zlines_paired(C *P, int kz, int j, const C (&a)[8]) {
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -208,17 +228,17 @@ __device__ __forceinline__ void put_zlines_paired(C *P, int kz, int j, const C (
         if (kz != 0) {
             z.x = a0.x - a1.y;
             z.y = a0.y + a1.x;
-            P[u * S + xpad(kz)] = z;
+            P[at<C>(u, kz)] = z;
             z.x = a0.x + a1.y;
             z.y = -a0.y + a1.x;
-            P[u * S + xpad(N - kz)] = z;
+            P[at<C>(u, N - kz)] = z;
         } else {
             z.x = a0.x;  // s0(u) + i s0(u + 32)
             z.y = a1.x;
-            P[u * S] = z;
+            P[at<C>(u, 0)] = z;
             z.x = a0.y;  // s32(u) + i s32(u + 32)
             z.y = a1.y;
-            P[u * S + xpad(N / 2)] = z;
+            P[at<C>(u, N / 2)] = z;
         }
     }
 }
@@ -227,7 +247,7 @@ __device__ __forceinline__ void put_zlines_paired(C *P, int kz, int j, const C (
 template <typename C>
 __device__ __forceinline__ void y_forward_paired(C *P, int kz, int j, int lane, C wf, unsigned mask, C *plane) {
     C a[8];
-    yfwd_paired_task<C, PR>(P, kz, j, wf, mask, a);
+    yfwd_paired_task<C>(P, kz, j, wf, mask, a);
     put_columns(plane, kz, a, j, lane, mask);
 }
 
@@ -236,8 +256,8 @@ template <typename C>
 __device__ __forceinline__ void y_inverse_paired(C *P, int kz, int j, C wi, unsigned mask, const C *plane) {
     C a[8];
     get_columns(plane, kz, a, j);
-    fft64<+1>(a, ColS<C>{P + xpad(kz)}, j, wi, mask);
-    put_zlines_paired<C, PR>(P, kz, j, a);
+    fft64<+1>(a, ColS<C>{P, kz}, j, wi, mask);
+    put_zlines_paired<C>(P, kz, j, a);
 }
 
 // ------------------------------------------------------------------------
@@ -280,19 +300,19 @@ __global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFT
                 a[m].x = qv[m] * f0;
                 a[m].y = qv[m] * f1;
             }
-            fft64<-1>(a, RowX<C>{P + y * PR}, j, wf, mask);
+            fft64<-1>(a, RowX<C>{P, y}, j, wf, mask);
 #pragma unroll
-            for (int k = 0; k < 8; k++) P[y * PR + 9 * k + j] = a[k];
+            for (int k = 0; k < 8; k++) P[at<C>(y, 8 * k + j)] = a[k];
         }
         __syncthreads();
         // y-columns: task kz splits the branches; branch 1 waits in its own
-        // column (xkc) while branch 0 is transformed and stored
-        const int kz = grp, xkz = xpad(kz), xkc = xpad(kz == 0 ? N / 2 : N - kz);
+        // column (ekc) while branch 0 is transformed and stored
+        const int kz = grp, ekz = kz, ekc = kz == 0 ? N / 2 : N - kz;
         C A[8];
 #pragma unroll
         for (int m = 0; m < 8; m++) {
             const int y = j + 8 * m;
-            const C zk = P[y * PR + xkz], zc = P[y * PR + xkc];
+            const C zk = P[at<C>(y, ekz)], zc = P[at<C>(y, ekc)];
             C b;
             if (kz != 0) {
                 split_pair(zk, cconj(zc), A[m], b);
@@ -302,15 +322,15 @@ __global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFT
                 b.x = zk.y;  // branch 1
                 b.y = zc.y;
             }
-            P[y * PR + xkc] = b;
+            P[at<C>(y, ekc)] = b;
         }
         __syncwarp(mask);
-        fft64<-1>(A, ColS<C>{P + xkz}, j, wf, mask);
+        fft64<-1>(A, ColS<C>{P, ekz}, j, wf, mask);
         put_columns(out, kz, A, j, lane, mask);
 #pragma unroll
-        for (int m = 0; m < 8; m++) A[m] = P[(j + 8 * m) * PR + xkc];
+        for (int m = 0; m < 8; m++) A[m] = P[at<C>(j + 8 * m, ekc)];
         __syncwarp(mask);
-        fft64<-1>(A, ColS<C>{P + xkc}, j, wf, mask);
+        fft64<-1>(A, ColS<C>{P, ekc}, j, wf, mask);
         put_columns(out + g.Mc, kz, A, j, lane, mask);
     } else {
         // z-lines: rows u and u + 32 packed as real / imaginary part
@@ -330,9 +350,9 @@ __global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFT
                 a[m].x = qa[m] * fmul_mode(fm0, fa[m]);
                 a[m].y = qb[m] * fmul_mode(fm0, fb[m]);
             }
-            fft64<-1>(a, RowX<C>{P + u * PR}, j, wf, mask);
+            fft64<-1>(a, RowX<C>{P, u}, j, wf, mask);
 #pragma unroll
-            for (int k = 0; k < 8; k++) P[u * PR + 9 * k + j] = a[k];
+            for (int k = 0; k < 8; k++) P[at<C>(u, 8 * k + j)] = a[k];
         }
         __syncthreads();
         y_forward_paired(P, grp, j, lane, wf, mask, out);
@@ -505,17 +525,17 @@ __global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFT
         }
         C a[8];
 #pragma unroll
-        for (int m = 0; m < 8; m++) a[m] = P[u * PR + 9 * m + j];
+        for (int m = 0; m < 8; m++) a[m] = P[at<C>(u, 8 * m + j)];
         __syncwarp(mask);
-        fft64<+1>(a, RowX<C>{P + u * PR}, j, wi, mask);
+        fft64<+1>(a, RowX<C>{P, u}, j, wi, mask);
 #pragma unroll
         for (int k = 0; k < 8; k++) {
             a[k].x = a[k].x * ea[k] * ea[k];
             a[k].y = a[k].y * eb[k] * eb[k];
         }
-        fft64<-1>(a, RowX<C>{P + u * PR}, j, wf, mask);
+        fft64<-1>(a, RowX<C>{P, u}, j, wf, mask);
 #pragma unroll
-        for (int k = 0; k < 8; k++) P[u * PR + 9 * k + j] = a[k];
+        for (int k = 0; k < 8; k++) P[at<C>(u, 8 * k + j)] = a[k];
     }
     __syncthreads();
     y_forward_paired(P, grp, j, lane, wf, mask, sp);
@@ -544,36 +564,36 @@ __global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFT
     const T THIRD = (T)(1.0 / 3.0);  // multiply, not divide: no iterative division per element
     if (NBR == 2) {
         {
-            // branch 0 first; its inverse column waits in column xkz while
+            // branch 0 first; its inverse column waits in column ekz while
             // branch 1 is transformed, then both are packed into the z-lines
-            const int kz = grp, xkz = xpad(kz), xkc = xpad(kz == 0 ? N / 2 : N - kz);
+            const int kz = grp, ekz = kz, ekc = kz == 0 ? N / 2 : N - kz;
             C A[8];
             get_columns(in, kz, A, j);
-            fft64<+1>(A, ColS<C>{P + xkz}, j, wi, mask);
+            fft64<+1>(A, ColS<C>{P, ekz}, j, wi, mask);
 #pragma unroll
-            for (int k = 0; k < 8; k++) P[(j + 8 * k) * PR + xkz] = A[k];
+            for (int k = 0; k < 8; k++) P[at<C>(j + 8 * k, ekz)] = A[k];
             get_columns(in + g.Mc, kz, A, j);
-            fft64<+1>(A, ColS<C>{P + xkc}, j, wi, mask);
+            fft64<+1>(A, ColS<C>{P, ekc}, j, wi, mask);
             // z-line y = j + 8k: A + i B (Hermitian extension at 64 - kz)
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 const int y = j + 8 * k;
-                const C a = P[y * PR + xkz], bb = A[k];
+                const C a = P[at<C>(y, ekz)], bb = A[k];
                 C z;
                 if (kz != 0) {
                     z.x = a.x - bb.y;
                     z.y = a.y + bb.x;
-                    P[y * PR + xkz] = z;
+                    P[at<C>(y, ekz)] = z;
                     z.x = a.x + bb.y;
                     z.y = -a.y + bb.x;
-                    P[y * PR + xkc] = z;
+                    P[at<C>(y, ekc)] = z;
                 } else {
                     z.x = a.x;  // A(kz = 0) + i B(kz = 0)
                     z.y = bb.x;
-                    P[y * PR + xkz] = z;
+                    P[at<C>(y, ekz)] = z;
                     z.x = a.y;  // A(kz = 32) + i B(kz = 32)
                     z.y = bb.y;
-                    P[y * PR + xkc] = z;
+                    P[at<C>(y, ekc)] = z;
                 }
             }
         }
@@ -586,9 +606,9 @@ __global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFT
             for (int k = 0; k < 8; k++) eh[k] = frow[8 * k];
             C a[8];
 #pragma unroll
-            for (int m = 0; m < 8; m++) a[m] = P[y * PR + 9 * m + j];
+            for (int m = 0; m < 8; m++) a[m] = P[at<C>(y, 8 * m + j)];
             __syncwarp(mask);
-            fft64<+1>(a, RowX<C>{P + y * PR}, j, wi, mask);
+            fft64<+1>(a, RowX<C>{P, y}, j, wi, mask);
 #pragma unroll
             for (int k = 0; k < 8; k++) qrow[8 * k] = ((T)4 * eh[k] * a[k].y - eh[k] * eh[k] * a[k].x) * THIRD;
         }
@@ -604,9 +624,9 @@ __global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFT
         }
         C a[8];
 #pragma unroll
-        for (int m = 0; m < 8; m++) a[m] = P[u * PR + 9 * m + j];
+        for (int m = 0; m < 8; m++) a[m] = P[at<C>(u, 8 * m + j)];
         __syncwarp(mask);
-        fft64<+1>(a, RowX<C>{P + u * PR}, j, wi, mask);
+        fft64<+1>(a, RowX<C>{P, u}, j, wi, mask);
 #pragma unroll
         for (int k = 0; k < 8; k++) {
             qout[u * N + j + 8 * k] = a[k].x * fmul_mode(fm0, fa[k]);

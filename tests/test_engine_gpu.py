@@ -248,3 +248,51 @@ def test_stress(nx, lx):
         ref = orc.segment_stress(g, q1[j], q2[j], 1.0, bas, bo if j % 2 else None) * (0.5 + j)
         assert np.allclose(got[j], ref, rtol=1e-11, atol=1e-9 * np.max(np.abs(ref))), (j, got[j], ref)
     ctx.close()
+
+
+@pytest.mark.parametrize("prec", [4, 8])
+def test_step_implementations_agree_64cubed(prec):
+    """The step implementations of the 64^3 grid agree: the register-resident
+    kernels and the compile-time cubic kernels to round-off, 13 jobs with two
+    inactive replicas, whose outputs stay untouched; an implementation the grid
+    lacks is refused."""
+    from langevinfts_b200.capi import StepJob, check
+    nx, lx = (64, 64, 64), (7.3, 7.3, 7.3)
+    dt = np.dtype(np.float64 if prec == 8 else np.float32)
+    ctx = _ctx(nx, prec)
+    M = ctx.M
+    rng = np.random.default_rng(23)
+    ds, b2, nj = 1 / 90, 1.0, 13
+    bond, bondh = _tables(ctx, nx, lx, b2, ds, dt)
+    active = np.ones(nj, dtype=np.int32)
+    active[[3, 10]] = 0
+    act = ctx.upload(active)
+    jobs, q0 = [], []
+    for r in range(nj):
+        wd = ctx.upload(rng.normal(0, 1.0, M))
+        fac = ctx.malloc(M * dt.itemsize)
+        check(ctx.lib.lfts_field_factors(ctx.h, wd, -ds / 4, fac))
+        q0.append((1.0 + 0.3 * rng.random(M)).astype(dt))
+        q = ctx.malloc(2 * M * dt.itemsize)
+        spec = ctx.malloc(2 * ctx.Mc * 2 * dt.itemsize)
+        jobs.append(StepJob(q, M, q + M * dt.itemsize, M, fac, bond, bondh, spec, act, r, 0))
+    jp = _jobs(ctx, jobs)
+    names = ["register-64", "cubic"]
+    out = {}
+    for name in names:
+        check(ctx.lib.lfts_set_step_impl(ctx.h, name.encode()))
+        got = C.create_string_buffer(64)
+        check(ctx.lib.lfts_step_impl(ctx.h, got, 64))
+        assert got.value.decode() == name
+        for r in range(nj):
+            ctx.h2d(jobs[r].in_, np.concatenate([q0[r], np.full(M, -7.0, dtype=dt)]))
+        check(ctx.lib.lfts_step_continuous(ctx.h, jp, nj, 0))
+        ctx.sync()
+        out[name] = np.array([ctx.d2h(jobs[r].in_, (2, M), dt)[1] for r in range(nj)])
+    for r in np.flatnonzero(active == 0):
+        assert np.all(out["register-64"][r] == -7.0)
+    tol = 1e-12 if prec == 8 else 2e-5
+    assert _rel(out["cubic"].astype(float), out["register-64"].astype(float)) < tol
+    with pytest.raises(RuntimeError):
+        check(ctx.lib.lfts_set_step_impl(ctx.h, b"register-96"))
+    ctx.close()
