@@ -437,31 +437,14 @@ def run_learned(args):
     X, Y, it_gen = generate_pairs(sim, args.learned_steps)
     t_gen = time.time() - t0
     t0 = time.time()
-    start, hist = train(X, Y, seconds=args.learned_train)  # torch autograd over cuDNN
+    start, hist = train(X, Y, seconds=args.learned_train, tcgen05=False)  # torch autograd over cuDNN, torch AdamW
     t_train = time.time() - t0
     t0 = time.time()
-    start_tc, hist_tc = train(X, Y, seconds=args.learned_train, tcgen05=True)  # every convolution on tcgen05
+    start_tc, hist_tc = train(X, Y, seconds=args.learned_train)  # every convolution on tcgen05, AdamW kernel
     t_train_tc = time.time() - t0
-    w0, xi0 = sim.fields(), sim.engine.get_noise_prev()
-    rng0 = [g.bit_generator.state for g in sim.rngs]
-
-    def run(st):
-        sim.engine.set_fields(w0)
-        sim.engine.find_saddle_point()  # concentrations at w0 (a saddle point already)
-        sim.engine.set_noise_prev(xi0)
-        for g, s0 in zip(sim.rngs, rng0):
-            g.bit_generator.state = s0
-        iters, fails = [], 0
-        torch.cuda.synchronize()
-        t = time.time()
-        for _ in range(args.steps):
-            out = sim.step(start=st) if st is not None else sim.step()
-            iters += list(out["iterations"])
-            fails += int(sum(out["failed"]))
-        torch.cuda.synchronize()
-        return float(np.mean(iters)), R * args.steps / (time.time() - t), fails
-
-    plain, learned, learned_tc = run(None), run(start), run(start_tc)
+    from langevinfts_b200.learned import ablation
+    res = ablation(sim, [None, start, start_tc], args.steps)
+    plain, learned, learned_tc = [(r["mean_iterations"], R * args.steps / r["seconds"], r["failed"]) for r in res]
     print(json.dumps({"metric": "mean saddle-point iterations per Langevin step (learned start ablation)",
                       "workload": args.workload, "grid": [args.nx] * 3, "replicas": R, "precision": args.precision,
                       "plain": {"mean_iterations": plain[0], "replica_steps_per_s": plain[1], "failed": plain[2]},
@@ -473,8 +456,164 @@ def run_learned(args):
                       "steps": args.steps, "training_pairs": int(len(X)), "data_steps": args.learned_steps,
                       "data_seconds": t_gen, "train_seconds": t_train, "epochs": len(hist),
                       "loss_first_last": [hist[0][1], hist[-1][1]],
-                      "model": "3-level periodic 3D U-Net, 24 base channels, 3^3 kernels; 'learned': torch conv3d with BF16 autocast",
+                      "model": "3-level periodic 3D U-Net, 24 base channels, 3^3 kernels; 'learned': trained by torch autograd over "
+                               "cuDNN (BF16 autocast) and torch AdamW; both run their inference on lfts_conv3d_bf16",
                       "timing": "wall clock around the steps, host noise"}))
+    return 0
+
+
+def structure_function_step(sim, w_aux, phi):
+    """This step's contribution to S_AB(k) of every replica, the term
+    examples/fts/lfts.py:756-767 accumulates (mu_A(k) conj(phi_B(k)), transforms
+    of the host fields by numpy.fft.rfftn), scaled by V sqrt(nbar) as its
+    recording does (:780-782).  Real part, [R, nx, ny, nz/2+1]."""
+    nx = list(sim.cb.get_nx())
+    M, S = sim.M, sim.S
+    a, b = 0, 1  # the pair (A, B) in monomer_types order
+    out = []
+    for r in range(sim.R):
+        phib = np.fft.rfftn(phi[r, b].reshape(nx)) / M
+        mua = np.zeros_like(phib)
+        for k in range(S - 1):
+            mua += np.fft.rfftn(w_aux[r, k].reshape(nx)) * sim.mpt.matrix_a_inv[k, a] / sim.mpt.eigenvalues[k] / M
+        out.append((mua * np.conj(phib)).real)
+    return np.array(out) * sim.cb.get_volume() * np.sqrt(sim.params["langevin"]["nbar"])
+
+
+def radial_bins(sim, nbins):
+    """|k| of the half spectrum and its bin index (nbins bins up to the largest |k|/2)."""
+    nx, lx = list(sim.cb.get_nx()), list(sim.cb.get_lx())
+    ks = [2 * np.pi * np.fft.fftfreq(n, d=l / n) for n, l in zip(nx[:-1], lx[:-1])]
+    ks.append(2 * np.pi * np.fft.rfftfreq(nx[-1], d=lx[-1] / nx[-1]))
+    K = np.sqrt(sum(np.meshgrid(*[k ** 2 for k in ks], indexing="ij")))
+    edges = np.linspace(0.0, K.max() / 2, nbins + 1)
+    idx = np.digitize(K, edges) - 1
+    return K, edges, idx
+
+
+def run_ensemble(args):
+    """Ensemble statistics of the three forms against the plain FP64 run
+    (examples/fts/lfts.py:733-767 records the same quantities).  After
+    args.warmup plain FP64 steps from the seeded start, each form runs the same
+    args.steps Langevin steps from that state with the same PCG64 noise:
+      fp64          plain batched FP64
+      fp32          FP32 propagators, compensated FP64 reductions
+      fp32_learned  FP32 with the learned saddle-point start (trained in this
+                    run on pairs from plain FP32 steps that continue the state)
+    Per replica the time averages of H, dH/dchiN and the radially averaged
+    S_AB(k) (every --sf-period steps) are formed; each form is compared with
+    fp64 in units of the standard error over replicas: paired (the mean of the
+    per-replica differences / its standard error) and unpaired (difference of
+    the ensemble means / the combined standard error).  One JSON line."""
+    import torch
+    from langevinfts_b200 import langevinfts as L
+    from langevinfts_b200.ensemble import replica_seeds
+    from langevinfts_b200.learned import generate_pairs, train
+    from langevinfts_b200.lfts import BatchedLFTS
+    torch.cuda.init()
+    R, K = args.replicas, args.steps
+    p = workload_params(args.workload, args.nx)
+    seeds = replica_seeds(0, R, base=WORKLOADS[args.workload]["seed"])
+    t_all = time.time()
+    sims = {"cuda": BatchedLFTS(p, seeds, module=L, platform="cuda"),
+            "cuda-fp32": BatchedLFTS(p, seeds, module=L, platform="cuda-fp32")}
+    for s_ in sims.values():
+        s_.engine.autotune()
+    sim = sims["cuda"]
+    sim.start([initial_fields(s, sim.M) for s in seeds])
+    for _ in range(args.warmup):
+        sim.step()
+    w0, xi0 = sim.fields(), sim.engine.get_noise_prev()
+    rng0 = [g.bit_generator.state for g in sim.rngs]
+
+    def restore(s_):
+        s_.engine.set_fields(w0)
+        s_.engine.find_saddle_point()
+        s_.engine.set_noise_prev(xi0)
+        for g, st in zip(s_.rngs, rng0):
+            g.bit_generator.state = st
+    # the learned start: pairs from plain FP32 steps continuing the equilibrated state
+    f32 = sims["cuda-fp32"]
+    restore(f32)
+    t0 = time.time()
+    X, Y, _ = generate_pairs(f32, LEARNED_PAIR_STEPS)
+    start, hist = train(X, Y, seconds=args.learned_train)
+    t_train = time.time() - t0
+    _, edges, idx = radial_bins(sim, args.sf_bins)
+    forms = [("fp64", "cuda", None), ("fp32", "cuda-fp32", None), ("fp32_learned", "cuda-fp32", start)]
+    rec = {}
+    for name, plat, st in forms:
+        s_ = sims[plat]
+        restore(s_)
+        # per replica sums over the steps that met the tolerance: a failed step
+        # restores the fields and records nothing, as lfts.py:712-737 does
+        Hs, dHs, nok = np.zeros(R), np.zeros(R), np.zeros(R)
+        sf, nsf = np.zeros([R, args.sf_bins]), np.zeros(R)
+        H_steps, iters, fails = [], [], 0
+        t0 = time.time()
+        for k in range(K):
+            out = s_.step(start=st)
+            ok = 1.0 - np.array(out["failed"], dtype=float)
+            h = np.nan_to_num(np.array(out["hamiltonian"]))
+            Hs += ok * h
+            dHs += ok * np.nan_to_num(np.array([d["A,B"] for d in s_.h_deriv_chin(out)]))
+            nok += ok
+            H_steps.append(np.where(ok > 0, h, np.nan))
+            iters.append(out["iterations"])
+            fails += int(sum(out["failed"]))
+            if (k + 1) % args.sf_period == 0:
+                sk = structure_function_step(s_, s_.fields(), s_.engine.get_concentrations(s_.S))
+                for b in range(args.sf_bins):
+                    m = idx == b
+                    if m.any():
+                        sf[:, b] += ok * sk[:, m].mean(axis=1)
+                nsf += ok
+        rec[name] = {"H": Hs / np.maximum(nok, 1), "dH": dHs / np.maximum(nok, 1), "sf": sf / np.maximum(nsf, 1)[:, None],
+                     "H_steps": np.array(H_steps), "iters": np.array(iters), "fails": fails, "seconds": time.time() - t0}
+        sys.stderr.write(f"[ensemble] {name}: {K} steps in {rec[name]['seconds']:.0f} s, mean iterations "
+                         f"{np.mean(iters):.2f}, <H> {rec[name]['H'].mean():.6f}, failed {fails}\n")
+
+    def compare(a, b):
+        """a, b: per-replica time averages [R] (or [R, nb]); z-scores."""
+        d = a - b
+        se_p = d.std(axis=0, ddof=1) / np.sqrt(R)
+        se_u = np.sqrt(a.var(axis=0, ddof=1) / R + b.var(axis=0, ddof=1) / R)
+        z_p = np.where(se_p > 0, d.mean(axis=0) / np.where(se_p > 0, se_p, 1), 0.0)
+        z_u = (a.mean(axis=0) - b.mean(axis=0)) / np.where(se_u > 0, se_u, 1)
+        return d.mean(axis=0), z_p, z_u, se_u
+    base = rec["fp64"]
+    res = {}
+    nb_low = max(1, args.sf_bins // 2)
+    for name in ("fp32", "fp32_learned"):
+        r = rec[name]
+        dh, zp, zu, se = compare(r["H"], base["H"])
+        dd, zdp, zdu, sed = compare(r["dH"], base["dH"])
+        ds, zsp, zsu, ses = compare(r["sf"], base["sf"])
+        res[name] = {
+            "H": {"mean": float(r["H"].mean()), "diff": float(dh), "z_paired": float(zp), "z_unpaired": float(zu),
+                  "se_unpaired": float(se),
+                  "max_abs_diff_per_step": float(np.nanmax(np.abs(r["H_steps"] - base["H_steps"])))},
+            "dH_dchiN": {"mean": float(r["dH"].mean()), "diff": float(dd), "z_paired": float(zdp), "z_unpaired": float(zdu)},
+            "S_AB_k": {"max_abs_z_paired": float(np.max(np.abs(zsp[:nb_low]))),
+                       "max_abs_z_unpaired": float(np.max(np.abs(zsu[:nb_low]))),
+                       "max_rel_diff": float(np.max(np.abs(ds[:nb_low]) / np.maximum(np.abs(base["sf"].mean(0)[:nb_low]), 1e-300))),
+                       "bins_compared": nb_low},
+            "mean_saddle_iterations": float(r["iters"].mean()), "failed_steps": r["fails"],
+            "seconds": r["seconds"], "replica_steps_per_s_wall": R * K / r["seconds"]}
+    out = {"ensemble": "forms vs plain FP64, same state and noise", "workload": workload_config(R, args.nx, args.workload),
+           "replicas": R, "steps": K, "equilibration_steps": args.warmup, "sf_period": args.sf_period,
+           "sf_bins": args.sf_bins, "sf_k_edges": [float(e) for e in edges[:nb_low + 1]],
+           "criterion": "z_unpaired: (form mean - fp64 mean) / combined standard error over replicas, |z| <= 2 is "
+                        "agreement within 2 sigma; z_paired: mean per-replica difference / its standard error (same "
+                        "noise, so it resolves the deterministic offset of the form, reported with its size in diff)",
+           "fp64": {"H_mean": float(base["H"].mean()), "H_se_replicas": float(base["H"].std(ddof=1) / np.sqrt(R)),
+                    "dH_dchiN_mean": float(base["dH"].mean()), "mean_saddle_iterations": float(base["iters"].mean()),
+                    "failed_steps": base["fails"], "seconds": base["seconds"],
+                    "S_AB_k_low": [float(v) for v in base["sf"].mean(0)[:nb_low]]},
+           "forms": res, "learned_training": {"pairs": int(len(X)), "seconds": t_train, "epochs": len(hist),
+                                               "loss_first_last": [hist[0][1], hist[-1][1]]},
+           "total_seconds": time.time() - t_all}
+    print(json.dumps(out))
     return 0
 
 
@@ -596,6 +735,117 @@ def run_scft(args):
     return 0
 
 
+# timed steps of each variant (capped so the default run stays within minutes)
+VARIANT_STEPS_MAX = 8
+# plain Langevin steps whose fields train the learned start, and its time budget (s)
+LEARNED_PAIR_STEPS = 12
+LEARNED_TRAIN_S = 90.0
+
+
+def time_batched(sim, K, start=None):
+    """value and e2e of K Langevin steps of a started BatchedLFTS: value with
+    each step's noise already in HBM (CUDA events on the engine stream), e2e
+    through the public step() with the noise drawn on the host every step and
+    the statistics copied out.  Returns (value, e2e, iterations, failed, launches, d2h bytes per step)."""
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    R = sim.R
+    stream = torch.cuda.ExternalStream(sim.engine.stream_ptr())
+    noises = [torch.from_numpy(sim.draw_noise()).cuda() for _ in range(K)]
+    torch.cuda.synchronize()
+    iters, fails = [], 0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    k0 = sim.engine.kernel_launches()
+    ev[0].record(stream)
+    for k in range(K):
+        st = sim.step_device(noises[k].data_ptr(), start=start)
+        iters += st["iterations"]
+        fails += sum(st["failed"])
+    ev[1].record(stream)
+    ev[1].synchronize()
+    launches = sim.engine.kernel_launches() - k0
+    t = ev[0].elapsed_time(ev[1]) / 1000.0
+    del noises
+    pool_noise = sim.draw_noise()
+    torch.cuda.synchronize()
+    ex = ThreadPoolExecutor(max_workers=1)
+    nxt = ex.submit(sim.draw_noise)
+    d2h = 0
+    e0 = time.perf_counter()
+    ev[2].record(stream)
+    for k in range(K):
+        st = sim.step(pool_noise, start=start)
+        d2h += 8 * (len(st["error"]) * 4 + len(st["partitions"]) + len(st["aux_mean"]) + len(st["aux_msq"]))
+        pool_noise = nxt.result()
+        nxt = ex.submit(sim.draw_noise)
+    ev[3].record(stream)
+    ev[3].synchronize()
+    t_e2e = max(time.perf_counter() - e0, ev[2].elapsed_time(ev[3]) / 1000.0)
+    ex.shutdown(wait=False)
+    return R * K / t, R * K / t_e2e, iters, int(fails), int(launches), int(d2h / max(K, 1))
+
+
+def run_variants(args, value_fp64):
+    """The forms beside the plain batched FP64 headline, same workload:
+      fp32              FP32 propagators and FFTs, FP64 reductions (cuda-fp32)
+      fp32_learned      the same with the learned saddle-point start: a U-Net
+                        trained in this run (tensor-core kernels, AdamW kernel)
+                        on pairs from LEARNED_PAIR_STEPS plain FP32 steps
+      fp64_one_replica  the unbatched plain FP64 form: one replica per engine
+    Each carries value, e2e, mean saddle iterations, failed steps and its
+    ratio to the plain FP64 value."""
+    from langevinfts_b200 import langevinfts as L
+    from langevinfts_b200.ensemble import replica_seeds
+    from langevinfts_b200.learned import generate_pairs, train
+    from langevinfts_b200.lfts import BatchedLFTS
+    K = min(args.steps, VARIANT_STEPS_MAX)
+    p = workload_params(args.workload, args.nx)
+    seeds = replica_seeds(0, args.replicas, base=WORKLOADS[args.workload]["seed"])
+    out = {}
+
+    def entry(v, e, iters, fails, launches, d2h, sim, extra=None):
+        d = {"value": v, "e2e": {"value": e, "unit": UNIT, "h2d_bytes_per_step": sim.R * sim.mpt.R * sim.M * 8,
+                                 "d2h_bytes_per_step": d2h},
+             "unit": UNIT, "steps": K, "mean_saddle_iterations": float(np.mean(iters)), "failed_steps": fails,
+             "gpu_launches": launches, "vs_plain_fp64_value": v / value_fp64}
+        if extra:
+            d.update(extra)
+        return d
+    sim = BatchedLFTS(p, seeds, module=L, platform="cuda-fp32")
+    tune = sim.engine.autotune()
+    sim.start([initial_fields(s, sim.M) for s in seeds])
+    for _ in range(args.warmup):
+        sim.step()
+    r = time_batched(sim, K)
+    out["fp32"] = entry(*r, sim, {"dtype": "f32", "step_autotune": tune,
+                                  "platform": "cuda-fp32: FP32 propagators and FFTs, compensated FP64 reductions"})
+    sys.stderr.write(f"[bench] fp32 {r[0]:.3f} {UNIT} ({np.mean(r[2]):.2f} iterations)\n")
+    t0 = time.time()
+    X, Y, _ = generate_pairs(sim, LEARNED_PAIR_STEPS)
+    t_pairs = time.time() - t0
+    start, hist = train(X, Y, seconds=LEARNED_TRAIN_S)
+    r = time_batched(sim, K, start=start)
+    out["fp32_learned"] = entry(*r, sim, {
+        "dtype": "f32", "training_pairs": int(len(X)), "pair_steps": LEARNED_PAIR_STEPS, "pair_seconds": t_pairs,
+        "train_seconds": LEARNED_TRAIN_S, "epochs": len(hist), "loss_first_last": [hist[0][1], hist[-1][1]],
+        "network": "3-level periodic 3D U-Net, 24 base channels; convolutions forward and backward on lfts_conv3d_bf16 / "
+                   "lfts_conv3d_wgrad_bf16 (tcgen05), AdamW on lfts_adamw_f32, inference on lfts_conv3d_bf16"})
+    sys.stderr.write(f"[bench] fp32_learned {r[0]:.3f} {UNIT} ({np.mean(r[2]):.2f} iterations)\n")
+    del sim
+    one = BatchedLFTS(p, seeds[:1], module=L, platform="cuda")
+    one.start([initial_fields(seeds[0], one.M)])
+    for _ in range(args.warmup):
+        one.step()
+    K1 = max(K, 10)
+    r = time_batched(one, K1)
+    out["fp64_one_replica"] = entry(*r, one, {"dtype": "f64", "steps": K1, "replicas": 1,
+                                              "note": "the plain FP64 form without batching: one replica per engine"})
+    for v in out.values():
+        v["vs_fp64_one_replica_value"] = v["value"] / out["fp64_one_replica"]["value"]
+    sys.stderr.write(f"[bench] fp64 one replica {r[0]:.3f} {UNIT}\n")
+    return out
+
+
 def roofline_step_kernel(nx, njobs, reps=20, prec=8, impl=None):
     """Time lfts_step_continuous at the batch shape of the workload (njobs =
     replicas x propagators per schedule slot) with CUDA events on its stream.
@@ -705,7 +955,7 @@ def run_ours(args):
     d2h = 0
     for k in range(args.steps):
         s = sim.step(pool_noise)
-        d2h += 8 * (len(s["error"]) * 3 + len(s["partitions"])) + 8 * R * (1 + 21) * max(s["iterations"])
+        d2h += 8 * (len(s["error"]) * 4 + len(s["partitions"]) + len(s["aux_mean"]) + len(s["aux_msq"]))
         pool_noise = nxt.result()
         nxt = ex.submit(sim.draw_noise)
     ev2[1].record(stream)
@@ -764,6 +1014,8 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
+    if world == 1 and not args.no_variants and args.precision == "fp64":
+        out["variants"] = run_variants(args, value)
     print(json.dumps(out))
     if dist is not None:
         dist.destroy_process_group()
@@ -783,6 +1035,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
                     help="fp64 (the headline) or fp32 propagators with FP64 reductions (platform cuda-fp32)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the fp32 / fp32_learned / one-replica FP64 forms after the headline")
     ap.add_argument("--ref-sample", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--ref-steps", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--ref-budget", type=float, default=REFERENCE_STEP_BUDGET_S, help=argparse.SUPPRESS)
@@ -790,6 +1044,10 @@ def main():
     ap.add_argument("--ref-scft", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--scft", action="store_true", help="SCFT of the 64^3 asymmetric diblock (device loop, FP64 and FP32)")
     ap.add_argument("--conv", action="store_true", help="time the tensor-core U-Net convolutions against cuDNN")
+    ap.add_argument("--ensemble", action="store_true",
+                    help="ensemble <H>, dH/dchiN and S(k) of the FP32 and learned forms against plain FP64 (same noise)")
+    ap.add_argument("--sf-period", type=int, default=5, help=argparse.SUPPRESS)
+    ap.add_argument("--sf-bins", type=int, default=24, help=argparse.SUPPRESS)
     ap.add_argument("--learned", action="store_true",
                     help="ablation of the learned saddle-point start (U-Net) on the workload's system")
     ap.add_argument("--learned-steps", type=int, default=20, help="plain Langevin steps that make the training pairs")
@@ -822,6 +1080,8 @@ def main():
         return run_learned(args)
     if args.conv:
         return run_conv(args)
+    if args.ensemble:
+        return run_ensemble(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.kernel_only:

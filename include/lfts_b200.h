@@ -402,6 +402,14 @@ int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, const float 
 int lfts_conv3d_wgrad_bf16(void *stream, const void *x, const void *gy, float *dw, int B, int D, int H, int W, int cin,
                            int cout, int taps);
 
+/* AdamW step of the U-Net's training on n FP32 parameters (device p, g, m,
+ * v on the given cudaStream_t), in torch.optim.AdamW's order: p *= 1 - lr wd;
+ * m += (1 - b1)(g - m); v = b2 v + (1 - b2) g^2; p -= (lr / (1 - b1^step)) m /
+ * (sqrt(v) / sqrt(1 - b2^step) + eps).  step >= 1 counts the calls.  No
+ * counterpart in the reference (it has no learned component). */
+int lfts_adamw_f32(void *stream, float *p, const float *g, float *m, float *v, long long n, double lr, double b1, double b2,
+                   double eps, double weight_decay, int step);
+
 /* Adam field update of the SCFT driver (examples/scft/scft.py:42-54), on n
  * doubles: m = b1 m + (1-b1) d; v = b2 v + (1-b2) d^2;
  * w_new = w + lr (m / (1 - b1^count)) / (sqrt(v / (1 - b2^count)) + eps).

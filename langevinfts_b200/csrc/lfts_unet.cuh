@@ -530,3 +530,38 @@ extern "C" int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, c
     if (e != cudaSuccess) return fail(std::string("conv3d launch: ") + cudaGetErrorString(e));
     return 0;
 }
+
+// ---------------------------------------------------------------- AdamW (training of the U-Net)
+// Decoupled weight decay, then the Adam moments and the bias-corrected step,
+// in the order torch.optim.AdamW applies them:
+//   p *= 1 - lr wd;  m += (1 - b1)(g - m);  v = b2 v + (1 - b2) g^2;
+//   p -= (lr / (1 - b1^t)) m / (sqrt(v) / sqrt(1 - b2^t) + eps).
+__global__ void k_adamw_f32(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m, float *__restrict__ v,
+                            long long n, float decay, float b1, float b2, float eps, float step_size, float bc2_sqrt) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        float mi = m[i];
+        mi = mi + (1.0f - b1) * (gi - mi);
+        const float vi = v[i] * b2 + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] * decay;
+        p[i] = pi - step_size * (mi / (sqrtf(vi) / bc2_sqrt + eps));
+    }
+}
+
+extern "C" int lfts_adamw_f32(void *stream, float *p, const float *g, float *m, float *v, long long n, double lr, double b1,
+                              double b2, double eps, double weight_decay, int step) {
+    if (!p || !g || !m || !v) return fail("adamw: null argument");
+    if (n < 0 || step < 1) return fail("adamw: n must be >= 0 and step >= 1");
+    if (n == 0) return 0;
+    const double bc1 = 1.0 - std::pow(b1, step), bc2 = 1.0 - std::pow(b2, step);
+    long long blocks = (n + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_adamw_f32<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(p, g, m, v, n, (float)(1.0 - lr * weight_decay), (float)b1,
+                                                                   (float)b2, (float)eps, (float)(lr / bc1),
+                                                                   (float)std::sqrt(bc2));
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) return fail(std::string("adamw launch: ") + cudaGetErrorString(e));
+    return 0;
+}

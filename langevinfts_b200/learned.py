@@ -26,14 +26,20 @@ Pieces:
                     lfts_conv3d_wgrad_bf16).
   generate_pairs    training pairs from the plain solver: inputs (w_-, w_+prev)
                     and target w_+ of every replica and step.
-  train             AdamW on the mean-squared error of the residual, over
-                    torch's convolutions or (tcgen05=True) the tensor-core ones.
+  FlatAdamW         AdamW on this library's kernel (lfts_adamw_f32): the
+                    parameters live in one flat FP32 buffer, one launch a step.
+  train             AdamW on the mean-squared error of the residual; by default
+                    every convolution's forward and backward on the tensor
+                    cores and the update by FlatAdamW (tcgen05=False: torch's
+                    convolutions under BF16 autocast and torch's AdamW, kept as
+                    the comparison).
   LearnedStart      the callable BatchedLFTS.step(start=...) uses: reads w_aux
                     on the device (zero copy), writes the predicted w_+ in place
-                    on the engine's stream.
+                    on the engine's stream; inference on the tensor cores by
+                    default.
 
-Pooling, upsampling, concatenation and AdamW are torch's.  Grids must have
-extents divisible by 4.
+Pooling, upsampling and concatenation are torch tensor operations between the
+convolutions.  Grids must have extents divisible by 4.
 """
 import time
 
@@ -284,11 +290,48 @@ class TcgenUNet:
         return o.permute(0, 4, 1, 2, 3).float().contiguous()
 
 
+class FlatAdamW:
+    """AdamW whose update runs on this library's kernel (lfts_adamw_f32).  The
+    parameters are moved into one flat FP32 buffer (each parameter becomes a
+    view of it), the gradients are gathered into a second one, and one launch
+    updates everything; the moments m and v live beside them."""
+
+    def __init__(self, params, lr=1e-3, betas=(0.9, 0.999), eps=1e-8, weight_decay=1e-2):
+        self.params = [p for p in params if p.requires_grad]
+        n = sum(p.numel() for p in self.params)
+        dev = self.params[0].device
+        self.flat = torch.empty(n, dtype=torch.float32, device=dev)
+        off = 0
+        for p in self.params:
+            k = p.numel()
+            self.flat[off:off + k].copy_(p.detach().reshape(-1))
+            p.data = self.flat[off:off + k].view_as(p)
+            off += k
+        self.grad = torch.zeros_like(self.flat)
+        self.m = torch.zeros_like(self.flat)
+        self.v = torch.zeros_like(self.flat)
+        self.lr, self.betas, self.eps, self.weight_decay, self.t = lr, betas, eps, weight_decay, 0
+
+    def zero_grad(self, set_to_none=True):
+        for p in self.params:
+            p.grad = None
+
+    def step(self):
+        from langevinfts_b200.capi import check, lib
+        torch.cat([(p.grad if p.grad is not None else torch.zeros_like(p)).reshape(-1) for p in self.params], out=self.grad)
+        self.t += 1
+        check(lib().lfts_adamw_f32(torch.cuda.current_stream().cuda_stream, self.flat.data_ptr(), self.grad.data_ptr(),
+                                   self.m.data_ptr(), self.v.data_ptr(), self.flat.numel(), self.lr, self.betas[0],
+                                   self.betas[1], self.eps, self.weight_decay, self.t))
+
+
 class LearnedStart:
     """Callable for BatchedLFTS.step(start=...): predicts the imaginary field
-    of every replica from the fields on the device and writes it in place."""
+    of every replica from the fields on the device and writes it in place.
+    tcgen05=True (default): every convolution on this library's tensor-core
+    kernel; False: torch's convolutions under BF16 autocast."""
 
-    def __init__(self, model, s_in, s_out, batch=8, tcgen05=False):
+    def __init__(self, model, s_in, s_out, batch=8, tcgen05=True):
         self.model, self.s_in, self.s_out, self.batch = model.eval(), float(s_in), float(s_out), batch
         # tcgen05=True: the convolutions run on this library's tensor-core kernel
         self.net = TcgenUNet(self.model) if tcgen05 else None
@@ -314,11 +357,45 @@ class LearnedStart:
                 wr[:, ii] += d
 
 
-def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_decay=1e-4, seed=0, log=None, tcgen05=False):
+def ablation(sim, starts, nsteps):
+    """Run the same nsteps Langevin steps of a started BatchedLFTS once per entry
+    of starts (None: the plain warm start; else a LearnedStart): each run
+    begins from the fields, previous noise and PCG64 states the simulation has
+    now, so every run sees the same noise.  Returns, per entry, a dict of the
+    mean saddle iterations, the failed steps, the iterations per step and the
+    wall time; the simulation is left at the end of the last run."""
+    import torch
+    w0, xi0 = sim.fields(), sim.engine.get_noise_prev()
+    rng0 = [g.bit_generator.state for g in sim.rngs]
+    step0 = sim.langevin_step
+    out = []
+    for st in starts:
+        sim.engine.set_fields(w0)
+        sim.engine.find_saddle_point()  # concentrations at w0, a saddle point already
+        sim.engine.set_noise_prev(xi0)
+        for g, s0 in zip(sim.rngs, rng0):
+            g.bit_generator.state = s0
+        sim.langevin_step = step0
+        iters, fails = [], 0
+        torch.cuda.synchronize()
+        t = time.time()
+        for _ in range(nsteps):
+            r = sim.step(start=st) if st is not None else sim.step()
+            iters.append(list(r["iterations"]))
+            fails += int(sum(r["failed"]))
+        torch.cuda.synchronize()
+        out.append({"mean_iterations": float(np.mean(iters)), "failed": fails, "iterations": iters,
+                    "seconds": time.time() - t})
+    return out
+
+
+def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_decay=1e-4, seed=0, log=None, tcgen05=True):
     """AdamW on MSE of the scaled residual target (Y - w_+prev) / s_out until
-    `seconds` or `epochs` run out; BF16 autocast over torch's convolutions, or
-    (tcgen05=True) every convolution's forward and backward on this library's
-    tensor-core kernels.  Returns (LearnedStart, history of (epoch, mean loss))."""
+    `seconds` or `epochs` run out.  tcgen05=True (default): every convolution's
+    forward and backward on this library's tensor-core kernels and the update
+    by FlatAdamW (lfts_adamw_f32); False: BF16 autocast over torch's
+    convolutions and torch's AdamW.  Returns (LearnedStart, history of (epoch,
+    mean loss))."""
     torch.manual_seed(seed)
     s_in = float(np.std(X[:, 0])) or 1.0
     s_out = float(np.std(X[:, 1])) or 1.0
@@ -326,7 +403,10 @@ def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_dec
     tgt = torch.from_numpy((Y - X[:, 1:]) / s_out).cuda()
     model = UNet3D(cin=2, cout=1, base=base).cuda()
     fwd = TcgenUNetTrain(model) if tcgen05 else None
-    opt = torch.optim.AdamW(model.parameters(), lr=lr, weight_decay=weight_decay)
+    if tcgen05:
+        opt = FlatAdamW(model.parameters(), lr=lr, weight_decay=weight_decay)
+    else:
+        opt = torch.optim.AdamW(model.parameters(), lr=lr, weight_decay=weight_decay)
     n = xin.shape[0]
     hist, t0 = [], time.time()
     for ep in range(epochs):

@@ -370,6 +370,18 @@ class BatchedLFTS:
         self.langevin_step += 1
         return stats
 
+    def step_device(self, noise_ptr, start=None):
+        """One Langevin step with this step's noise already on the device (a
+        pointer to [R][n_real][M] doubles); start as in step()."""
+        if start is None:
+            stats = self.engine.step_device(noise_ptr)
+        else:
+            self.engine.langevin_update_device(noise_ptr)
+            start(self)
+            stats = self.engine.finish_step()
+        self.langevin_step += 1
+        return stats
+
     def fields(self):
         return self.engine.get_fields(self.S)
 

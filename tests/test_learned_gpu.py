@@ -61,3 +61,39 @@ def test_generate_pairs_and_training_lowers_the_loss():
     # the network can fit a handful of pairs: 150 AdamW steps on 4 of them
     start, hist = train(X[:4], Y[:4], base=8, seconds=120, epochs=150, batch=4, lr=3e-3)
     assert hist[-1][1] < 0.6 * hist[0][1], hist[:: max(1, len(hist) // 6)]
+
+
+def gain_params():
+    """The benchmark system (f = 0.5, chiN = 17, nbar = 100, N = 90, dt = 0.8,
+    tolerance 1e-4) on a 32^3 box of the same grid spacing (3.65)."""
+    return {
+        "nx": [32, 32, 32], "lx": [3.65, 3.65, 3.65], "chain_model": "continuous", "ds": 1 / 90,
+        "segment_lengths": {"A": 1.0, "B": 1.0}, "chi_n": {"A,B": 17.0},
+        "distinct_polymers": [{"volume_fraction": 1.0, "blocks": [{"type": "A", "length": 0.5}, {"type": "B", "length": 0.5}]}],
+        "langevin": {"dt": 0.8, "nbar": 100}, "saddle": {"max_iter": 100, "tolerance": 1e-4},
+        "am": {"max_hist": 20, "start_error": 5e-1, "mix_min": 0.01, "mix_init": 0.01},
+    }
+
+
+def test_trained_start_cuts_saddle_iterations():
+    """What the trained network gains: 16 replicas at 32^3, pairs from 12 plain
+    steps, 60 s of training on the tensor cores (convolutions forward and
+    backward, AdamW kernel), then the same 6 Langevin steps (same state, same
+    noise) from the plain warm start and from the network's prediction.  The
+    learned start needs at least 10 % fewer saddle-point iterations and every
+    step still reaches the 1e-4 tolerance."""
+    from langevinfts_b200.learned import ablation, generate_pairs, train
+    from langevinfts_b200.lfts import BatchedLFTS
+    seeds = list(range(300, 316))
+    sim = BatchedLFTS(gain_params(), random_seeds=seeds)
+    rng = np.random.Generator(np.random.PCG64(8))
+    sim.start([{"A": rng.normal(0, 1, sim.M), "B": rng.normal(0, 1, sim.M)} for _ in seeds])
+    for _ in range(3):
+        sim.step()
+    X, Y, it_pairs = generate_pairs(sim, 12)
+    start, hist = train(X, Y, seconds=60.0)
+    assert start.net is not None  # inference on the tensor cores
+    plain, learned = ablation(sim, [None, start], 6)
+    assert plain["failed"] == 0 and learned["failed"] == 0
+    assert learned["mean_iterations"] <= 0.9 * plain["mean_iterations"], (plain["mean_iterations"],
+                                                                          learned["mean_iterations"], hist[-1])

@@ -147,3 +147,62 @@ def test_training_on_the_tensor_cores_lowers_the_loss():
     start, hist = train(X, Y, base=8, seconds=120, epochs=40, batch=4, lr=3e-3, tcgen05=True)
     assert start.net is not None
     assert hist[-1][1] < 0.6 * hist[0][1], hist[:: max(1, len(hist) // 6)]
+
+
+def test_adamw_kernel_matches_torch_adamw():
+    """lfts_adamw_f32 (FlatAdamW) against torch.optim.AdamW in FP32 on the same
+    parameters and gradients, six steps."""
+    import torch
+    from langevinfts_b200.learned import FlatAdamW
+    torch.manual_seed(9)
+    shapes = [(24, 2, 3, 3, 3), (24,), (48, 24, 3, 3, 3), (1, 24, 1, 1, 1)]
+    a = [torch.nn.Parameter(torch.randn(s, device="cuda")) for s in shapes]
+    b = [torch.nn.Parameter(p.detach().clone()) for p in a]
+    ours = FlatAdamW(a, lr=2e-3, weight_decay=1e-2)
+    ref = torch.optim.AdamW(b, lr=2e-3, weight_decay=1e-2)
+    for _ in range(6):
+        for pa, pb in zip(a, b):
+            g = torch.randn_like(pa)
+            pa.grad, pb.grad = g.clone(), g.clone()
+        ours.step()
+        ref.step()
+    for pa, pb in zip(a, b):
+        assert float((pa.detach() - pb.detach()).abs().max()) <= 1e-5 * float(pb.detach().abs().max())
+
+
+@pytest.mark.parametrize("cin,cin_pad,cout,grid", [(24, 32, 48, (8, 8, 8)), (2, 16, 24, (16, 16, 16))])
+def test_conv_gradients_match_cpu_float64(cin, cin_pad, cout, grid):
+    """Input, weight and bias gradients of the tensor-core convolution
+    (_ConvFn: lfts_conv3d_bf16 with mirrored taps, lfts_conv3d_wgrad_bf16)
+    against float64 autograd of torch's CPU periodic conv3d on the same
+    BF16-rounded input, weights and output gradient."""
+    import torch
+    import torch.nn.functional as F
+    from langevinfts_b200.learned import _ConvFn
+    torch.manual_seed(cin + cout)
+    B = 2
+    w = (0.2 * torch.randn(cout, cin, 3, 3, 3)).to(torch.bfloat16).float()
+    bias = torch.randn(cout)
+    x = torch.randn(B, cin, *grid).to(torch.bfloat16).float()
+    gy = torch.randn(B, cout, *grid).to(torch.bfloat16).float()
+    # reference: float64 on the CPU
+    xr = x.double().requires_grad_(True)
+    wr = w.double().requires_grad_(True)
+    br = bias.double().requires_grad_(True)
+    F.conv3d(F.pad(xr, (1,) * 6, mode="circular"), wr, br).backward(gy.double())
+    # tensor cores: channels-last BF16 with padded input channels, no ReLU
+    xc = torch.nn.functional.pad(x.permute(0, 2, 3, 4, 1), (0, cin_pad - cin)).to(torch.bfloat16).cuda().contiguous()
+    xc.requires_grad_(True)
+    wc = w.cuda().requires_grad_(True)
+    bc = bias.cuda().requires_grad_(True)
+    y = _ConvFn.apply(xc, wc, bc, list(range(cin)), cin_pad, False)
+    gyc = torch.nn.functional.pad(gy.permute(0, 2, 3, 4, 1), (0, y.shape[-1] - cout)).to(torch.bfloat16).cuda()
+    y.backward(gyc)
+    torch.cuda.synchronize()
+    dx = xc.grad[..., :cin].float().cpu().permute(0, 4, 1, 2, 3).double()
+    dw, db = wc.grad.double().cpu(), bc.grad.double().cpu()
+    # FP32 accumulation of exact BF16 products: the weight and bias gradients to
+    # 1e-5 of their scale; the input gradient is a BF16 output (2^-8 relative)
+    assert float((dw - wr.grad).abs().max()) <= 1e-5 * float(wr.grad.abs().max())
+    assert float((db - br.grad).abs().max()) <= 1e-5 * float(br.grad.abs().max())
+    assert float((dx - xr.grad).abs().max()) <= 8e-3 * float(xr.grad.abs().max())
