@@ -915,6 +915,7 @@ def run_ours(args):
     sim = BatchedLFTS(p, seeds, module=L, platform="cuda" if args.precision == "fp64" else "cuda-fp32")
     M = sim.M
     tune = sim.engine.autotune()  # step implementation timed at this batch (before the first captured graph)
+    sim.engine.set_step_graph(args.step_graph == "on")
     st0 = sim.start([initial_fields(s, M) for s in seeds])
     for _ in range(args.warmup):
         sim.step()
@@ -1002,6 +1003,8 @@ def run_ours(args):
         "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
         "config": {**workload_config(R, args.nx, args.workload), "parallelism": f"replicas x{world}", "step_autotune": tune,
+                   "step_graph": ("one CUDA graph per Langevin step (saddle loop as a device-controlled WHILE node)"
+                                  if sim.engine.step_graph() else "saddle loop driven from the host"),
                    "mean_saddle_iterations": float(np.mean(iters)) if iters else None, "failed_steps": fails,
                    "initial_saddle_iterations": max(st0["iterations"])},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": R * nreal * M * 8,
@@ -1035,6 +1038,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
                     help="fp64 (the headline) or fp32 propagators with FP64 reductions (platform cuda-fp32)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--step-graph", default="on", choices=["on", "off"],
+                    help="off: drive the saddle loop from the host (one graph per iteration) instead of one graph per step")
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the fp32 / fp32_learned / one-replica FP64 forms after the headline")
     ap.add_argument("--ref-sample", type=int, default=0, help=argparse.SUPPRESS)

@@ -48,6 +48,8 @@ struct lfts_ctx_s {
     int fastN = 0;            // cubic grid handled by the compile-time specialised kernels (0: generic)
     int r8 = 0;               // 64^3: register-resident 8x8 line transforms (lfts_step_r8.cuh)
     int fast_ok = 0, r8_ok = 0, r12_ok = 0;  // families set up at creation (lfts_set_step_impl)
+    int pf = 1;               // plane kernels L2-prefetch the next wave's inputs (GridPlan::ahead)
+    int ah_r8[5] = {}, ah_r12[3] = {};  // co-resident blocks of each plane kernel (its prefetch distance)
     int r12 = 0;              // 96^3: register-resident 12x8 plane kernels (lfts_step_r12.cuh)
     int nsm = 0;              // streaming multiprocessors of the device
     int xcap = 0;             // CTAs per SM of the persistent x-passes (0: the kernel's own residency)
@@ -184,6 +186,32 @@ template <typename T> static int r8_setup(int max_smem) {
     return 1;
 }
 
+// blocks of a kernel resident on the whole device at once (0 if unknown)
+template <class K> static int resident_blocks(lfts_ctx c, K kernel, int threads, size_t smem) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return nb * c->nsm;
+}
+template <typename T> static void prefetch_distances(lfts_ctx c) {
+    using C = typename CT<T>::type;
+    if (c->r8) {
+        const size_t ps = r8::plane_smem<C>();
+        c->ah_r8[0] = resident_blocks(c, r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC>, NTHR, ps);
+        c->ah_r8[1] = resident_blocks(c, r8::kr_plane_mid<T>, NTHR, ps);
+        c->ah_r8[2] = resident_blocks(c, r8::kr_plane_inverse<T, 2, EPI_RICH>, NTHR, ps);
+        c->ah_r8[3] = resident_blocks(c, r8::kr_plane_forward<T, 1, FM_NONE, FM_NONE>, NTHR, ps);
+        c->ah_r8[4] = resident_blocks(c, r8::kr_plane_inverse<T, 1, EPI_SCALE>, NTHR, ps);
+    }
+    if (c->r12) {
+        c->ah_r12[0] = resident_blocks(c, r12::kq_plane_forward<T, FM_FAC_SQ, FM_FAC>, r12::NT, r12::plane_smem<C>(r12::N));
+        c->ah_r12[1] = resident_blocks(c, r12::kq_plane_mid<T>, r12::NT, r12::plane_smem<C>(r12::N / 2));
+        c->ah_r12[2] = resident_blocks(c, r12::kq_plane_inverse<T>, r12::NT, r12::plane_smem<C>(r12::N));
+    }
+}
+
 template <typename T> static int setup_plan(lfts_ctx c) {
     using C = typename CT<T>::type;
     GridPlan &g = c->g;
@@ -237,6 +265,7 @@ template <typename T> static int setup_plan(lfts_ctx c) {
     c->nbr2 = (int)c->sm_pf2 <= max_smem && (int)c->sm_x2 <= max_smem;
     CK((c->gen ? set_attrs_t<T, true>(max_smem) : set_attrs_t<T, false>(max_smem)));
     g.stw = nullptr;
+    g.ahead = 0;
     if (g.n0 == g.n1 && g.n1 == g.n2 && !std::getenv("LFTS_NO_FAST")) {
         const int N = g.n0;
         int ok = 0;
@@ -272,6 +301,8 @@ template <typename T> static int setup_plan(lfts_ctx c) {
             c->fast_ok = N;
             c->r8_ok = c->r8;
             c->r12_ok = c->r12;
+            prefetch_distances<T>(c);
+            if (std::getenv("LFTS_NO_L2_PREFETCH")) c->pf = 0;
         }
     }
     return 0;
@@ -596,11 +627,15 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
             const size_t ps = r8::plane_smem<C>();
             const long long it2 = (long long)nj * 2 * r8::xpipe_tiles<C>(), it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = (long long)(c->xcap ? c->xcap : 3) * c->nsm;
             const dim3 px2((unsigned)(it2 < cap ? it2 : cap)), px1((unsigned)(it1 < cap ? it1 : cap));
-            r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC><<<rp, NTHR, ps, st>>>(g, jobs, s, 0);
+            GridPlan g1 = g, g3 = g, g5 = g;
+            g1.ahead = c->pf ? c->ah_r8[0] : 0;
+            g3.ahead = c->pf ? c->ah_r8[1] : 0;
+            g5.ahead = c->pf ? c->ah_r8[2] : 0;
+            r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC><<<rp, NTHR, ps, st>>>(g1, jobs, s, 0);
             r8::kp_xpass<T, 2><<<px2, NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, 0, 1);
-            r8::kr_plane_mid<T><<<rp, NTHR, ps, st>>>(g, jobs, 1);
+            r8::kr_plane_mid<T><<<rp, NTHR, ps, st>>>(g3, jobs, 1);
             r8::kp_xpass<T, 1><<<px1, NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 1, 1, 1);
-            r8::kr_plane_inverse<T, 2, EPI_RICH><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, 0);
+            r8::kr_plane_inverse<T, 2, EPI_RICH><<<rp, NTHR, ps, st>>>(g5, jobs, s, 0, 0);
             CKLAUNCH();
             return 0;
         }
@@ -610,11 +645,15 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
             const size_t p2 = r12::plane_smem<C>(N), p1 = r12::plane_smem<C>(N / 2), xs = r12::xpipe_smem<C>();
             const long long it2 = (long long)nj * 2 * r12::XTILES, it1 = (long long)nj * r12::XTILES;
             const long long cap = (long long)(c->xcap ? c->xcap : r12::minb_xpass<T>()) * c->nsm;
-            r12::kq_plane_forward<T, FM_FAC_SQ, FM_FAC><<<gp, r12::NT, p2, st>>>(g, jobs, s, 0);
+            GridPlan g1 = g, g3 = g, g5 = g;
+            g1.ahead = c->pf ? c->ah_r12[0] : 0;
+            g3.ahead = c->pf ? c->ah_r12[1] : 0;
+            g5.ahead = c->pf ? c->ah_r12[2] : 0;
+            r12::kq_plane_forward<T, FM_FAC_SQ, FM_FAC><<<gp, r12::NT, p2, st>>>(g1, jobs, s, 0);
             r12::kq_xpass<T, 2><<<(unsigned)(it2 < cap ? it2 : cap), NTHR, xs, st>>>(g, jobs, nj, 0, 0, 1);
-            r12::kq_plane_mid<T><<<gp, r12::NT, p1, st>>>(g, jobs, 1);
+            r12::kq_plane_mid<T><<<gp, r12::NT, p1, st>>>(g3, jobs, 1);
             r12::kq_xpass<T, 1><<<(unsigned)(it1 < cap ? it1 : cap), NTHR, xs, st>>>(g, jobs, nj, 1, 1, 1);
-            r12::kq_plane_inverse<T><<<gp, r12::NT, p2, st>>>(g, jobs, s, 0);
+            r12::kq_plane_inverse<T><<<gp, r12::NT, p2, st>>>(g5, jobs, s, 0);
             CKLAUNCH();
             return 0;
         }
@@ -640,10 +679,13 @@ static int step_disc_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, 
         if (c->r8) {
             const dim3 rp(N, nj);
             const size_t ps = r8::plane_smem<C>();
-            r8::kr_plane_forward<T, 1, FM_NONE, FM_NONE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0);
+            GridPlan g1 = g, g5 = g;
+            g1.ahead = c->pf ? c->ah_r8[3] : 0;
+            g5.ahead = c->pf ? c->ah_r8[4] : 0;
+            r8::kr_plane_forward<T, 1, FM_NONE, FM_NONE><<<rp, NTHR, ps, st>>>(g1, jobs, s, 0);
             const long long it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = (long long)(c->xcap ? c->xcap : 3) * c->nsm;
             r8::kp_xpass<T, 1><<<(unsigned)(it1 < cap ? it1 : cap), NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, half, half);
-            r8::kr_plane_inverse<T, 1, EPI_SCALE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
+            r8::kr_plane_inverse<T, 1, EPI_SCALE><<<rp, NTHR, ps, st>>>(g5, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
             CKLAUNCH();
             return 0;
         }
@@ -1352,7 +1394,7 @@ extern "C" int lfts_dots_static(int precision, long long M, const lfts_dot_job *
 // the choice (and with it the last bits of the results) is stable.
 namespace {
 struct TuneCand {
-    int fastN, r8, r12, xcap;
+    int fastN, r8, r12, xcap, pf;
     const char *name;
 };
 }  // namespace
@@ -1361,18 +1403,20 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
     if (!c) return fail("null context");
     if (njobs < 1 || njobs > 65535) return fail("autotune: njobs must be 1..65535");
     if (reps < 1) reps = 5;
-    const int fastN = c->fastN, r8v = c->r8, r12v = c->r12, xcap0 = c->xcap;
+    const int fastN = c->fastN, r8v = c->r8, r12v = c->r12, xcap0 = c->xcap, pf0 = c->pf;
     std::vector<TuneCand> cands;
     if (r8v) {
-        cands.push_back({fastN, 1, 0, 0, "register-64"});
-        cands.push_back({fastN, 1, 0, 2, "register-64 xcap2"});
+        cands.push_back({fastN, 1, 0, 0, 1, "register-64"});
+        cands.push_back({fastN, 1, 0, 0, 0, "register-64 no-l2-prefetch"});
+        cands.push_back({fastN, 1, 0, 2, 1, "register-64 xcap2"});
     }
     if (r12v) {
-        cands.push_back({fastN, 0, 1, 0, "register-96"});
-        cands.push_back({fastN, 0, 1, 1, "register-96 xcap1"});
+        cands.push_back({fastN, 0, 1, 0, 1, "register-96"});
+        cands.push_back({fastN, 0, 1, 0, 0, "register-96 no-l2-prefetch"});
+        cands.push_back({fastN, 0, 1, 1, 1, "register-96 xcap1"});
     }
-    if (fastN) cands.push_back({fastN, 0, 0, 0, "cubic"});
-    cands.push_back({0, 0, 0, 0, "generic"});
+    if (fastN) cands.push_back({fastN, 0, 0, 0, 1, "cubic"});
+    cands.push_back({0, 0, 0, 0, 1, "generic"});
     const size_t sb = (size_t)c->prec, M = (size_t)c->g.M, Mc = (size_t)c->g.Mc;
     void *q = nullptr, *fac = nullptr, *bond = nullptr, *spec = nullptr, *w = nullptr;
     lfts_step_job *djobs = nullptr;
@@ -1429,6 +1473,7 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
         c->r8 = cands[k].r8;
         c->r12 = cands[k].r12;
         c->xcap = cands[k].xcap;
+        c->pf = cands[k].pf;
         for (int i = 0; i < 2 && rc == 0; i++) rc = lfts_step_continuous(c, djobs, njobs, 0);
         if (rc) break;
         CK(cudaEventRecord(e0, c->stream));
@@ -1446,6 +1491,7 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
         c->r8 = cands[best].r8;
         c->r12 = cands[best].r12;
         c->xcap = cands[best].xcap;
+        c->pf = cands[best].pf;
         char buf[96];
         for (size_t k = 0; k < cands.size(); k++) {
             std::snprintf(buf, sizeof buf, "%s%s %.4f ms", k ? "; " : "", cands[k].name, (double)ms[k]);
@@ -1458,6 +1504,7 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
         c->r8 = r8v;
         c->r12 = r12v;
         c->xcap = xcap0;
+        c->pf = pf0;
     }
     cleanup();
     if (report && report_cap) {
@@ -1469,13 +1516,17 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
 
 extern "C" int lfts_set_step_impl(lfts_ctx c, const char *name) {
     if (!c || !name) return fail("null argument");
-    const std::string n(name);
+    std::string n(name);
+    const std::string suffix = " no-l2-prefetch";
+    const bool nopf = n.size() > suffix.size() && n.compare(n.size() - suffix.size(), suffix.size(), suffix) == 0;
+    if (nopf) n.resize(n.size() - suffix.size());
     const int fastN = c->fast_ok;
     auto set = [&](int f, int r8, int r12) {
         c->fastN = f;
         c->r8 = r8;
         c->r12 = r12;
         c->xcap = 0;
+        c->pf = nopf ? 0 : 1;
         return 0;
     };
     if (n == "register-64" && c->r8_ok) return set(fastN, 1, 0);
@@ -1490,6 +1541,7 @@ extern "C" int lfts_step_impl(lfts_ctx c, char *name, size_t cap) {
     std::string n = c->r8 ? (c->xcap ? "register-64 xcap" + std::to_string(c->xcap) : std::string("register-64"))
                   : c->r12 ? (c->xcap ? "register-96 xcap" + std::to_string(c->xcap) : std::string("register-96"))
                   : c->fastN ? std::string("cubic") : std::string("generic");
+    if ((c->r8 || c->r12) && !c->pf) n += " no-l2-prefetch";
     std::strncpy(name, n.c_str(), cap - 1);
     name[cap - 1] = 0;
     return 0;

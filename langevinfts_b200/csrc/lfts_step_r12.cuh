@@ -16,7 +16,12 @@
 // X[k] = sum_n x[n] exp(SIGN 2 pi i n k / 96) in both.
 // The exchange slot of (k2, j) is 8 k2 + ((j + k2) & 7): the writes (fixed k2)
 // and the reads (fixed j) of a lane group each touch eight banks, in a row and
-// down a column of row stride 97 alike.
+// down a column alike.  Plane positions go through PlaneLayout96: FP64
+// (16-byte complex, one lane group per wavefront) uses rows of stride 97;
+// FP32 (8-byte complex, two groups per wavefront) uses rows of 96 with
+// position p at p XOR 8 (row parity) XOR (row AND 6), which keeps the two
+// groups of a wavefront apart as well (43 % fewer shared-memory wavefronts
+// than stride 97 with 8-byte elements, per a count of the kernels' patterns).
 //
 // Plane kernels run 48 lane groups (384 threads) per CTA.  K1 and K5 keep one
 // x-plane of packed z-lines (both branches as real / imaginary part, 96 rows of
@@ -29,10 +34,20 @@ namespace lfts {
 namespace r12 {
 
 constexpr int N = 96, NZC = N / 2 + 1, PLANE = N * NZC;
-constexpr int S = 97;  // plane row stride (complex elements)
 constexpr int GROUPS = 48, NT = 8 * GROUPS;
 
-template <typename C> constexpr size_t plane_smem(int rows) { return sizeof(C) * (size_t)rows * S; }
+template <typename C> struct PlaneLayout96;
+template <> struct PlaneLayout96<double2> {
+    static constexpr int RS = 97;
+    __device__ __forceinline__ static int at(int r, int p) { return r * RS + p; }
+};
+template <> struct PlaneLayout96<float2> {
+    static constexpr int RS = 96;
+    __device__ __forceinline__ static int at(int r, int p) { return r * RS + (p ^ ((r & 1) << 3) ^ (r & 6)); }
+};
+// index of position p of row r of a plane in shared memory
+template <typename C> __device__ __forceinline__ int at(int r, int p) { return PlaneLayout96<C>::at(r, p); }
+template <typename C> constexpr size_t plane_smem(int rows) { return sizeof(C) * (size_t)rows * PlaneLayout96<C>::RS; }
 
 __device__ __forceinline__ int slot(int k2, int j) { return 8 * k2 + ((j + k2) & 7); }
 
@@ -48,19 +63,24 @@ __device__ __forceinline__ C tw96(int e, int sign) {
 }
 
 // exchange spaces: position p of a 96-slot line
-template <typename C> struct Row {  // a plane row
-    C *b;
-    __device__ __forceinline__ C &at(int p) const { return b[p]; }
-    __device__ __forceinline__ C &ref(int k2, int j) const { return b[slot(k2, j)]; }
-};
-template <typename C> struct Col {  // a column of a 96-row plane
-    C *b;
-    __device__ __forceinline__ C &at(int p) const { return b[p * S]; }
+template <typename C> struct Row {  // row r of plane P
+    C *P;
+    int r;
+    __device__ __forceinline__ C &at(int p) const { return P[lfts::r12::at<C>(r, p)]; }
     __device__ __forceinline__ C &ref(int k2, int j) const { return at(slot(k2, j)); }
 };
-template <typename C> struct Col2 {  // two columns of a 48-row plane (positions 0..47, 48..95)
-    C *b0, *b1;
-    __device__ __forceinline__ C &at(int p) const { return p < N / 2 ? b0[p * S] : b1[(p - N / 2) * S]; }
+template <typename C> struct Col {  // column c of a 96-row plane P
+    C *P;
+    int c;
+    __device__ __forceinline__ C &at(int p) const { return P[lfts::r12::at<C>(p, c)]; }
+    __device__ __forceinline__ C &ref(int k2, int j) const { return at(slot(k2, j)); }
+};
+template <typename C> struct Col2 {  // columns c0, c1 of a 48-row plane P (positions 0..47, 48..95)
+    C *P;
+    int c0, c1;
+    __device__ __forceinline__ C &at(int p) const {
+        return p < N / 2 ? P[lfts::r12::at<C>(p, c0)] : P[lfts::r12::at<C>(p - N / 2, c1)];
+    }
     __device__ __forceinline__ C &ref(int k2, int j) const { return at(slot(k2, j)); }
 };
 
@@ -211,22 +231,22 @@ __device__ __forceinline__ void put_columns(C *st, const AT &xs, int kz, const C
 // Write A + i B of row y at columns kz and kc = 96 - kz of a packed plane
 // (Hermitian extension); task 0 carries (DC, Nyquist) in (x, y) of A and B.
 template <typename C>
-__device__ __forceinline__ void put_packed(C *row, int kz, int kc, C A, C B) {
+__device__ __forceinline__ void put_packed(C *P, int y, int kz, int kc, C A, C B) {
     C z;
     if (kz != 0) {
         z.x = A.x - B.y;
         z.y = A.y + B.x;
-        row[kz] = z;
+        P[at<C>(y, kz)] = z;
         z.x = A.x + B.y;
         z.y = -A.y + B.x;
-        row[kc] = z;
+        P[at<C>(y, kc)] = z;
     } else {
         z.x = A.x;
         z.y = B.x;
-        row[0] = z;
+        P[at<C>(y, 0)] = z;
         z.x = A.y;
         z.y = B.y;
-        row[N / 2] = z;
+        P[at<C>(y, N / 2)] = z;
     }
 }
 
@@ -244,6 +264,7 @@ __global__ void __launch_bounds__(NT, minb_two_branch<T>()) kq_plane_forward(Gri
     constexpr int fm0 = FM0, fm1 = FM1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;
+    prefetch_next_plane<T>(g, jobs, s, true, true, 0, 0);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, j = lane & 7, grp = tid >> 3;
@@ -271,12 +292,12 @@ __global__ void __launch_bounds__(NT, minb_two_branch<T>()) kq_plane_forward(Gri
             a[m].y = qv[m] * f1;
         }
         C o0[8], o1[8];
-        fft96a<-1>(a, Row<C>{P + y * S}, j, wf, mask, o0, o1);
+        fft96a<-1>(a, Row<C>{P, y}, j, wf, mask, o0, o1);
 #pragma unroll
-        for (int k = 0; k < 8; k++) P[y * S + j + 12 * k] = o0[k];
+        for (int k = 0; k < 8; k++) P[at<C>(y, j + 12 * k)] = o0[k];
         if (j < 4) {
 #pragma unroll
-            for (int k = 0; k < 8; k++) P[y * S + 8 + j + 12 * k] = o1[k];
+            for (int k = 0; k < 8; k++) P[at<C>(y, 8 + j + 12 * k)] = o1[k];
         }
     }
     __syncthreads();
@@ -287,7 +308,7 @@ __global__ void __launch_bounds__(NT, minb_two_branch<T>()) kq_plane_forward(Gri
 #pragma unroll
     for (int m = 0; m < 12; m++) {
         const int y = j + 8 * m;
-        const C zk = P[y * S + kz], zc = P[y * S + kc];
+        const C zk = P[at<C>(y, kz)], zc = P[at<C>(y, kc)];
         C b;
         if (kz != 0) {
             split_pair(zk, cconj(zc), A[m], b);
@@ -297,17 +318,17 @@ __global__ void __launch_bounds__(NT, minb_two_branch<T>()) kq_plane_forward(Gri
             b.x = zk.y;  // branch 1
             b.y = zc.y;
         }
-        P[y * S + kc] = b;
+        P[at<C>(y, kc)] = b;
     }
     __syncwarp(mask);
     C o0[8], o1[8];
-    fft96a<-1>(A, Col<C>{P + kz}, j, wf, mask, o0, o1);
-    put_columns(out, Col<C>{P + kz}, kz, o0, o1, j, mask);
+    fft96a<-1>(A, Col<C>{P, kz}, j, wf, mask, o0, o1);
+    put_columns(out, Col<C>{P, kz}, kz, o0, o1, j, mask);
 #pragma unroll
-    for (int m = 0; m < 12; m++) A[m] = P[(j + 8 * m) * S + kc];
+    for (int m = 0; m < 12; m++) A[m] = P[at<C>(j + 8 * m, kc)];
     __syncwarp(mask);
-    fft96a<-1>(A, Col<C>{P + kc}, j, wf, mask, o0, o1);
-    put_columns(out + g.Mc, Col<C>{P + kc}, kz, o0, o1, j, mask);
+    fft96a<-1>(A, Col<C>{P, kc}, j, wf, mask, o0, o1);
+    put_columns(out + g.Mc, Col<C>{P, kc}, kz, o0, o1, j, mask);
 }
 
 // ------------------------------------------------------------------------
@@ -317,6 +338,7 @@ __global__ void __launch_bounds__(NT, minb_mid<T>()) kq_plane_mid(GridPlan g, co
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;  // 48 packed rows: z-line u = row u + i row (u + 48)
+    prefetch_next_plane<T>(g, jobs, 0, false, true, spec_idx, 1);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, j = lane & 7, grp = tid >> 3;
@@ -328,12 +350,12 @@ __global__ void __launch_bounds__(NT, minb_mid<T>()) kq_plane_mid(GridPlan g, co
         // inverse y: lane t ends with rows t + 12k; rows u and u + 48 are k and k + 4
         C a[12], o0[8], o1[8];
         get_columns(sp, kz, a, j);
-        fft96a<+1>(a, Col2<C>{P + kz, P + kc}, j, tw96<C>(j, +1), mask, o0, o1);
+        fft96a<+1>(a, Col2<C>{P, kz, kc}, j, tw96<C>(j, +1), mask, o0, o1);
 #pragma unroll
-        for (int k = 0; k < 4; k++) put_packed(P + (j + 12 * k) * S, kz, kc, o0[k], o0[k + 4]);
+        for (int k = 0; k < 4; k++) put_packed(P, j + 12 * k, kz, kc, o0[k], o0[k + 4]);
         if (j < 4) {
 #pragma unroll
-            for (int k = 0; k < 4; k++) put_packed(P + (8 + j + 12 * k) * S, kz, kc, o1[k], o1[k + 4]);
+            for (int k = 0; k < 4; k++) put_packed(P, 8 + j + 12 * k, kz, kc, o1[k], o1[k + 4]);
         }
     }
     __syncthreads();
@@ -355,9 +377,9 @@ __global__ void __launch_bounds__(NT, minb_mid<T>()) kq_plane_mid(GridPlan g, co
         }
         C a[12], o0[8], o1[8];
 #pragma unroll
-        for (int m = 0; m < 12; m++) a[m] = P[u * S + j + 8 * m];
+        for (int m = 0; m < 12; m++) a[m] = P[at<C>(u, j + 8 * m)];
         __syncwarp(mask);
-        fft96a<+1>(a, Row<C>{P + u * S}, j, tw96<C>(j, +1), mask, o0, o1);
+        fft96a<+1>(a, Row<C>{P, u}, j, tw96<C>(j, +1), mask, o0, o1);
 #pragma unroll
         for (int k = 0; k < 8; k++) {
             o0[k].x *= ea0[k] * ea0[k];
@@ -370,9 +392,9 @@ __global__ void __launch_bounds__(NT, minb_mid<T>()) kq_plane_mid(GridPlan g, co
                 o1[k].y *= eb1[k] * eb1[k];
             }
         }
-        fft96b<-1>(o0, o1, Row<C>{P + u * S}, j, tw96<C>(j, -1), tw96<C>(8 + j, -1), mask, a);
+        fft96b<-1>(o0, o1, Row<C>{P, u}, j, tw96<C>(j, -1), tw96<C>(8 + j, -1), mask, a);
 #pragma unroll
-        for (int k = 0; k < 12; k++) P[u * S + j + 8 * k] = a[k];
+        for (int k = 0; k < 12; k++) P[at<C>(u, j + 8 * k)] = a[k];
     }
     __syncthreads();
     {
@@ -380,11 +402,11 @@ __global__ void __launch_bounds__(NT, minb_mid<T>()) kq_plane_mid(GridPlan g, co
         C c[12];
 #pragma unroll
         for (int m = 0; m < 6; m++) {
-            const C *row = P + (j + 8 * m) * S;
+            const int u = j + 8 * m;
             if (kz != 0) {
-                split_pair(row[kz], cconj(row[kc]), c[m], c[m + 6]);
+                split_pair(P[at<C>(u, kz)], cconj(P[at<C>(u, kc)]), c[m], c[m + 6]);
             } else {
-                const C z0 = row[0], z48 = row[N / 2];
+                const C z0 = P[at<C>(u, 0)], z48 = P[at<C>(u, N / 2)];
                 c[m].x = z0.x;  // row u: DC + i Nyquist
                 c[m].y = z48.x;
                 c[m + 6].x = z0.y;  // row u + 48
@@ -393,8 +415,8 @@ __global__ void __launch_bounds__(NT, minb_mid<T>()) kq_plane_mid(GridPlan g, co
         }
         __syncwarp(mask);
         C o0[8], o1[8];
-        fft96a<-1>(c, Col2<C>{P + kz, P + kc}, j, tw96<C>(j, -1), mask, o0, o1);
-        put_columns(sp, Col2<C>{P + kz, P + kc}, kz, o0, o1, j, mask);
+        fft96a<-1>(c, Col2<C>{P, kz, kc}, j, tw96<C>(j, -1), mask, o0, o1);
+        put_columns(sp, Col2<C>{P, kz, kc}, kz, o0, o1, j, mask);
     }
 }
 
@@ -407,6 +429,7 @@ __global__ void __launch_bounds__(NT, minb_two_branch<T>()) kq_plane_inverse(Gri
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;
+    prefetch_next_plane<T>(g, jobs, 0, false, true, spec_in0, 2);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, j = lane & 7, grp = tid >> 3;
@@ -423,25 +446,25 @@ __global__ void __launch_bounds__(NT, minb_two_branch<T>()) kq_plane_inverse(Gri
         const int kz = grp, kc = kz == 0 ? N / 2 : N - kz;
         C A[12], o0[8], o1[8];
         get_columns(in, kz, A, j);
-        fft96a<+1>(A, Col<C>{P + kz}, j, wi, mask, o0, o1);
+        fft96a<+1>(A, Col<C>{P, kz}, j, wi, mask, o0, o1);
 #pragma unroll
-        for (int k = 0; k < 8; k++) P[(j + 12 * k) * S + kz] = o0[k];
+        for (int k = 0; k < 8; k++) P[at<C>(j + 12 * k, kz)] = o0[k];
         if (j < 4) {
 #pragma unroll
-            for (int k = 0; k < 8; k++) P[(8 + j + 12 * k) * S + kz] = o1[k];
+            for (int k = 0; k < 8; k++) P[at<C>(8 + j + 12 * k, kz)] = o1[k];
         }
         get_columns(in + g.Mc, kz, A, j);
-        fft96a<+1>(A, Col<C>{P + kc}, j, wi, mask, o0, o1);
+        fft96a<+1>(A, Col<C>{P, kc}, j, wi, mask, o0, o1);
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-            C *row = P + (j + 12 * k) * S;
-            put_packed(row, kz, kc, row[kz], o0[k]);
+            const int y = j + 12 * k;
+            put_packed(P, y, kz, kc, P[at<C>(y, kz)], o0[k]);
         }
         if (j < 4) {
 #pragma unroll
             for (int k = 0; k < 8; k++) {
-                C *row = P + (8 + j + 12 * k) * S;
-                put_packed(row, kz, kc, row[kz], o1[k]);
+                const int y = 8 + j + 12 * k;
+                put_packed(P, y, kz, kc, P[at<C>(y, kz)], o1[k]);
             }
         }
     }
@@ -458,9 +481,9 @@ __global__ void __launch_bounds__(NT, minb_two_branch<T>()) kq_plane_inverse(Gri
         }
         C a[12], o0[8], o1[8];
 #pragma unroll
-        for (int m = 0; m < 12; m++) a[m] = P[y * S + j + 8 * m];
+        for (int m = 0; m < 12; m++) a[m] = P[at<C>(y, j + 8 * m)];
         __syncwarp(mask);
-        fft96a<+1>(a, Row<C>{P + y * S}, j, wi, mask, o0, o1);
+        fft96a<+1>(a, Row<C>{P, y}, j, wi, mask, o0, o1);
 #pragma unroll
         for (int k = 0; k < 8; k++) qrow[j + 12 * k] = ((T)4 * e0[k] * o0[k].y - e0[k] * e0[k] * o0[k].x) * THIRD;
         if (j < 4) {
