@@ -892,6 +892,43 @@ def roofline_step_kernel(nx, njobs, reps=20, prec=8, impl=None):
     return ms, M, Mc
 
 
+def time_realspace_step(nx, njobs, reps=20, bc=("absorbing", "absorbing", "reflecting", "reflecting", "periodic", "periodic")):
+    """CUDA-event time of one lfts_step_realspace call at njobs jobs of an nx^3
+    FP64 box with the given walls; returns (ms, M)."""
+    import torch
+    from langevinfts_b200.capi import Context, StepJob, check
+    ctx = Context([nx] * 3, precision=8)
+    M = ctx.M
+    codes = {"periodic": 0, "reflecting": 1, "absorbing": 2}
+    tab = np.zeros(ctx.lib.lfts_realspace_table_size(ctx.h))
+    check(ctx.lib.lfts_realspace_tables(ctx.h, 1.0, 1 / 90, 3, (C.c_double * 3)(*[7.3 / nx] * 3),
+                                        (C.c_int * 6)(*[codes[b] for b in bc]), tab.ctypes.data))
+    tdev = ctx.upload(tab)
+    fac = ctx.malloc(njobs * M * 8)
+    check(ctx.lib.lfts_field_factors_batch(ctx.h, ctx.upload(np.random.default_rng(0).normal(0, 1, njobs * M)), -1 / 360, fac,
+                                           njobs))
+    q = ctx.malloc(njobs * 2 * M * 8)
+    for j in range(njobs):
+        ctx.h2d(q + j * 2 * M * 8, np.ones(M))
+    spec = ctx.malloc(njobs * 2 * M * 8)
+    jobs = (StepJob * njobs)(*[StepJob(q + j * 2 * M * 8, 0, q + (j * 2 + 1) * M * 8, 0, fac + j * M * 8, tdev, None,
+                                       spec + j * 2 * M * 8, None, 0, 0) for j in range(njobs)])
+    jp = ctx.upload(np.frombuffer(jobs, dtype=np.uint8))
+    stream = torch.cuda.ExternalStream(ctx.lib.lfts_ctx_stream(ctx.h))
+    for _ in range(3):
+        check(ctx.lib.lfts_step_realspace(ctx.h, jp, njobs, 0, 3))
+    ctx.sync()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    for _ in range(reps):
+        check(ctx.lib.lfts_step_realspace(ctx.h, jp, njobs, 0, 3))
+    ev[1].record(stream)
+    ev[1].synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / reps
+    ctx.close()
+    return ms, M
+
+
 def run_ours(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1062,6 +1099,8 @@ def main():
     ap.add_argument("--threads", type=int, default=1, help=argparse.SUPPRESS)
     ap.add_argument("--step-impl", default=None,
                     help="with --kernel-only: the step implementation to time (default: the context's own choice)")
+    ap.add_argument("--realspace", action="store_true",
+                    help="with --kernel-only: time the real-space Crank-Nicolson step (lfts_step_realspace) instead")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only time the fused continuous step at 2*replicas jobs (for profiling)")
     args = ap.parse_args()
@@ -1089,6 +1128,16 @@ def main():
         return run_ensemble(args)
     if args.warmup < 3:
         args.warmup = 3
+    if args.kernel_only and args.realspace:
+        import torch
+        torch.cuda.init()
+        ms, M = time_realspace_step(args.nx, 2 * args.replicas, reps=args.steps)
+        # compulsory bytes per job: q in, q out, the factors (8 B each) and the
+        # two intermediate sweeps written and read once (4 x 8 B)
+        unit = 8 * 7 * M
+        print(json.dumps({"kernel": "lfts_step_realspace", "jobs": 2 * args.replicas, "nx": args.nx, "launch_ms": ms,
+                          "bytes_per_job": unit, "GBps": 2 * args.replicas * unit / (ms * 1e-3) / 1e9}))
+        return 0
     if args.kernel_only:
         import torch
         torch.cuda.init()

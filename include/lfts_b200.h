@@ -49,6 +49,12 @@ const char *lfts_last_error(void);
 
 int lfts_malloc(lfts_ctx ctx, void **ptr, size_t bytes);
 int lfts_free(lfts_ctx ctx, void *ptr);
+/* Pinned host memory mapped into the device's address space (the same
+ * address on both sides): kernels read and write it in place over the host
+ * link.  The propagator slices of the reduce-memory mode live there.  Free
+ * with lfts_free_host. */
+int lfts_malloc_host(lfts_ctx ctx, void **ptr, size_t bytes);
+int lfts_free_host(lfts_ctx ctx, void *ptr);
 int lfts_memset_async(lfts_ctx ctx, void *ptr, int value, size_t bytes);
 /* Blocking copies (used by the host wrapper for numpy inputs/outputs). */
 int lfts_memcpy_h2d(lfts_ctx ctx, void *dst, const void *src, size_t bytes);
@@ -131,6 +137,36 @@ typedef struct {
  * CudaSolverPseudo::advance_propagator_continuous (CudaSolverPseudo.cu:345-412)
  * and CpuSolverPseudo::advance_propagator_continuous (CpuSolverPseudo.cpp:120-188). */
 int lfts_step_continuous(lfts_ctx ctx, const lfts_step_job *jobs, int njobs, int s);
+/* ---- real-space solver (continuous chains) ------------------------------- */
+
+/* Tables of the real-space Crank-Nicolson step for one monomer type, on the
+ * host, in DOUBLES: for each padded axis a = 0, 1, 2 (extent n_a; 1D and 2D
+ * boxes pad to 3D with leading extents of 1, the box's axis d being padded
+ * axis 3 - dim + d) seven rows of n_a values: the tridiagonal coefficients
+ * l, d, h of src/common/FiniteDifference.cpp:6-101 (off-diagonals -b^2 ds /
+ * (12 dx^2), diagonal 1 + b^2 ds / (6 dx^2); at a reflecting side the outer
+ * off-diagonal folds into the diagonal, at an absorbing side it is dropped),
+ * then the Thomas pivots p, the ratios c = h / p and, for a periodic axis,
+ * the Sherman-Morrison vector v of CpuSolverReal.cpp:480-549, and 1 / p: seven rows
+ * (tridiagonal_periodic, :509-549), in the reference's operation order; after the
+ * three axes, the periodic denominators 1 + v[0] + l[0] v[n-1] (3 values) and
+ * the periodic flags (3 values, 1.0 or 0.0).  bc: 2 * dim codes (0 periodic,
+ * 1 reflecting, 2 absorbing), lower side first; dx: dim spacings.  Size in
+ * doubles: lfts_realspace_table_size.  No counterpart in the reference (its
+ * solver recomputes the pivots on every line). */
+long long lfts_realspace_table_size(lfts_ctx ctx);
+int lfts_realspace_tables(lfts_ctx ctx, double b2, double ds, int dim, const double *dx, const int *bc, double *tables_host);
+/* One real-space Crank-Nicolson step of each job (CpuSolverReal.cpp:135-478,
+ * CudaSolverReal.cu:371-407, continuous chains, FP64 contexts):
+ * q_out = e ADI(e q_in), e = fac^2 = exp(-w ds/2) (fac holds exp(-w ds/4) as
+ * for the pseudo-spectral step), ADI = the alternating-direction sweeps of
+ * the reference (the first implicit in the box's first axis with the full
+ * explicit operator on the right, then one implicit sweep per further axis).
+ * jobs[j].bond: the job's device copy of its type's tables; jobs[j].spec:
+ * 2 * M doubles of scratch; in/out/in_stride/out_stride/active as for
+ * lfts_step_continuous (step index s).  dim: the box's dimension (1..3). */
+int lfts_step_realspace(lfts_ctx ctx, const lfts_step_job *jobs, int njobs, int s, int dim);
+
 /* Step autotuner (no counterpart in the reference, whose cuFFT plans are fixed):
  * times lfts_step_continuous for every implementation this grid supports
  * (register-resident line transforms at 64^3 / 96^3 with their x-pass CTA

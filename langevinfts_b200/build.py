@@ -24,7 +24,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["lfts_engine.cu", "lfts_langevin.cu"]
 HOST_SOURCES = ["lfts_host.cpp", "lfts_computation.cpp", "lfts_langevin_host.cpp", "lfts_scft_host.cpp", "lfts_pybind.cpp"]
-HEADERS = ["lfts_fft.cuh", "lfts_step_kernels.cuh", "lfts_step_fast.cuh", "lfts_step_r8.cuh", "lfts_step_r12.cuh", "lfts_unet.cuh", "lfts_bulk.cuh", "lfts_host.h", "lfts_computation.h", "lfts_langevin.h", "lfts_scft.h"]
+HEADERS = ["lfts_fft.cuh", "lfts_step_kernels.cuh", "lfts_step_fast.cuh", "lfts_step_r8.cuh", "lfts_step_r12.cuh", "lfts_realspace.cuh", "lfts_unet.cuh", "lfts_bulk.cuh", "lfts_host.h", "lfts_computation.h", "lfts_langevin.h", "lfts_scft.h"]
 
 ENGINE = os.path.join(HERE, "liblfts_b200.so")
 MODULE = os.path.join(HERE, "langevinfts" + sysconfig.get_config_var("EXT_SUFFIX"))

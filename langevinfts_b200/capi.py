@@ -43,6 +43,8 @@ _SIGS = {
     "lfts_ctx_info": [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_int)],
     "lfts_malloc": [C.c_void_p, C.POINTER(C.c_void_p), C.c_size_t],
     "lfts_free": [C.c_void_p, C.c_void_p],
+    "lfts_malloc_host": [C.c_void_p, C.POINTER(C.c_void_p), C.c_size_t],
+    "lfts_free_host": [C.c_void_p, C.c_void_p],
     "lfts_memset_async": [C.c_void_p, C.c_void_p, C.c_int, C.c_size_t],
     "lfts_memcpy_h2d": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t],
     "lfts_memcpy_d2h": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t],
@@ -97,6 +99,8 @@ _SIGS = {
     "lfts_status_wait": [C.c_void_p, C.c_int, C.c_void_p],
     "lfts_autotune": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_size_t],
     "lfts_step_impl": [C.c_void_p, C.c_char_p, C.c_size_t],
+    "lfts_realspace_tables": [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p],
+    "lfts_step_realspace": [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int],
     "lfts_set_step_impl": [C.c_void_p, C.c_char_p],
     "lfts_graph_while_begin": [C.c_void_p, C.POINTER(C.c_ulonglong)],
     "lfts_graph_while_end": [C.c_void_p],
@@ -135,13 +139,15 @@ def lib():
         L.lfts_ctx_stream.argtypes = [C.c_void_p]
         L.lfts_ctx_launches.restype = C.c_longlong
         L.lfts_ctx_launches.argtypes = [C.c_void_p]
+        L.lfts_realspace_table_size.restype = C.c_longlong
+        L.lfts_realspace_table_size.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
 
 def declared_symbols():
     """Names of every entry point declared in include/lfts_b200.h."""
-    return list(_SIGS) + ["lfts_last_error", "lfts_ctx_stream", "lfts_ctx_launches"]
+    return list(_SIGS) + ["lfts_last_error", "lfts_ctx_stream", "lfts_ctx_launches", "lfts_realspace_table_size"]
 
 
 def check(rc):

@@ -76,17 +76,4 @@ __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.w
 // make this thread's generic-proxy shared-memory writes visible to bulk copies
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// Bring [p, p + bytes) into L2 without waiting for it (a hint: no completion,
-// no effect on results).  Chunk c (32 KB each) is issued by thread first + c;
-// ranges that are not 16-byte aligned are skipped.
-__device__ __forceinline__ void prefetch_l2_range(const void *p, uint32_t bytes, int first) {
-    const int t = (int)threadIdx.x - first;
-    if (!p || t < 0) return;
-    const uint32_t off = (uint32_t)t * 32768u;
-    if (off >= bytes) return;
-    const uint32_t n = bytes - off < 32768u ? bytes - off : 32768u;
-    if ((((uintptr_t)p + off) | n) & 15) return;
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((const char *)p + off), "r"(n) : "memory");
-}
-
 }  // namespace lfts

@@ -25,10 +25,21 @@ void DevBuf::alloc(lfts_ctx c, size_t bytes) {
     n_ = bytes;
     check_rc(lfts_malloc(c, &p_, bytes));
 }
+void DevBuf::alloc_host(lfts_ctx c, size_t bytes) {
+    release();
+    ctx_ = c;
+    n_ = bytes;
+    check_rc(lfts_malloc_host(c, &p_, bytes));
+    host_ = true;
+}
 void DevBuf::release() {
-    if (p_ && ctx_) lfts_free(ctx_, p_);
+    if (p_ && ctx_) {
+        if (host_) lfts_free_host(ctx_, p_);
+        else lfts_free(ctx_, p_);
+    }
     p_ = nullptr;
     n_ = 0;
+    host_ = false;
 }
 
 static std::vector<double> simpson(int N) {
@@ -61,13 +72,23 @@ static size_t arena_push(std::vector<unsigned char> &a, const std::vector<T> &v)
 }
 
 GpuComputation::GpuComputation(ComputationBox *cb, Molecules *mol, PropagatorAnalyzer *pa, int precision, int device,
-                               int n_replicas)
+                               int n_replicas, const std::string &method, bool reduce_memory)
     : cb_(cb), mol_(mol), pa_(pa), prec_(precision), R_(n_replicas), esz_(precision) {
     if (!cb || !mol || !pa) LFTS_THROW("null ComputationBox, Molecules or PropagatorAnalyzer");
     if (n_replicas < 1) LFTS_THROW("n_replicas must be positive");
     if (pa->get_computation_propagators().empty()) LFTS_THROW("There is no propagator code. Add polymers first.");
     if (pa->get_computation_blocks().empty()) LFTS_THROW("There is no block. Add polymers first.");
     continuous_ = mol->get_model_name() == "continuous";
+    if (method == "realspace") {
+        // src/platforms/cpu/MklFactory.cpp:62-80, CpuSolverReal.cpp:15-16
+        if (!continuous_) LFTS_THROW("The real-space solver does not support discrete chain model.");
+        if (precision != 8) LFTS_THROW("The real-space solver runs in FP64 (platform \"cuda\") only.");
+        realspace_ = true;
+    } else if (method != "pseudospectral") {
+        LFTS_THROW("unknown propagator method " + method);
+    } else if (!cb->is_periodic()) {
+        LFTS_THROW("Currently, pseudo-spectral method only supports periodic boundary conditions");  // Pseudo.cpp:49-50
+    }
     const std::vector<int> nx = cb->get_nx();
     check_rc(lfts_ctx_create(&ctx_, device, (int)nx.size(), nx.data(), precision));
     check_rc(lfts_ctx_info(ctx_, &M_, &Mc_, nullptr));
@@ -78,17 +99,21 @@ GpuComputation::GpuComputation(ComputationBox *cb, Molecules *mol, PropagatorAna
         TypeStore &t = types_[kv.first];
         t.w.alloc(ctx_, sizeof(double) * RM);
         t.fac.alloc(ctx_, esz_ * RM);
-        t.bond.alloc(ctx_, esz_ * Mc_);
+        t.bond.alloc(ctx_, std::max<size_t>(esz_ * Mc_, sizeof(double) * (size_t)lfts_realspace_table_size(ctx_)));
         t.bond_half.alloc(ctx_, esz_ * Mc_);
         phi_type_[kv.first].alloc(ctx_, sizeof(double) * RM);
     }
     for (const auto &it : pa->get_computation_propagators()) {
         KeyStore &ks = keys_[it.first];
-        ks.q.alloc(ctx_, esz_ * RM * (it.second.max_n_segment + 1));
+        auto slices = [&](DevBuf &b, size_t bytes) {
+            if (reduce_memory) b.alloc_host(ctx_, bytes);
+            else b.alloc(ctx_, bytes);
+        };
+        slices(ks.q, esz_ * RM * (it.second.max_n_segment + 1));
         if (!continuous_) {
-            if (!it.second.deps.empty()) ks.half[0].alloc(ctx_, esz_ * RM);
+            if (!it.second.deps.empty()) slices(ks.half[0], esz_ * RM);
             for (int n : it.second.junction_ends)
-                if (n >= 1 && n <= it.second.max_n_segment && !ks.half.count(n)) ks.half[n].alloc(ctx_, esz_ * RM);
+                if (n >= 1 && n <= it.second.max_n_segment && !ks.half.count(n)) slices(ks.half[n], esz_ * RM);
         }
         if (it.first[0] == '{') {
             const std::string name = code::q_input_from_key(it.first);
@@ -457,11 +482,22 @@ void GpuComputation::build_stress_jobs() {
 
 void GpuComputation::update_laplacian_operator() {
     const std::vector<double> lx = cb_->get_lx();
-    for (const auto &kv : mol_->get_bond_lengths()) {
-        TypeStore &t = types_.at(kv.first);
-        check_rc(lfts_bond_tables(ctx_, kv.second * kv.second, mol_->get_ds(), lx.data(), t.bond.get(), t.bond_half.get()));
+    if (realspace_) {
+        // Crank-Nicolson tables of every monomer type (CpuSolverReal.cpp:86-106)
+        const std::vector<double> dx = cb_->get_dx();
+        std::vector<double> tab((size_t)lfts_realspace_table_size(ctx_));
+        for (const auto &kv : mol_->get_bond_lengths()) {
+            check_rc(lfts_realspace_tables(ctx_, kv.second * kv.second, mol_->get_ds(), cb_->get_dim(), dx.data(),
+                                           cb_->get_boundary_conditions().data(), tab.data()));
+            check_rc(lfts_memcpy_h2d(ctx_, types_.at(kv.first).bond.get(), tab.data(), sizeof(double) * tab.size()));
+        }
+    } else {
+        for (const auto &kv : mol_->get_bond_lengths()) {
+            TypeStore &t = types_.at(kv.first);
+            check_rc(lfts_bond_tables(ctx_, kv.second * kv.second, mol_->get_ds(), lx.data(), t.bond.get(), t.bond_half.get()));
+        }
+        check_rc(lfts_fourier_basis(ctx_, lx.data(), basis_.as<double>()));
     }
-    check_rc(lfts_fourier_basis(ctx_, lx.data(), basis_.as<double>()));
     // partition scale dv / (n_aggregated V): n_aggregated is structural, dv and V follow the box
     const auto *jobs = (const lfts_dot_job *)(arena_host_.data() + dot_jobs_);
     std::vector<lfts_dot_job> dj(jobs, jobs + n_dot_jobs_);
@@ -496,8 +532,12 @@ void GpuComputation::enqueue_propagation() {
                                         (const void *const *)(base + L.deps), (const double *)(base + L.wts)));
                 break;
             case 1:
-                for (int s = 0; s < L.nsteps; s++)
-                    check_rc(lfts_step_continuous(ctx_, (const lfts_step_job *)(base + L.jobs), L.njobs, s));
+                for (int s = 0; s < L.nsteps; s++) {
+                    if (realspace_)
+                        check_rc(lfts_step_realspace(ctx_, (const lfts_step_job *)(base + L.jobs), L.njobs, s, cb_->get_dim()));
+                    else
+                        check_rc(lfts_step_continuous(ctx_, (const lfts_step_job *)(base + L.jobs), L.njobs, s));
+                }
                 break;
             case 2:
                 for (int s = 0; s < L.nsteps; s++)
@@ -728,6 +768,7 @@ void GpuComputation::get_solvent_concentration(int s, double *phi) {
 }
 
 void GpuComputation::compute_stress() {
+    if (realspace_) LFTS_THROW("Currently, the real-space method does not support stress computation.");  // CpuSolverReal.cpp:460-476
     if (!have_propagators_) LFTS_THROW("compute_propagators must be called before compute_stress");
     const int DIM = cb_->get_dim();
     const int P = mol_->get_n_polymer_types();

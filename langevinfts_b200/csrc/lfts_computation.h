@@ -27,8 +27,10 @@ class DevBuf {
     ~DevBuf() { release(); }
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
-    DevBuf(DevBuf &&o) noexcept : ctx_(o.ctx_), p_(o.p_), n_(o.n_) { o.p_ = nullptr; }
+    DevBuf(DevBuf &&o) noexcept : ctx_(o.ctx_), p_(o.p_), n_(o.n_), host_(o.host_) { o.p_ = nullptr; }
     void alloc(lfts_ctx c, size_t bytes);
+    // pinned host memory mapped into the device (lfts_malloc_host)
+    void alloc_host(lfts_ctx c, size_t bytes);
     void release();
     void *get() const { return p_; }
     size_t size() const { return n_; }
@@ -38,14 +40,22 @@ class DevBuf {
     lfts_ctx ctx_ = nullptr;
     void *p_ = nullptr;
     size_t n_ = 0;
+    bool host_ = false;
 };
 
 class GpuComputation {
    public:
     // n_replicas independent systems of the same molecules and box advance in
     // the same launches (replica r of every device array at offset r * size).
+    // method: "pseudospectral" (periodic boxes) or "realspace" (the
+    // Crank-Nicolson step of lfts_step_realspace, continuous chains, FP64;
+    // any boundary conditions, no stress).  reduce_memory: every propagator
+    // slice in pinned host memory mapped into the device, read and written in
+    // place by the same kernels (the reference's memory-saving mode keeps its
+    // slices in pinned host memory too); device memory then holds the fields,
+    // tables, concentrations and step scratch only.
     GpuComputation(ComputationBox *cb, Molecules *molecules, PropagatorAnalyzer *analyzer, int precision, int device,
-                   int n_replicas = 1);
+                   int n_replicas = 1, const std::string &method = "pseudospectral", bool reduce_memory = false);
     ~GpuComputation();
 
     int get_n_grid() const { return cb_->get_n_grid(); }
@@ -129,6 +139,7 @@ class GpuComputation {
     void enqueue_concentrations();
     void sync_partitions();
 
+    bool realspace_ = false;
     ComputationBox *cb_;
     Molecules *mol_;
     PropagatorAnalyzer *pa_;

@@ -15,6 +15,7 @@
 #include "lfts_step_fast.cuh"
 #include "lfts_step_r8.cuh"
 #include "lfts_step_r12.cuh"
+#include "lfts_realspace.cuh"
 
 using namespace lfts;
 
@@ -48,8 +49,6 @@ struct lfts_ctx_s {
     int fastN = 0;            // cubic grid handled by the compile-time specialised kernels (0: generic)
     int r8 = 0;               // 64^3: register-resident 8x8 line transforms (lfts_step_r8.cuh)
     int fast_ok = 0, r8_ok = 0, r12_ok = 0;  // families set up at creation (lfts_set_step_impl)
-    int pf = 1;               // plane kernels L2-prefetch the next wave's inputs (GridPlan::ahead)
-    int ah_r8[5] = {}, ah_r12[3] = {};  // co-resident blocks of each plane kernel (its prefetch distance)
     int r12 = 0;              // 96^3: register-resident 12x8 plane kernels (lfts_step_r12.cuh)
     int nsm = 0;              // streaming multiprocessors of the device
     int xcap = 0;             // CTAs per SM of the persistent x-passes (0: the kernel's own residency)
@@ -186,32 +185,6 @@ template <typename T> static int r8_setup(int max_smem) {
     return 1;
 }
 
-// blocks of a kernel resident on the whole device at once (0 if unknown)
-template <class K> static int resident_blocks(lfts_ctx c, K kernel, int threads, size_t smem) {
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    return nb * c->nsm;
-}
-template <typename T> static void prefetch_distances(lfts_ctx c) {
-    using C = typename CT<T>::type;
-    if (c->r8) {
-        const size_t ps = r8::plane_smem<C>();
-        c->ah_r8[0] = resident_blocks(c, r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC>, NTHR, ps);
-        c->ah_r8[1] = resident_blocks(c, r8::kr_plane_mid<T>, NTHR, ps);
-        c->ah_r8[2] = resident_blocks(c, r8::kr_plane_inverse<T, 2, EPI_RICH>, NTHR, ps);
-        c->ah_r8[3] = resident_blocks(c, r8::kr_plane_forward<T, 1, FM_NONE, FM_NONE>, NTHR, ps);
-        c->ah_r8[4] = resident_blocks(c, r8::kr_plane_inverse<T, 1, EPI_SCALE>, NTHR, ps);
-    }
-    if (c->r12) {
-        c->ah_r12[0] = resident_blocks(c, r12::kq_plane_forward<T, FM_FAC_SQ, FM_FAC>, r12::NT, r12::plane_smem<C>(r12::N));
-        c->ah_r12[1] = resident_blocks(c, r12::kq_plane_mid<T>, r12::NT, r12::plane_smem<C>(r12::N / 2));
-        c->ah_r12[2] = resident_blocks(c, r12::kq_plane_inverse<T>, r12::NT, r12::plane_smem<C>(r12::N));
-    }
-}
-
 template <typename T> static int setup_plan(lfts_ctx c) {
     using C = typename CT<T>::type;
     GridPlan &g = c->g;
@@ -265,7 +238,6 @@ template <typename T> static int setup_plan(lfts_ctx c) {
     c->nbr2 = (int)c->sm_pf2 <= max_smem && (int)c->sm_x2 <= max_smem;
     CK((c->gen ? set_attrs_t<T, true>(max_smem) : set_attrs_t<T, false>(max_smem)));
     g.stw = nullptr;
-    g.ahead = 0;
     if (g.n0 == g.n1 && g.n1 == g.n2 && !std::getenv("LFTS_NO_FAST")) {
         const int N = g.n0;
         int ok = 0;
@@ -301,8 +273,6 @@ template <typename T> static int setup_plan(lfts_ctx c) {
             c->fast_ok = N;
             c->r8_ok = c->r8;
             c->r12_ok = c->r12;
-            prefetch_distances<T>(c);
-            if (std::getenv("LFTS_NO_L2_PREFETCH")) c->pf = 0;
         }
     }
     return 0;
@@ -397,12 +367,30 @@ extern "C" int lfts_free(lfts_ctx c, void *ptr) {
     if (ptr) CK(cudaFree(ptr));
     return 0;
 }
+extern "C" int lfts_malloc_host(lfts_ctx c, void **ptr, size_t bytes) {
+    if (!c || !ptr) return fail("null argument");
+    CK(cudaSetDevice(c->device));
+    void *h = nullptr, *d = nullptr;
+    CK(cudaHostAlloc(&h, bytes ? bytes : 16, cudaHostAllocMapped | cudaHostAllocPortable));
+    const cudaError_t e = cudaHostGetDevicePointer(&d, h, 0);
+    if (e != cudaSuccess || d != h) {
+        cudaFreeHost(h);
+        return fail("lfts_malloc_host: the pinned allocation has no device address equal to its host address");
+    }
+    *ptr = h;
+    return 0;
+}
+extern "C" int lfts_free_host(lfts_ctx c, void *ptr) {
+    if (!c) return fail("null context");
+    if (ptr) CK(cudaFreeHost(ptr));
+    return 0;
+}
 extern "C" int lfts_memset_async(lfts_ctx c, void *ptr, int v, size_t bytes) {
     CK(cudaMemsetAsync(ptr, v, bytes, c->stream));
     return 0;
 }
 extern "C" int lfts_memcpy_h2d(lfts_ctx c, void *dst, const void *src, size_t bytes) {
-    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c->stream));  // dst may be mapped host memory
     CK(cudaStreamSynchronize(c->stream));
     return 0;
 }
@@ -421,12 +409,12 @@ static int check_kernel_errors() {
 }
 
 extern "C" int lfts_memcpy_d2h(lfts_ctx c, void *dst, const void *src, size_t bytes) {
-    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return check_kernel_errors();
 }
 extern "C" int lfts_memcpy_d2d_async(lfts_ctx c, void *dst, const void *src, size_t bytes) {
-    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c->stream));  // either side may be mapped host memory
     return 0;
 }
 extern "C" int lfts_status_post(lfts_ctx c, const int *d_word, int slot) {
@@ -627,15 +615,11 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
             const size_t ps = r8::plane_smem<C>();
             const long long it2 = (long long)nj * 2 * r8::xpipe_tiles<C>(), it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = (long long)(c->xcap ? c->xcap : 3) * c->nsm;
             const dim3 px2((unsigned)(it2 < cap ? it2 : cap)), px1((unsigned)(it1 < cap ? it1 : cap));
-            GridPlan g1 = g, g3 = g, g5 = g;
-            g1.ahead = c->pf ? c->ah_r8[0] : 0;
-            g3.ahead = c->pf ? c->ah_r8[1] : 0;
-            g5.ahead = c->pf ? c->ah_r8[2] : 0;
-            r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC><<<rp, NTHR, ps, st>>>(g1, jobs, s, 0);
+            r8::kr_plane_forward<T, 2, FM_FAC_SQ, FM_FAC><<<rp, NTHR, ps, st>>>(g, jobs, s, 0);
             r8::kp_xpass<T, 2><<<px2, NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, 0, 1);
-            r8::kr_plane_mid<T><<<rp, NTHR, ps, st>>>(g3, jobs, 1);
+            r8::kr_plane_mid<T><<<rp, NTHR, ps, st>>>(g, jobs, 1);
             r8::kp_xpass<T, 1><<<px1, NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 1, 1, 1);
-            r8::kr_plane_inverse<T, 2, EPI_RICH><<<rp, NTHR, ps, st>>>(g5, jobs, s, 0, 0);
+            r8::kr_plane_inverse<T, 2, EPI_RICH><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, 0);
             CKLAUNCH();
             return 0;
         }
@@ -645,15 +629,11 @@ static int step_cont_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s) 
             const size_t p2 = r12::plane_smem<C>(N), p1 = r12::plane_smem<C>(N / 2), xs = r12::xpipe_smem<C>();
             const long long it2 = (long long)nj * 2 * r12::XTILES, it1 = (long long)nj * r12::XTILES;
             const long long cap = (long long)(c->xcap ? c->xcap : r12::minb_xpass<T>()) * c->nsm;
-            GridPlan g1 = g, g3 = g, g5 = g;
-            g1.ahead = c->pf ? c->ah_r12[0] : 0;
-            g3.ahead = c->pf ? c->ah_r12[1] : 0;
-            g5.ahead = c->pf ? c->ah_r12[2] : 0;
-            r12::kq_plane_forward<T, FM_FAC_SQ, FM_FAC><<<gp, r12::NT, p2, st>>>(g1, jobs, s, 0);
+            r12::kq_plane_forward<T, FM_FAC_SQ, FM_FAC><<<gp, r12::NT, p2, st>>>(g, jobs, s, 0);
             r12::kq_xpass<T, 2><<<(unsigned)(it2 < cap ? it2 : cap), NTHR, xs, st>>>(g, jobs, nj, 0, 0, 1);
-            r12::kq_plane_mid<T><<<gp, r12::NT, p1, st>>>(g3, jobs, 1);
+            r12::kq_plane_mid<T><<<gp, r12::NT, p1, st>>>(g, jobs, 1);
             r12::kq_xpass<T, 1><<<(unsigned)(it1 < cap ? it1 : cap), NTHR, xs, st>>>(g, jobs, nj, 1, 1, 1);
-            r12::kq_plane_inverse<T><<<gp, r12::NT, p2, st>>>(g5, jobs, s, 0);
+            r12::kq_plane_inverse<T><<<gp, r12::NT, p2, st>>>(g, jobs, s, 0);
             CKLAUNCH();
             return 0;
         }
@@ -679,13 +659,10 @@ static int step_disc_fast(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, 
         if (c->r8) {
             const dim3 rp(N, nj);
             const size_t ps = r8::plane_smem<C>();
-            GridPlan g1 = g, g5 = g;
-            g1.ahead = c->pf ? c->ah_r8[3] : 0;
-            g5.ahead = c->pf ? c->ah_r8[4] : 0;
-            r8::kr_plane_forward<T, 1, FM_NONE, FM_NONE><<<rp, NTHR, ps, st>>>(g1, jobs, s, 0);
+            r8::kr_plane_forward<T, 1, FM_NONE, FM_NONE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0);
             const long long it1 = (long long)nj * r8::xpipe_tiles<C>(), cap = (long long)(c->xcap ? c->xcap : 3) * c->nsm;
             r8::kp_xpass<T, 1><<<(unsigned)(it1 < cap ? it1 : cap), NTHR, r8::xpipe_smem<C>(), st>>>(g, jobs, nj, 0, half, half);
-            r8::kr_plane_inverse<T, 1, EPI_SCALE><<<rp, NTHR, ps, st>>>(g5, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
+            r8::kr_plane_inverse<T, 1, EPI_SCALE><<<rp, NTHR, ps, st>>>(g, jobs, s, 0, with_fac ? FM_FAC : FM_NONE);
             CKLAUNCH();
             return 0;
         }
@@ -1394,7 +1371,7 @@ extern "C" int lfts_dots_static(int precision, long long M, const lfts_dot_job *
 // the choice (and with it the last bits of the results) is stable.
 namespace {
 struct TuneCand {
-    int fastN, r8, r12, xcap, pf;
+    int fastN, r8, r12, xcap;
     const char *name;
 };
 }  // namespace
@@ -1403,20 +1380,18 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
     if (!c) return fail("null context");
     if (njobs < 1 || njobs > 65535) return fail("autotune: njobs must be 1..65535");
     if (reps < 1) reps = 5;
-    const int fastN = c->fastN, r8v = c->r8, r12v = c->r12, xcap0 = c->xcap, pf0 = c->pf;
+    const int fastN = c->fastN, r8v = c->r8, r12v = c->r12, xcap0 = c->xcap;
     std::vector<TuneCand> cands;
     if (r8v) {
-        cands.push_back({fastN, 1, 0, 0, 1, "register-64"});
-        cands.push_back({fastN, 1, 0, 0, 0, "register-64 no-l2-prefetch"});
-        cands.push_back({fastN, 1, 0, 2, 1, "register-64 xcap2"});
+        cands.push_back({fastN, 1, 0, 0, "register-64"});
+        cands.push_back({fastN, 1, 0, 2, "register-64 xcap2"});
     }
     if (r12v) {
-        cands.push_back({fastN, 0, 1, 0, 1, "register-96"});
-        cands.push_back({fastN, 0, 1, 0, 0, "register-96 no-l2-prefetch"});
-        cands.push_back({fastN, 0, 1, 1, 1, "register-96 xcap1"});
+        cands.push_back({fastN, 0, 1, 0, "register-96"});
+        cands.push_back({fastN, 0, 1, 1, "register-96 xcap1"});
     }
-    if (fastN) cands.push_back({fastN, 0, 0, 0, 1, "cubic"});
-    cands.push_back({0, 0, 0, 0, 1, "generic"});
+    if (fastN) cands.push_back({fastN, 0, 0, 0, "cubic"});
+    cands.push_back({0, 0, 0, 0, "generic"});
     const size_t sb = (size_t)c->prec, M = (size_t)c->g.M, Mc = (size_t)c->g.Mc;
     void *q = nullptr, *fac = nullptr, *bond = nullptr, *spec = nullptr, *w = nullptr;
     lfts_step_job *djobs = nullptr;
@@ -1473,7 +1448,6 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
         c->r8 = cands[k].r8;
         c->r12 = cands[k].r12;
         c->xcap = cands[k].xcap;
-        c->pf = cands[k].pf;
         for (int i = 0; i < 2 && rc == 0; i++) rc = lfts_step_continuous(c, djobs, njobs, 0);
         if (rc) break;
         CK(cudaEventRecord(e0, c->stream));
@@ -1491,7 +1465,6 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
         c->r8 = cands[best].r8;
         c->r12 = cands[best].r12;
         c->xcap = cands[best].xcap;
-        c->pf = cands[best].pf;
         char buf[96];
         for (size_t k = 0; k < cands.size(); k++) {
             std::snprintf(buf, sizeof buf, "%s%s %.4f ms", k ? "; " : "", cands[k].name, (double)ms[k]);
@@ -1504,7 +1477,6 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
         c->r8 = r8v;
         c->r12 = r12v;
         c->xcap = xcap0;
-        c->pf = pf0;
     }
     cleanup();
     if (report && report_cap) {
@@ -1516,17 +1488,13 @@ extern "C" int lfts_autotune(lfts_ctx c, int njobs, int reps, char *report, size
 
 extern "C" int lfts_set_step_impl(lfts_ctx c, const char *name) {
     if (!c || !name) return fail("null argument");
-    std::string n(name);
-    const std::string suffix = " no-l2-prefetch";
-    const bool nopf = n.size() > suffix.size() && n.compare(n.size() - suffix.size(), suffix.size(), suffix) == 0;
-    if (nopf) n.resize(n.size() - suffix.size());
+    const std::string n(name);
     const int fastN = c->fast_ok;
     auto set = [&](int f, int r8, int r12) {
         c->fastN = f;
         c->r8 = r8;
         c->r12 = r12;
         c->xcap = 0;
-        c->pf = nopf ? 0 : 1;
         return 0;
     };
     if (n == "register-64" && c->r8_ok) return set(fastN, 1, 0);
@@ -1541,9 +1509,130 @@ extern "C" int lfts_step_impl(lfts_ctx c, char *name, size_t cap) {
     std::string n = c->r8 ? (c->xcap ? "register-64 xcap" + std::to_string(c->xcap) : std::string("register-64"))
                   : c->r12 ? (c->xcap ? "register-96 xcap" + std::to_string(c->xcap) : std::string("register-96"))
                   : c->fastN ? std::string("cubic") : std::string("generic");
-    if ((c->r8 || c->r12) && !c->pf) n += " no-l2-prefetch";
     std::strncpy(name, n.c_str(), cap - 1);
     name[cap - 1] = 0;
+    return 0;
+}
+
+// ---------------------------------------------------------------- real-space solver
+extern "C" long long lfts_realspace_table_size(lfts_ctx c) {
+    if (!c) return 0;
+    return (long long)rs::ROWS * (c->g.n0 + c->g.n1 + c->g.n2) + 6;
+}
+
+// Tridiagonal rows of the Crank-Nicolson step along one axis
+// (src/common/FiniteDifference.cpp:20-99), then the pivots of the reference's
+// line solves (CpuSolverReal.cpp:480-549) for that matrix, in its order.
+static void realspace_axis(double b2, double ds, double dx, int n, int bc_lo, int bc_hi, double *t, double &denom,
+                           double &periodic) {
+    double *l = t, *d = t + n, *h = t + 2 * n, *p = t + 3 * n, *c = t + 4 * n, *v = t + 5 * n, *rp = t + 6 * n;
+    const double xf = b2 * ds / (std::pow(dx, 2) * 6.0);
+    for (int i = 0; i < n; i++) {
+        l[i] = -0.5 * xf;
+        d[i] = 1.0 + xf;
+        h[i] = -0.5 * xf;
+        c[i] = 0.0;
+        v[i] = 0.0;
+    }
+    if (bc_lo == 1) {  // reflecting
+        d[0] += l[0];
+        l[0] = 0.0;
+    } else if (bc_lo == 2) {  // absorbing
+        l[0] = 0.0;
+    }
+    if (bc_hi == 1) {
+        d[n - 1] += h[n - 1];
+        h[n - 1] = 0.0;
+    } else if (bc_hi == 2) {
+        h[n - 1] = 0.0;
+    }
+    periodic = bc_lo == 0 ? 1.0 : 0.0;
+    denom = 1.0;
+    if (bc_lo != 0) {
+        p[0] = d[0];
+        for (int i = 1; i < n; i++) {
+            c[i - 1] = h[i - 1] / p[i - 1];
+            p[i] = d[i] - l[i] * c[i - 1];
+        }
+    } else {
+        p[0] = d[0] - 1.0;
+        v[0] = 1.0 / p[0];
+        for (int i = 1; i < n - 1; i++) {
+            c[i - 1] = h[i - 1] / p[i - 1];
+            p[i] = d[i] - l[i] * c[i - 1];
+            v[i] = (-l[i] * v[i - 1]) / p[i];
+        }
+        c[n - 2] = h[n - 2] / p[n - 2];
+        p[n - 1] = d[n - 1] - h[n - 1] * l[0] - l[n - 1] * c[n - 2];
+        v[n - 1] = (h[n - 1] - l[n - 1] * v[n - 2]) / p[n - 1];
+        for (int i = n - 2; i >= 0; i--) v[i] = v[i] - c[i] * v[i + 1];
+        denom = 1.0 + v[0] + l[0] * v[n - 1];
+    }
+    for (int i = 0; i < n; i++) rp[i] = 1.0 / p[i];
+}
+
+extern "C" int lfts_realspace_tables(lfts_ctx c, double b2, double ds, int dim, const double *dx, const int *bc,
+                                     double *out) {
+    if (!c || !dx || !bc || !out) return fail("null argument");
+    if (dim < 1 || dim > 3 || dim != c->dim) return fail("realspace tables: dim must be the context's dimension");
+    const int n[3] = {c->g.n0, c->g.n1, c->g.n2};
+    const long long tail = (long long)rs::ROWS * (n[0] + n[1] + n[2]);
+    for (int d = 0; d < dim; d++) {
+        if (bc[2 * d] < 0 || bc[2 * d] > 2 || bc[2 * d + 1] < 0 || bc[2 * d + 1] > 2)
+            return fail("realspace tables: boundary codes are 0 (periodic), 1 (reflecting), 2 (absorbing)");
+        if ((bc[2 * d] == 0) != (bc[2 * d + 1] == 0))
+            return fail("realspace tables: a periodic side needs a periodic opposite side");
+        if (n[3 - dim + d] < 2) return fail("realspace tables: every axis of the box needs at least 2 points");
+    }
+    long long off = 0;
+    for (int a = 0; a < 3; a++) {
+        const int d = a - (3 - dim);
+        if (d < 0) {  // padding axis (extent 1): never solved
+            for (int r = 0; r < rs::ROWS; r++) out[off + (long long)r * n[a]] = r == 1 || r == 3 || r == 6 ? 1.0 : 0.0;
+            out[tail + a] = 1.0;
+            out[tail + 3 + a] = 0.0;
+        } else {
+            realspace_axis(b2, ds, dx[d], n[a], bc[2 * d], bc[2 * d + 1], out + off, out[tail + a], out[tail + 3 + a]);
+        }
+        off += (long long)rs::ROWS * n[a];
+    }
+    return 0;
+}
+
+extern "C" int lfts_step_realspace(lfts_ctx c, const lfts_step_job *jobs, int nj, int s, int dim) {
+    if (!c || !jobs) return fail("null argument");
+    if (c->prec != 8) return fail("the real-space step runs in FP64 contexts only");
+    if (dim < 1 || dim > 3 || dim != c->dim) return fail("real-space step: dim must be the context's dimension");
+    if (nj <= 0) return 0;
+    if (nj > 65535) return fail("real-space step: at most 65535 jobs per call");
+    const GridPlan &g = c->g;
+    cudaStream_t st = c->stream;
+    auto blocks = [&](long long n_axis) { return (unsigned)((g.M / n_axis + NTHR - 1) / NTHR); };
+    // the last-axis sweep through a shared-memory tile of ZL lines
+    // (a tile of long lines that does not fit shared memory walks the lines in global memory)
+    const size_t zsm = sizeof(double) * 2 * rs::ZL * (size_t)(g.n2 + 1);
+    const unsigned zblocks = (unsigned)((g.M / g.n2 + rs::ZL - 1) / rs::ZL);
+    const bool tiled = zsm <= 200 * 1024;
+    if (tiled && zsm > 48 * 1024)
+        CK(cudaFuncSetAttribute(rs::k_rs_last_axis<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsm));
+    auto last_axis = [&](int src_half) {
+        if (tiled) rs::k_rs_last_axis<true><<<dim3(zblocks, nj), rs::ZL, zsm, st>>>(g, jobs, s, src_half);
+        else rs::k_rs_next<2, true><<<dim3(blocks(g.n2), nj), NTHR, 0, st>>>(g, jobs, s, src_half);
+    };
+    if (dim == 3) {
+        rs::k_rs_first<3><<<dim3(blocks(g.n0), nj), NTHR, 0, st>>>(g, jobs, s);
+        rs::k_rs_next<1, false><<<dim3(blocks(g.n1), nj), NTHR, 0, st>>>(g, jobs, s, 0);
+        last_axis(1);
+        c->launches += 3;
+    } else if (dim == 2) {
+        rs::k_rs_first<2><<<dim3(blocks(g.n1), nj), NTHR, 0, st>>>(g, jobs, s);
+        last_axis(0);
+        c->launches += 2;
+    } else {
+        rs::k_rs_first<1><<<dim3(blocks(g.n2), nj), NTHR, 0, st>>>(g, jobs, s);
+        c->launches += 1;
+    }
+    CKLAUNCH();
     return 0;
 }
 

@@ -62,7 +62,6 @@ struct GridPlan {
     const void *tw[3];       // twiddles exp(-2 pi i j / n), n entries, precision T
     const short *perm[3];    // digit-reversal permutation, n entries
     const void *stw;         // per-stage twiddles of the cubic fast path (lfts_step_fast.cuh), or NULL
-    int ahead;               // plane kernels: L2-prefetch the inputs of block b + ahead (0: no prefetch)
 };
 
 // w_n^e for the forward (sign<0) or inverse (sign>0) direction, table in shared memory

@@ -603,11 +603,22 @@ ComputationBox::ComputationBox(const std::vector<int> &nx, const std::vector<dou
     if (!bc.empty() && bc.size() != 2 * nx.size())
         LFTS_THROW("We expect 0 or " + std::to_string(2 * nx.size()) + " boundary conditions, but we get " +
                    std::to_string(bc.size()) + ". For each dimension, two boundary conditions (top and bottom) are required.");
+    std::vector<std::string> lower;
     for (auto b : bc) {
         std::transform(b.begin(), b.end(), b.begin(), [](unsigned char c) { return std::tolower(c); });
-        if (b != "periodic")
-            LFTS_THROW("Currently, pseudo-spectral method only supports periodic boundary conditions");
+        lower.push_back(b);
     }
+    for (size_t i = 0; i < lower.size(); i += 2)
+        if ((lower[i] == "periodic") != (lower[i + 1] == "periodic"))
+            LFTS_THROW(lower[i] + " and " + lower[i + 1] + " are an invalid boundary condition combination. " +
+                       "If one side imposes a periodic boundary condition, the other side must also be a periodic boundary condition.");
+    for (const auto &b : lower) {
+        if (b == "periodic") bc_.push_back(0);
+        else if (b == "reflecting") bc_.push_back(1);
+        else if (b == "absorbing") bc_.push_back(2);
+        else LFTS_THROW(b + " is an invalid boundary condition. Choose among ['periodic', 'reflecting', 'absorbing']");
+    }
+    if (bc_.empty()) bc_.assign(2 * nx.size(), 0);
     nx_ = nx;
     lx_ = lx;
     n_grid_ = 1;
@@ -617,6 +628,12 @@ ComputationBox::ComputationBox(const std::vector<int> &nx, const std::vector<dou
     for (double d : dx_) dv_ *= d;
     volume_ = 1.0;
     for (double l : lx) volume_ *= l;
+}
+
+bool ComputationBox::is_periodic() const {
+    for (int b : bc_)
+        if (b != 0) return false;
+    return true;
 }
 
 int ComputationBox::get_nx(int i) const {

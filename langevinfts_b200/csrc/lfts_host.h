@@ -187,8 +187,13 @@ class ComputationBox {
     void set_lx(const std::vector<double> &lx);
     double integral(const double *g) const;
     double inner_product(const double *g, const double *h) const;
+    // boundary condition of each side, lower side of axis d at 2d: 0 periodic,
+    // 1 reflecting, 2 absorbing (src/common/ComputationBox.cpp:88-150)
+    const std::vector<int> &get_boundary_conditions() const { return bc_; }
+    bool is_periodic() const;
 
    private:
+    std::vector<int> bc_;
     std::vector<int> nx_;
     std::vector<double> lx_, dx_;
     int n_grid_ = 0;

@@ -41,9 +41,6 @@ struct PlatformSelector {
         }
         f->name = platform;
         f->reduce_memory = reduce_memory;
-        if (reduce_memory)
-            std::cout << "(warning) every propagator is kept in GPU memory; the reduce_memory_usage option is ignored."
-                      << std::endl;
         return f;
     }
 };
@@ -300,11 +297,13 @@ PYBIND11_MODULE(langevinfts, m) {
         .def("create_pseudospectral_solver", [](Factory &f, ComputationBox *cb, Molecules *mol, PropagatorAnalyzer *pa) {
             if (pa->get_model_name() != mol->get_model_name())
                 throw std::runtime_error("molecules and propagator analyzer use different chain models");
-            return new GpuComputation(cb, mol, pa, f.precision, f.device);
+            return new GpuComputation(cb, mol, pa, f.precision, f.device, 1, "pseudospectral", f.reduce_memory);
         }, py::keep_alive<0, 2>(), py::keep_alive<0, 3>(), py::keep_alive<0, 4>())
-        .def("create_realspace_solver", [](Factory &, py::object, py::object, py::object) -> py::object {
-            throw std::runtime_error("The real-space (Crank-Nicolson) solver is not part of this build");
-        })
+        .def("create_realspace_solver", [](Factory &f, ComputationBox *cb, Molecules *mol, PropagatorAnalyzer *pa) {
+            if (pa->get_model_name() != mol->get_model_name())
+                throw std::runtime_error("molecules and propagator analyzer use different chain models");
+            return new GpuComputation(cb, mol, pa, f.precision, f.device, 1, "realspace", f.reduce_memory);
+        }, py::keep_alive<0, 2>(), py::keep_alive<0, 3>(), py::keep_alive<0, 4>())
         .def("create_anderson_mixing", [](Factory &f, int n_var, int max_hist, double start_error, double mix_min, double mix_init) {
             return new GpuAndersonMixing(n_var, max_hist, start_error, mix_min, mix_init, f.device);
         })

@@ -264,7 +264,6 @@ __global__ void __launch_bounds__(NT, minb_two_branch<T>()) kq_plane_forward(Gri
     constexpr int fm0 = FM0, fm1 = FM1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;
-    prefetch_next_plane<T>(g, jobs, s, true, true, 0, 0);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, j = lane & 7, grp = tid >> 3;
@@ -338,7 +337,6 @@ __global__ void __launch_bounds__(NT, minb_mid<T>()) kq_plane_mid(GridPlan g, co
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;  // 48 packed rows: z-line u = row u + i row (u + 48)
-    prefetch_next_plane<T>(g, jobs, 0, false, true, spec_idx, 1);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, j = lane & 7, grp = tid >> 3;
@@ -429,7 +427,6 @@ __global__ void __launch_bounds__(NT, minb_two_branch<T>()) kq_plane_inverse(Gri
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;
-    prefetch_next_plane<T>(g, jobs, 0, false, true, spec_in0, 2);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, j = lane & 7, grp = tid >> 3;

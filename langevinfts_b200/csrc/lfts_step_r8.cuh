@@ -33,30 +33,6 @@
 
 namespace lfts {
 
-// L2 prefetch for the plane kernels (one x-plane per block, blocks (x, job) =
-// (blockIdx.x, blockIdx.y), launched in linear order): a block asks L2 for
-// the inputs of the block g.ahead places later, about the block that takes
-// its slot in the next wave, so those loads find their lines in L2 instead of
-// DRAM.  Inputs: the plane of q slice s (with_q), of the factors (with_fac),
-// and of spectrum slots spec0 .. spec0 + nspec - 1.  Threads 0-15 issue it;
-// inactive jobs are skipped.  A hint only: results do not depend on it.
-template <typename T>
-__device__ __forceinline__ void prefetch_next_plane(const GridPlan &g, const lfts_step_job *__restrict__ jobs, int s, bool with_q,
-                                                    bool with_fac, int spec0, int nspec) {
-    using C = typename CT<T>::type;
-    if (g.ahead <= 0 || threadIdx.x >= 16) return;
-    const long long b = blockIdx.x + (long long)gridDim.x * blockIdx.y + g.ahead;
-    if (b >= (long long)gridDim.x * gridDim.y) return;
-    const long long x = b % gridDim.x;
-    const lfts_step_job &jb = jobs[b / gridDim.x];
-    if (jb.active && !jb.active[jb.replica]) return;
-    const long long rp = (long long)g.n1 * g.n2, cp = (long long)g.n1 * g.nzc;
-    const uint32_t rb = (uint32_t)(rp * sizeof(T)), cb = (uint32_t)(cp * sizeof(C));
-    if (with_q) prefetch_l2_range((const T *)jb.in + s * jb.in_stride + x * rp, rb, 0);
-    if (with_fac) prefetch_l2_range((const T *)jb.fac + x * rp, rb, 4);
-    for (int k = 0; k < nspec; k++) prefetch_l2_range((const C *)jb.spec + (size_t)(spec0 + k) * g.Mc + x * cp, cb, 8 + 4 * k);
-}
-
 namespace r8 {
 
 constexpr int N = 64, NZC = N / 2 + 1, PLANE = N * NZC;
@@ -298,7 +274,6 @@ __global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFT
     constexpr int fm0 = FM0, fm1 = FM1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;
-    prefetch_next_plane<T>(g, jobs, s, true, fm0 != FM_NONE, 0, 0);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, j = lane & 7, grp = tid >> 3;
@@ -531,7 +506,6 @@ __global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFT
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;
-    prefetch_next_plane<T>(g, jobs, 0, false, true, spec_idx, 1);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, j = lane & 7, grp = tid >> 3;
@@ -579,7 +553,6 @@ __global__ void __launch_bounds__(NTHR, (sizeof(T) == 4 ? LFTS_R8_MINB_F32 : LFT
     using C = typename CT<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *P = (C *)smem_raw;
-    prefetch_next_plane<T>(g, jobs, 0, false, NBR == 2 || fm0 != FM_NONE, spec_in0, NBR);
     const lfts_step_job jb = jobs[blockIdx.y];
     if (jb.active && !jb.active[jb.replica]) return;
     const int x = blockIdx.x, tid = threadIdx.x, lane = tid & 31, j = lane & 7, grp = tid >> 3;

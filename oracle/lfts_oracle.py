@@ -117,6 +117,101 @@ def segment_stress(g, q1, q2, bond_length_sq, basis, bond=None):
 
 
 # ---------------------------------------------------------------- full solver
+# ---------------------------------------------------------------- real-space step
+BC_CODES = {"periodic": 0, "reflecting": 1, "absorbing": 2}
+
+
+def laplacian_rows(n, dx, bond_length_sq, ds, bc_lo, bc_hi):
+    """Tridiagonal rows (l, d, h) of one axis of the Crank-Nicolson step
+    (src/common/FiniteDifference.cpp:20-99): off-diagonals -b^2 ds / (12 dx^2),
+    diagonal 1 + b^2 ds / (6 dx^2); a reflecting side folds its outer
+    off-diagonal into the diagonal, an absorbing side drops it."""
+    xf = bond_length_sq * ds / (dx ** 2 * 6.0)
+    l, d, h = np.full(n, -0.5 * xf), np.full(n, 1.0 + xf), np.full(n, -0.5 * xf)
+    if bc_lo == 1:
+        d[0] += l[0]; l[0] = 0.0
+    elif bc_lo == 2:
+        l[0] = 0.0
+    if bc_hi == 1:
+        d[-1] += h[-1]; h[-1] = 0.0
+    elif bc_hi == 2:
+        h[-1] = 0.0
+    return l, d, h
+
+
+def tridiagonal_lines(l, d, h, rhs, periodic):
+    """Solve the tridiagonal (or cyclic, by Sherman-Morrison with gamma = 1)
+    system along axis 0 of rhs for every other index at once
+    (src/platforms/cpu/CpuSolverReal.cpp:480-549, same recurrences)."""
+    n = rhs.shape[0]
+    x = np.empty_like(rhs)
+    c = np.zeros(n)
+    if not periodic:
+        t = d[0]
+        x[0] = rhs[0] / t
+        for i in range(1, n):
+            c[i - 1] = h[i - 1] / t
+            t = d[i] - l[i] * c[i - 1]
+            x[i] = (rhs[i] - l[i] * x[i - 1]) / t
+        for i in range(n - 2, -1, -1):
+            x[i] = x[i] - c[i] * x[i + 1]
+        return x
+    q = np.zeros(n)
+    t = d[0] - 1.0
+    x[0] = rhs[0] / t
+    q[0] = 1.0 / t
+    for i in range(1, n - 1):
+        c[i - 1] = h[i - 1] / t
+        t = d[i] - l[i] * c[i - 1]
+        x[i] = (rhs[i] - l[i] * x[i - 1]) / t
+        q[i] = (-l[i] * q[i - 1]) / t
+    c[n - 2] = h[n - 2] / t
+    t = d[n - 1] - h[n - 1] * l[0] - l[n - 1] * c[n - 2]
+    x[n - 1] = (rhs[n - 1] - l[n - 1] * x[n - 2]) / t
+    q[n - 1] = (h[n - 1] - l[n - 1] * q[n - 2]) / t
+    for i in range(n - 2, -1, -1):
+        x[i] = x[i] - c[i] * x[i + 1]
+        q[i] = q[i] - c[i] * q[i + 1]
+    value = (x[0] + l[0] * x[n - 1]) / (1.0 + q[0] + l[0] * q[n - 1])
+    return x - q.reshape([n] + [1] * (rhs.ndim - 1)) * value
+
+
+def step_realspace(nx, lx, q_in, exp_dw, bond_length_sq, ds, bc):
+    """One real-space Crank-Nicolson step, q_out = e ADI(e q_in), e = exp(-w ds/2)
+    (src/platforms/cpu/CpuSolverReal.cpp:135-478): the first sweep implicit in
+    axis 0 with the full explicit operator on the right, then one implicit
+    sweep per further axis.  nx, lx: the box (1..3 axes); bc: 2 * dim names."""
+    dim = len(nx)
+    codes = [BC_CODES[b.lower()] for b in bc] if bc else [0] * (2 * dim)
+    rows = [laplacian_rows(nx[a], lx[a] / nx[a], bond_length_sq, ds, codes[2 * a], codes[2 * a + 1]) for a in range(dim)]
+    per = [codes[2 * a] == 0 for a in range(dim)]
+    q = (exp_dw * q_in).reshape(nx)
+
+    def shift(a, s_):  # q at i - 1 (s_ = -1) or i + 1 (s_ = +1) along axis a, with the boundary rule
+        if per[a]:
+            return np.roll(q, -s_, axis=a)
+        idx = np.clip(np.arange(nx[a]) + s_, 0, nx[a] - 1)
+        return np.take(q, idx, axis=a)
+
+    def coef(a, r):  # row r of axis a broadcast along that axis
+        shape = [1] * dim
+        shape[a] = nx[a]
+        return rows[a][r].reshape(shape)
+    L, D, H = 0, 1, 2
+    if dim == 1:
+        rhs = (2.0 - coef(0, D)) * q - coef(0, L) * shift(0, -1) - coef(0, H) * shift(0, +1)
+    else:
+        inner = (float(dim) - 0.5 * coef(0, D) - sum(coef(a, D) for a in range(1, dim))) * q
+        for a in range(dim - 1, 0, -1):
+            inner = inner - coef(a, L) * shift(a, -1) - coef(a, H) * shift(a, +1)
+        rhs = 2.0 * inner - coef(0, L) * shift(0, -1) - coef(0, H) * shift(0, +1)
+    x = tridiagonal_lines(*rows[0], rhs, per[0])
+    for a in range(1, dim):
+        r = x + (coef(a, D) - 1.0) * q + coef(a, L) * shift(a, -1) + coef(a, H) * shift(a, +1)
+        x = np.moveaxis(tridiagonal_lines(*rows[a], np.moveaxis(r, a, 0), per[a]), 0, a)
+    return (x.reshape(-1) * exp_dw)
+
+
 class PropagatorSolver:
     """compute_propagators / compute_concentrations / compute_stress for an
     arbitrary acyclic molecule, driven by the analyzer tables (propagators and
