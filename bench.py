@@ -259,7 +259,8 @@ def run_reference(args):
 def step_traffic_per_job(s_bytes):
     """DRAM bytes (read + write) per (replica, key, contour step) of one
     continuous step, from the ncu summary committed under profiles/ (the line
-    'dram_bytes_per_job_step f64 <bytes>'), or None when it is absent."""
+    'dram_bytes_per_job_step f64 <bytes>', captured one kernel at a time at 32
+    jobs), or None when it is absent."""
     tag = {8: "f64", 4: "f32"}[s_bytes]
     try:
         with open(os.path.join(ROOT, "profiles", "step_continuous_64cubed.txt")) as fh:
@@ -1050,7 +1051,10 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "lfts_step_continuous (5 fused FFT-pass kernels)",
                      "launch_ms": ms, "jobs_per_launch": njobs,
-                     "bytes_model": f"{s_bytes}*(12M+24Mc) per job (pass model), peak = measured hbm_gbs"},
+                     "bytes_model": f"{s_bytes}*(12M+24Mc) per job (pass model), peak = measured hbm_gbs",
+                     "traffic_source": "ncu dram bytes per job-step captured one kernel at a time at 32 jobs "
+                                       "(profiles/step_continuous_64cubed.txt) x jobs per launch; at 128 jobs L2 "
+                                       "keeps less, so this is a lower bound"},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
