@@ -739,8 +739,8 @@ def run_scft(args):
 # timed steps of each variant (capped so the default run stays within minutes)
 VARIANT_STEPS_MAX = 8
 # plain Langevin steps whose fields train the learned start, and its time budget (s)
-LEARNED_PAIR_STEPS = 12
-LEARNED_TRAIN_S = 90.0
+LEARNED_PAIR_STEPS = 16
+LEARNED_TRAIN_S = 120.0
 
 
 def time_batched(sim, K, start=None):
