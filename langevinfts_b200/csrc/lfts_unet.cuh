@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <string>
 
 #include "lfts_bulk.cuh"
@@ -195,49 +196,83 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_umma(const uint4 *__restrict_
 }
 
 // ------------------------------------------------------------------------
-// 3x3x3 convolution with the input of a tile staged once: the tile is 1 x 16
-// x 8 output positions (z, y, x) and its halo 3 x 18 x 10 positions sits in
-// shared memory as planes [kc][zh][yh][xh] of 16-byte units.  For tap (dz, dy,
-// dx) the A operand of the MMA is read in place: the 8 output positions of a
-// y row map to 8 consecutive halo rows (one core matrix), the 16 y rows are
-// HX units apart (SBO), the channel chunks a plane apart (LBO); only the
-// tap's weights are copied per tap.  Needs H % 16 == 0 and W % 8 == 0.
-constexpr int HT_Y = 16, HT_X = 8, HZ = 3, HY = HT_Y + 2, HX = HT_X + 2, HPLANE = HZ * HY * HX;
+// 3x3x3 convolution with the input of a tile staged once: the tile is TZ x 16
+// x 8 output positions (z, y, x; TZ = 1 or 2) and its halo (TZ + 2) x 18 x 10
+// positions sits in shared memory as planes [kc][zh][yh][xh] of 16-byte
+// units (a chunk's plane padded to an odd length).  For tap (dz, dy, dx) and
+// output plane j the A operand of the MMA is read in place: the 8 output
+// positions of a y row map to 8 consecutive halo rows (one core matrix), the
+// 16 y rows are HX units apart (SBO), the channel chunks a plane apart (LBO).  Each staged tap of weights feeds TZ MMAs (one
+// per output plane, TZ accumulators of COUT columns in tensor memory).  Needs
+// H % 16 == 0, W % 8 == 0 and D % TZ == 0.
+constexpr int HT_Y = 16, HT_X = 8, HY = HT_Y + 2, HX = HT_X + 2, HROW = HY * HX;  // halo positions per z plane
 
-// Warp roles after the halo is staged: warps 1-3 copy the tap weights into a
-// ring of NS stages (full[st]: 96 producer arrivals), lane 0 of warp 0 issues
-// each tap's MMAs once its stage is full and commits them to empty[st], which
-// frees the stage; a last commit to bar_done releases the epilogue.
+// Thread 32 streams the tap weights with one bulk copy per tap into a ring of
+// NS stages (full[st]: transaction bytes), starting before the halo is staged;
+// lane 0 of warp 0 issues each tap's MMAs once its stage is full and commits
+// them to empty[st], which lets the next bulk copy into the stage; a last
+// commit to done releases the epilogue.
+template <int TZ>
 __global__ void __launch_bounds__(CONV_M) k_conv3d_halo_umma(const uint4 *__restrict__ in, const uint4 *__restrict__ wpk,
                                                              const float *__restrict__ bias, uint16_t *__restrict__ out,
                                                              int B, int D, int H, int W, int cin, int cout, int relu,
                                                              uint32_t tmem_cols, int NS) {
+    // halo units per channel chunk, odd so that the chunks of one position fall in different banks
+    constexpr int HPL = (TZ + 2) * HROW + 1;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int kc_n = cin / 8, b_units = kc_n * cout;
-    uint4 *halo = (uint4 *)smem_raw;                 // kc_n * HPLANE units
-    uint4 *wst = halo + kc_n * HPLANE;               // NS weight stages
+    const uint32_t b_bytes = (uint32_t)b_units * 16;
+    uint4 *halo = (uint4 *)smem_raw;                 // kc_n * HPL units
+    uint4 *wst = halo + kc_n * HPL;                  // NS weight stages
     uint64_t *full = (uint64_t *)(wst + (size_t)NS * b_units), *empty = full + NS, *done = empty + NS;
     uint32_t *tmem_slot = (uint32_t *)(done + 1);
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int x0 = blockIdx.x * HT_X, y0 = blockIdx.y * HT_Y, z = blockIdx.z % D, n = blockIdx.z / D;
-    if (tid == 0) {
+    const int ztiles = D / TZ;
+    const int x0 = blockIdx.x * HT_X, y0 = blockIdx.y * HT_Y, z0 = (blockIdx.z % ztiles) * TZ, n = blockIdx.z / ztiles;
+    int issued = 0;  // taps whose bulk copy thread 32 started
+    if (tid == 32) {
         for (int i = 0; i < NS; i++) {
-            mbar_init(full + i, CONV_M - 32);
+            mbar_init(full + i, 1);
             mbar_init(empty + i, 1);
         }
         mbar_init(done, 1);
+        // the first NS taps stream in while the halo is staged
+        for (; issued < NS && issued < 27; issued++) {
+            mbar_arrive_expect_tx(full + issued, b_bytes);
+            bulk_load(wst + (size_t)issued * b_units, wpk + (long long)issued * b_units, b_bytes, full + issued);
+        }
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
                      "r"(tmem_cols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    // the halo, periodic
-    for (int i = tid; i < kc_n * HPLANE; i += CONV_M) {
-        const int kc = i / HPLANE, r = i - kc * HPLANE;
-        const int zh = r / (HY * HX), yh = (r / HX) % HY, xh = r % HX;
-        const int zz = (z + zh - 1 + D) % D, yy = (y0 + yh - 1 + H) % H, xx = (x0 + xh - 1 + W) % W;
-        cp_async16(halo + i, in + ((((long long)n * D + zz) * H + yy) * W + xx) * kc_n + kc);
+    // the halo, periodic: halo row r = zh * HY + yh holds HX positions x kc_n
+    // chunks, contiguous in global memory apart from the wrapped ends; thread
+    // items run chunk-fastest along a row so that a warp's copies are coalesced
+    {
+        const int rowu = HX * kc_n, nrows = (TZ + 2) * HY;
+        const int dr = CONV_M / rowu, df = CONV_M - dr * rowu;
+        const float rk = 1.0f / (float)kc_n;
+        int r = tid / rowu, f = tid - r * rowu;
+        while (r < nrows) {
+            const int xh = (int)(((float)f + 0.5f) * rk), kc = f - xh * kc_n;
+            const int zh = r / HY, yh = r - zh * HY;
+            int xx = x0 + xh - 1, yy = y0 + yh - 1, zz = z0 + zh - 1;
+            xx += xx < 0 ? W : 0;
+            xx -= xx >= W ? W : 0;
+            yy += yy < 0 ? H : 0;
+            yy -= yy >= H ? H : 0;
+            zz += zz < 0 ? D : 0;
+            zz -= zz >= D ? D : 0;
+            cp_async16(halo + kc * HPL + r * HX + xh, in + ((((long long)n * D + zz) * H + yy) * W + xx) * kc_n + kc);
+            f += df;
+            r += dr;
+            if (f >= rowu) {
+                f -= rowu;
+                r++;
+            }
+        }
     }
     cp_async_wait_all();
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -246,21 +281,16 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_halo_umma(const uint4 *__rest
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
-    if (warp > 0) {
-        // producers: tap t into stage t % NS once the MMAs of tap t - NS freed it
-        const int pt = tid - 32;
-        for (int t = 0; t < 27 && ok; t++) {
-            const int st = t % NS, u = t / NS;
-            if (u > 0 && !mbar_wait(empty + st, (u - 1) & 1)) {
+    if (tid == 32) {
+        // producer: tap t into stage t % NS once the MMAs of tap t - NS freed it
+        for (; issued < 27; issued++) {
+            const int st = issued % NS, u = issued / NS;
+            if (!mbar_wait(empty + st, (u - 1) & 1)) {
                 ok = false;
                 break;
             }
-            uint4 *sb = wst + (size_t)st * b_units;
-            const uint4 *src = wpk + (long long)t * b_units;
-            for (int i = pt; i < b_units; i += CONV_M - 32) cp_async16(sb + i, src + i);
-            cp_async_wait_all();
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(full + st)) : "memory");
+            mbar_arrive_expect_tx(full + st, b_bytes);
+            bulk_load(wst + (size_t)st * b_units, wpk + (long long)issued * b_units, b_bytes, full + st);
         }
     } else if (tid == 0) {
         const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(cout >> 3) << 17) | ((uint32_t)(CONV_M >> 4) << 24);
@@ -273,41 +303,51 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_halo_umma(const uint4 *__rest
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;  // halo offsets of the tap (0..2)
-            const uint32_t a_tap = halo0 + (uint32_t)(((dz * HY + dy) * HX + dx) * 16);
             const uint32_t b0 = smem_addr(wst + (size_t)st * b_units);
-            for (int s = 0; s < kc_n / 2; s++) {
-                const uint64_t da = umma_desc(a_tap + (uint32_t)(2 * s * HPLANE * 16), HPLANE * 16, HX * 16);
-                const uint64_t db = umma_desc(b0 + (uint32_t)(2 * s * cout * 16), (uint32_t)cout * 16, 128);
-                umma_bf16(tmem, da, db, idesc, (t > 0 || s > 0) ? 1u : 0u);
+#pragma unroll
+            for (int j = 0; j < TZ; j++) {
+                const uint32_t a_tap = halo0 + (uint32_t)((((j + dz) * HY + dy) * HX + dx) * 16);
+                for (int s = 0; s < kc_n / 2; s++) {
+                    const uint64_t da = umma_desc(a_tap + (uint32_t)(2 * s * HPL * 16), HPL * 16, HX * 16);
+                    const uint64_t db = umma_desc(b0 + (uint32_t)(2 * s * cout * 16), (uint32_t)cout * 16, 128);
+                    umma_bf16(tmem + (uint32_t)(j * cout), da, db, idesc, (t > 0 || s > 0) ? 1u : 0u);
+                }
             }
             umma_commit(empty + st);
         }
         if (ok) umma_commit(done);
     }
     {
-        // every thread: the accumulator is complete (or some wait gave up)
+        // every thread: the accumulators are complete (or some wait gave up)
         const bool fin = __syncthreads_and(ok) ? mbar_wait(done, 0) : false;
         ok = __syncthreads_and(fin);
     }
     if (!ok) {
-        mbar_wait(done, 0);  // a second bounded wait for MMAs still in flight
+        // a second bounded wait for MMAs still in flight, and for the weight
+        // copies that no MMA consumed
+        mbar_wait(done, 0);
+        if (tid == 32)
+            for (int t = issued > NS ? issued - NS : 0; t < issued; t++) mbar_wait(full + t % NS, (t / NS) & 1);
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int m = tid;  // accumulator row = 8 j + l: position (y0 + j, x0 + l)
-        const long long p = (((long long)n * D + z) * H + (y0 + m / 8)) * W + (x0 + m % 8);
-        for (int c0 = 0; c0 < cout; c0 += 16) {
-            uint32_t v[16];
-            tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
-            uint16_t h[16];
 #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                float f = __uint_as_float(v[i]) + bias[c0 + i];
-                if (relu && f < 0.f) f = 0.f;
-                h[i] = to_bf16(f);
+        for (int j = 0; j < TZ; j++) {
+            const long long p = (((long long)n * D + z0 + j) * H + (y0 + m / 8)) * W + (x0 + m % 8);
+            for (int c0 = 0; c0 < cout; c0 += 16) {
+                uint32_t v[16];
+                tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(j * cout + c0), v);
+                uint16_t h[16];
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    float f = __uint_as_float(v[i]) + bias[c0 + i];
+                    if (relu && f < 0.f) f = 0.f;
+                    h[i] = to_bf16(f);
+                }
+                uint4 *o = (uint4 *)(out + p * cout + c0);
+                o[0] = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
+                o[1] = make_uint4(h[8] | (h[9] << 16), h[10] | (h[11] << 16), h[12] | (h[13] << 16), h[14] | (h[15] << 16));
             }
-            uint4 *o = (uint4 *)(out + p * cout + c0);
-            o[0] = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
-            o[1] = make_uint4(h[8] | (h[9] << 16), h[10] | (h[11] << 16), h[12] | (h[13] << 16), h[14] | (h[15] << 16));
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -320,35 +360,103 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_halo_umma(const uint4 *__rest
 //   dw[tap][co][ci] += sum_p gy[p][co] x[p + tap][ci]
 // per tap a GEMM with M = co (padded to 128 rows), N = cin, K = positions.
 // Both operands are MN-major in channels-last memory (16 bytes = 8 channels of
-// one position), so they are staged without transposition: chunk c of
-// position k at (c * WG_K + k) * 16 bytes; 8 consecutive positions form a core
-// matrix (LBO = 128 bytes), channel chunks are WG_K * 16 bytes apart (SBO).
-// A CTA takes one (kz, ky) row of taps (kx = 0..2; the single tap of a 1x1x1
-// kernel) over WG_CHUNK positions, keeps one accumulator per tap in tensor
-// memory, and adds them to dw (FP32, zeroed by the caller) with atomics.
+// one position), so they are staged without transposition: 8 consecutive
+// positions of one channel chunk form a core matrix (16-byte rows), channel
+// chunks are a fixed stride apart (SBO).  gy (A): chunk c of position k at
+// (c * WG_K + k) * 16 bytes.  A CTA takes one (kz, ky) row of taps (kx = 0..2;
+// the single tap of a 1x1x1 kernel) over WG_CHUNK positions, keeps one
+// accumulator per tap in tensor memory, and adds them to dw (FP32, zeroed by
+// the caller) with atomics.
+//
+// x (B), ROWS form (W % 8 == 0): the WG_K positions of a stage are R = WG_K /
+// SEG segments of SEG consecutive x positions of one row (SEG = 64, 32, 16 or
+// 8, dividing W), each staged once with a one-position periodic halo on both
+// sides, shifted by (dz, dy): chunk c of halo position h of segment r at
+// (c * XS + r * (SEG + 2) + h) * 16 bytes, XS = R * (SEG + 2).  The three kx
+// taps read the same staged rows, offset by kx units; the two core matrices
+// of a K-step are 128 bytes apart inside a segment (SEG >= 16) or one segment
+// apart (SEG = 8).  Gather form (other W): per tap, the shifted row of each
+// position, chunk c of position k at (c * WG_K + k) * 16 bytes.
+//
+// The stages go through a ring of WS slots: every thread copies its share of
+// stage v with cp.async (one commit group per stage; items run chunk-fastest so
+// a warp's copies are coalesced), and at stage u waits only for its own group
+// of stage u (WS - 2 newer groups may still be in flight), fences and arrives
+// on full[u % WS]; thread 0 issues the stage's MMAs once all 128 arrived and
+// commits them to empty[u % WS], which each thread waits for before it refills
+// the slot.
 constexpr int WG_K = 64;        // positions per stage (4 MMA K-steps)
 constexpr int WG_CHUNK = 2048;  // positions per CTA
+constexpr int WG_STAGES = WG_CHUNK / WG_K;
 
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// The MMA reads A as 128 rows (16 chunks of WG_K positions from the slot's
+// start): rows at and above cout read whatever follows (the slot's B, the next
+// slot), and their accumulator rows are never stored.  The ring is padded so
+// that the last slot's 16 chunks stay inside it.
+__host__ __device__ constexpr int wgrad_ring_units(int ws, int st_units) {
+    return (ws - 1) * st_units + (st_units > 16 * WG_K ? st_units : 16 * WG_K);
+}
+// 16-byte units of one slot: gy, then x (ROWS form: seg > 0)
+__host__ __device__ constexpr int wgrad_slot_units(int cin, int cout, int ntap, int seg) {
+    return (cout / 8) * WG_K + (seg > 0 ? (cin / 8) * (WG_K / seg) * (seg + 2) : ntap * (cin / 8) * WG_K);
+}
+
+template <int WS, bool ROWS>
 __global__ void __launch_bounds__(CONV_M) k_conv3d_wgrad_umma(const uint4 *__restrict__ x, const uint4 *__restrict__ gy,
                                                               float *__restrict__ dw, int B, int D, int H, int W, int cin,
-                                                              int cout, int taps, uint32_t tmem_cols) {
+                                                              int cout, int taps, uint32_t tmem_cols, int seg) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int ntap = taps == 27 ? 3 : 1;
     const int xc = cin / 8, gc = cout / 8;             // 16-byte chunks per position
-    const int a_units = 16 * WG_K, b_units = xc * WG_K; // A: 128 rows (16 chunks), B per tap
-    const int st_units = a_units + ntap * b_units;
+    const int R = ROWS ? WG_K / seg : 0, SW = seg + 2, XS = R * SW;
+    const int a_units = gc * WG_K, b_units = xc * WG_K; // A: the cout rows; B per tap (gather form)
+    const int st_units = wgrad_slot_units(cin, cout, ntap, ROWS ? seg : 0);
     uint4 *stage0 = (uint4 *)smem_raw;
-    uint64_t *bar = (uint64_t *)(stage0 + 2 * st_units);
-    uint32_t *tmem_slot = (uint32_t *)(bar + 2);
+    uint64_t *full = (uint64_t *)(stage0 + wgrad_ring_units(WS, st_units)), *empty = full + WS;
+    uint32_t *tmem_slot = (uint32_t *)(empty + WS);
+    long long *seg_row = (long long *)(empty + WS + 1);  // ROWS: per (stage, segment) shifted row start, -1 past the end
+    int *seg_x0 = (int *)(seg_row + WG_STAGES * R);       // ROWS: x of the segment's first position
     const int tid = threadIdx.x, warp = tid >> 5;
     const long long npos = (long long)B * D * H * W;
     const long long p0 = (long long)blockIdx.x * WG_CHUNK;
     const int g = blockIdx.y;  // tap row: kz = g / 3, ky = g % 3
-    // rows of A beyond cout stay zero in both stages
-    for (int i = tid; i < 2 * st_units; i += CONV_M) stage0[i] = make_uint4(0, 0, 0, 0);
+    const int dz = taps == 27 ? g / 3 - 1 : 0, dy = taps == 27 ? g % 3 - 1 : 0;
     if (tid == 0) {
-        mbar_init(bar, 1);
-        mbar_init(bar + 1, 1);
+        for (int s = 0; s < WS; s++) {
+            mbar_init(full + s, CONV_M);
+            mbar_init(empty + s, 1);
+        }
+    }
+    if (ROWS) {
+        for (int e = tid; e < WG_STAGES * R; e += CONV_M) {
+            const long long ps = p0 + (long long)e * seg;  // stage e / R, segment e % R
+            long long base = -1;
+            int x0 = 0;
+            if (ps < npos) {
+                long long q = ps / W;
+                x0 = (int)(ps - q * W);
+                int y = (int)(q % H) + dy;
+                q /= H;
+                int z = (int)(q % D) + dz;
+                const long long n = q / D;
+                y += y < 0 ? H : 0;
+                y -= y >= H ? H : 0;
+                z += z < 0 ? D : 0;
+                z -= z >= D ? D : 0;
+                base = ((n * D + z) * H + y) * W;
+            }
+            seg_row[e] = base;
+            seg_x0[e] = x0;
+        }
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
@@ -362,70 +470,116 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_wgrad_umma(const uint4 *__res
     // M = 128, N = cin, both operands MN-major, FP32 accumulate
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(cin >> 3) << 17) |
                            ((uint32_t)(CONV_M >> 4) << 24);
-    const int k = tid & (WG_K - 1), half = tid / WG_K;  // two threads per staged position
-    const int nst = WG_CHUNK / WG_K;
-    bool ok = true;
-    for (int u = 0; u < nst; u++) {
-        const int st = u & 1;
-        if (u >= 2 && !__syncthreads_and(mbar_wait(bar + st, ((u >> 1) - 1) & 1))) {
-            ok = false;
-            break;
-        }
-        uint4 *sa = stage0 + st * st_units, *sb = sa + a_units;
-        const long long p = p0 + (long long)u * WG_K + k;
-        const bool valid = p < npos;
-        int n = 0, z = 0, y = 0, xx = 0;
-        if (valid) {
-            long long q = p;
-            xx = (int)(q % W);
-            q /= W;
-            y = (int)(q % H);
-            q /= H;
-            z = (int)(q % D);
-            n = (int)(q / D);
-        }
-        for (int c = half; c < gc; c += 2) {
-            if (valid) cp_async16(sa + c * WG_K + k, gy + p * gc + c);
+    const float rgc = 1.0f / (float)gc, rxc = 1.0f / (float)xc, rsw = 1.0f / (float)SW;
+    // this thread's copies of stage v into its slot (zeros beyond the last position)
+    auto load = [&](int v) {
+        uint4 *sa = stage0 + (v % WS) * st_units, *sb = sa + a_units;
+        const long long pv = p0 + (long long)v * WG_K;
+        // gy: WG_K positions x gc chunks, contiguous in global memory
+        for (int i = tid; i < WG_K * gc; i += CONV_M) {
+            const int k = (int)(((float)i + 0.5f) * rgc), c = i - k * gc;
+            if (pv + k < npos) cp_async16(sa + c * WG_K + k, gy + pv * gc + i);
             else sa[c * WG_K + k] = make_uint4(0, 0, 0, 0);
         }
-        for (int j = 0; j < ntap; j++) {
-            uint4 *dst = sb + j * b_units + k;
-            if (valid) {
-                int dz = 0, dy = 0, dx = 0;
-                if (taps == 27) {
-                    dz = g / 3 - 1;
-                    dy = g % 3 - 1;
-                    dx = j - 1;
+        if (ROWS) {
+            // x: R segments x (SEG + 2) halo positions x xc chunks
+            for (int i = tid; i < XS * xc; i += CONV_M) {
+                const int q = (int)(((float)i + 0.5f) * rxc), c = i - q * xc;
+                const int r = (int)(((float)q + 0.5f) * rsw), h = q - r * SW;
+                const int e = v * R + r;
+                const long long base = seg_row[e];
+                uint4 *dst = sb + c * XS + r * SW + h;
+                if (base >= 0) {
+                    int xw = seg_x0[e] + h - 1;
+                    xw += xw < 0 ? W : 0;
+                    xw -= xw >= W ? W : 0;
+                    cp_async16(dst, x + (base + xw) * xc + c);
+                } else {
+                    *dst = make_uint4(0, 0, 0, 0);
                 }
-                const int zz = (z + dz + D) % D, yy = (y + dy + H) % H, x2 = (xx + dx + W) % W;
-                const uint4 *src = x + ((((long long)n * D + zz) * H + yy) * W + x2) * xc;
-                for (int c = half; c < xc; c += 2) cp_async16(dst + c * WG_K, src + c);
-            } else {
-                for (int c = half; c < xc; c += 2) dst[c * WG_K] = make_uint4(0, 0, 0, 0);
+            }
+        } else {
+            // x: per tap the shifted row of each position
+            for (int i = tid; i < ntap * WG_K * xc; i += CONV_M) {
+                const int q = (int)(((float)i + 0.5f) * rxc), c = i - q * xc;
+                const int j = q / WG_K, k = q - j * WG_K;
+                uint4 *dst = sb + j * b_units + c * WG_K + k;
+                const long long p = pv + k;
+                if (p < npos) {
+                    long long t = p / W;
+                    int xx = (int)(p - t * W) + (taps == 27 ? j - 1 : 0);
+                    int y = (int)(t % H) + dy;
+                    t /= H;
+                    int z = (int)(t % D) + dz;
+                    const long long n = t / D;
+                    xx += xx < 0 ? W : 0;
+                    xx -= xx >= W ? W : 0;
+                    y += y < 0 ? H : 0;
+                    y -= y >= H ? H : 0;
+                    z += z < 0 ? D : 0;
+                    z -= z >= D ? D : 0;
+                    cp_async16(dst, x + (((n * D + z) * H + y) * W + xx) * xc + c);
+                } else {
+                    *dst = make_uint4(0, 0, 0, 0);
+                }
             }
         }
-        cp_async_wait_all();
+    };
+    // one commit group per stage (empty past the last), so group u holds stage u
+    for (int v = 0; v < WS - 1; v++) {
+        if (v < WG_STAGES) load(v);
+        cp_async_commit();
+    }
+    bool ok = true;
+    int u = 0;
+    for (; u < WG_STAGES; u++) {
+        const int st = u % WS;
+        cp_async_wait_group<WS - 2>();  // this thread's stage u has landed (WS - 2 newer groups may not)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
+        mbar_arrive(full + st);
         if (tid == 0) {
+            if (!mbar_wait(full + st, (u / WS) & 1)) {
+                ok = false;
+                break;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t a0 = smem_addr(sa), b0 = smem_addr(sb);
+            const uint32_t a0 = smem_addr(stage0 + st * st_units), b0 = a0 + (uint32_t)a_units * 16;
             for (int s = 0; s < WG_K / 16; s++) {
                 const uint64_t da = umma_desc(a0 + (uint32_t)(16 * s * 16), 128, WG_K * 16);
                 for (int j = 0; j < ntap; j++) {
-                    const uint64_t db = umma_desc(b0 + (uint32_t)((j * b_units + 16 * s) * 16), 128, WG_K * 16);
+                    uint64_t db;
+                    if (ROWS) {
+                        const int k0 = 16 * s, r = k0 / seg;
+                        const int unit = r * SW + (k0 - r * seg) + (taps == 27 ? j : 1);
+                        db = umma_desc(b0 + (uint32_t)unit * 16, seg >= 16 ? 128u : (uint32_t)SW * 16, (uint32_t)XS * 16);
+                    } else {
+                        db = umma_desc(b0 + (uint32_t)((j * b_units + 16 * s) * 16), 128, WG_K * 16);
+                    }
                     umma_bf16(tmem + (uint32_t)(j * cin), da, db, idesc, (u > 0 || s > 0) ? 1u : 0u);
                 }
             }
-            umma_commit(bar + st);
+            umma_commit(empty + st);
         }
+        // refill the slot of stage u - 1 with stage u + WS - 1 once its MMAs are done
+        const int v = u + WS - 1;
+        if (v < WG_STAGES) {
+            if (v >= WS && !mbar_wait(empty + v % WS, (v / WS - 1) & 1)) {
+                ok = false;
+                break;
+            }
+            load(v);
+        }
+        cp_async_commit();
     }
+    cp_async_wait_all();
     {
-        const bool fin = ok ? mbar_wait(bar + ((nst - 1) & 1), ((nst - 1) >> 1) & 1) : false;
+        // the last stage's MMAs are the last to complete (one thread issues them in order)
+        const bool fin = __syncthreads_and(ok) ? mbar_wait(empty + (WG_STAGES - 1) % WS, ((WG_STAGES - 1) / WS) & 1) : false;
         ok = __syncthreads_and(fin);
     }
     if (!ok) {
-        mbar_wait(bar + ((nst - 1) & 1), ((nst - 1) >> 1) & 1);
+        // a second bounded wait for MMAs still in flight: the last stage thread 0 committed
+        if (tid == 0 && u > 0) mbar_wait(empty + (u - 1) % WS, ((u - 1) / WS) & 1);
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int co = 32 * warp + (tid & 31);  // accumulator row of this thread
@@ -465,18 +619,40 @@ extern "C" int lfts_conv3d_wgrad_bf16(void *stream, const void *x, const void *g
     const int ntap = taps == 27 ? 3 : 1;
     uint32_t cols = 32;
     while ((int)cols < ntap * cin) cols <<= 1;
-    const size_t st_units = (size_t)16 * lfts::unet::WG_K + (size_t)ntap * (cin / 8) * lfts::unet::WG_K;
-    const size_t smem = 2 * 16 * st_units + 2 * sizeof(uint64_t) + 16;
-    if (smem > 200 * 1024) return fail("conv3d wgrad: cin too large for the shared-memory stages");
     if (cout > 128) return fail("conv3d wgrad: cout (the accumulator rows) must be <= 128");
-    {
-        cudaError_t e = cudaFuncSetAttribute(lfts::unet::k_conv3d_wgrad_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        if (e != cudaSuccess) return fail(std::string("conv3d wgrad: ") + cudaGetErrorString(e));
+    using namespace lfts::unet;
+    // x staged as row segments with a halo when W % 8 == 0 (segment: the longest of 64, 32, 16, 8 dividing W)
+    const int seg = W % 64 == 0 ? 64 : W % 32 == 0 ? 32 : W % 16 == 0 ? 16 : W % 8 == 0 ? 8 : 0;
+    const int st_units = wgrad_slot_units(cin, cout, ntap, seg);
+    const size_t table = seg ? (size_t)WG_STAGES * (WG_K / seg) * (sizeof(long long) + sizeof(int)) : 0;
+    auto smem_of = [&](int ws) {
+        return (size_t)16 * wgrad_ring_units(ws, st_units) + (2 * (size_t)ws + 1) * sizeof(uint64_t) + table + 16;
+    };
+    // ring depth: the most stages in flight per SM (CTAs per SM by shared memory
+    // and tensor-memory columns, times WS - 1); ties go to the deeper ring
+    int WS = 0, best = 0;
+    for (int ws = 2; ws <= 4; ws++) {
+        if (smem_of(ws) > 200 * 1024) continue;
+        int ctas = (int)((228 * 1024) / (smem_of(ws) + 1024));
+        if (ctas > (int)(512 / cols)) ctas = (int)(512 / cols);
+        if (ctas * (ws - 1) >= best) {
+            best = ctas * (ws - 1);
+            WS = ws;
+        }
     }
-    lfts::unet::k_conv3d_wgrad_umma<<<dim3((unsigned)chunks, taps == 27 ? 9 : 1), lfts::unet::CONV_M, smem,
-                                      (cudaStream_t)stream>>>((const uint4 *)x, (const uint4 *)gy, dw, B, D, H, W, cin, cout,
-                                                              taps, cols);
-    cudaError_t e = cudaPeekAtLastError();
+    if (const char *env = std::getenv("LFTS_CONV_WGRAD_RING")) {  // 2, 3 or 4 overrides the choice
+        const int ws = env[0] - '0';
+        if (ws >= 2 && ws <= 4 && smem_of(ws) <= 200 * 1024) WS = ws;
+    }
+    if (WS == 0) return fail("conv3d wgrad: cin too large for the shared-memory stages");
+    using Kern = void (*)(const uint4 *, const uint4 *, float *, int, int, int, int, int, int, int, uint32_t, int);
+    Kern kern = seg ? (WS == 2 ? k_conv3d_wgrad_umma<2, true> : WS == 3 ? k_conv3d_wgrad_umma<3, true> : k_conv3d_wgrad_umma<4, true>)
+                    : (WS == 2 ? k_conv3d_wgrad_umma<2, false> : WS == 3 ? k_conv3d_wgrad_umma<3, false> : k_conv3d_wgrad_umma<4, false>);
+    cudaError_t e = cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess) return fail(std::string("conv3d wgrad: ") + cudaGetErrorString(e));
+    kern<<<dim3((unsigned)chunks, taps == 27 ? 9 : 1), CONV_M, smem_of(WS), (cudaStream_t)stream>>>(
+        (const uint4 *)x, (const uint4 *)gy, dw, B, D, H, W, cin, cout, taps, cols, seg);
+    e = cudaPeekAtLastError();
     if (e != cudaSuccess) return fail(std::string("conv3d wgrad launch: ") + cudaGetErrorString(e));
     return 0;
 }
@@ -496,23 +672,43 @@ extern "C" int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, c
     if (blocks > 0x7fffffffLL) return fail("conv3d: too many positions");
     uint32_t cols = 32;
     while ((int)cols < cout) cols <<= 1;
-    {
-        // halo-staged kernel: 3x3x3, H % 16 == 0, W % 8 == 0, halo + weight stages within 200 KB
+    if (taps == 27 && H % lfts::unet::HT_Y == 0 && W % lfts::unet::HT_X == 0) {
+        // halo-staged kernel: TZ output planes per CTA, a ring of NS weight stages
         using namespace lfts::unet;
-        // weight stages: as many (2..4) as fit beside the halo in 200 KB
-        auto hs = [&](int ns) {
-            return (size_t)16 * ((size_t)(cin / 8) * HPLANE + (size_t)ns * (cin / 8) * cout) + (2 * (size_t)ns + 1) * sizeof(uint64_t) + 16;
+        auto hs = [&](int tz, int ns) {
+            return (size_t)16 * ((size_t)(cin / 8) * ((tz + 2) * HROW + 1) + (size_t)ns * (cin / 8) * cout) +
+                   (2 * (size_t)ns + 1) * sizeof(uint64_t) + 16;
         };
-        int NS = 4;
-        while (NS > 2 && hs(NS) > 200 * 1024) NS--;
-        const size_t hsmem = hs(NS);
-        if (taps == 27 && H % HT_Y == 0 && W % HT_X == 0 && hsmem <= 200 * 1024 && (long long)B * D <= 65535) {
+        // CTAs per SM that the shared memory allows (228 KB per SM, 1 KB reserved per CTA)
+        auto fit = [](size_t smem) { return (int)((228 * 1024) / (smem + 1024)); };
+        // the most weight stages (2..8) within 200 KB that keep the occupancy of two stages
+        auto stages = [&](int tz) {
+            int ns = 8;
+            while (ns > 2 && (hs(tz, ns) > 200 * 1024 || fit(hs(tz, ns)) < fit(hs(tz, 2)))) ns--;
+            return ns;
+        };
+        // two output planes per CTA when the halo of 4 planes keeps two CTAs per SM (LFTS_CONV_TZ=1|2 overrides)
+        int tz = (D % 2 == 0 && 2 * cout <= 256 && hs(2, 2) <= 200 * 1024 && fit(hs(2, 2)) >= 2) ? 2 : 1;
+        if (const char *env = std::getenv("LFTS_CONV_TZ")) {
+            if (env[0] == '1') tz = 1;
+            if (env[0] == '2' && D % 2 == 0 && 2 * cout <= 512 && hs(2, 2) <= 200 * 1024) tz = 2;
+        }
+        const int NS = stages(tz);
+        const size_t hsmem = hs(tz, NS);
+        uint32_t hcols = 32;
+        while ((int)hcols < tz * cout) hcols <<= 1;
+        if (hsmem <= 200 * 1024 && (long long)B * D / tz <= 65535) {
             // per device (the attribute belongs to the current device), so set on every call
-            cudaError_t e = cudaFuncSetAttribute(k_conv3d_halo_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaError_t e = tz == 2 ? cudaFuncSetAttribute(k_conv3d_halo_umma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)
+                                    : cudaFuncSetAttribute(k_conv3d_halo_umma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             if (e != cudaSuccess) return fail(std::string("conv3d: ") + cudaGetErrorString(e));
-            k_conv3d_halo_umma<<<dim3((unsigned)(W / HT_X), (unsigned)(H / HT_Y), (unsigned)(B * D)), CONV_M, hsmem,
-                                 (cudaStream_t)stream>>>((const uint4 *)in, (const uint4 *)wpk, bias, (uint16_t *)out, B, D, H,
-                                                         W, cin, cout, relu, cols, NS);
+            const dim3 grid((unsigned)(W / HT_X), (unsigned)(H / HT_Y), (unsigned)(B * D / tz));
+            if (tz == 2)
+                k_conv3d_halo_umma<2><<<grid, CONV_M, hsmem, (cudaStream_t)stream>>>(
+                    (const uint4 *)in, (const uint4 *)wpk, bias, (uint16_t *)out, B, D, H, W, cin, cout, relu, hcols, NS);
+            else
+                k_conv3d_halo_umma<1><<<grid, CONV_M, hsmem, (cudaStream_t)stream>>>(
+                    (const uint4 *)in, (const uint4 *)wpk, bias, (uint16_t *)out, B, D, H, W, cin, cout, relu, hcols, NS);
             e = cudaPeekAtLastError();
             if (e != cudaSuccess) return fail(std::string("conv3d launch: ") + cudaGetErrorString(e));
             return 0;

@@ -51,6 +51,57 @@ def test_conv_matches_torch(cin, cin_pad, cout, k, grid, batch, relu):
     assert float(got[..., cout:].abs().max() if got.shape[-1] > cout else 0) == 0.0  # padded channels stay zero
 
 
+@pytest.mark.parametrize("tz", ["1", "2"])
+@pytest.mark.parametrize("cin,cin_pad,cout,grid,batch", [
+    (2, 16, 24, (16, 16, 16), 2), (24, 32, 48, (8, 32, 16), 1), (48, 48, 48, (4, 16, 8), 3),
+    (96, 96, 96, (6, 32, 24), 1), (72, 80, 24, (2, 16, 8), 2)])
+def test_conv_halo_tiles(monkeypatch, tz, cin, cin_pad, cout, grid, batch):
+    """The halo kernel with one and with two output planes per CTA (the
+    LFTS_CONV_TZ override), each with the ring depth its shared memory allows."""
+    import torch
+    from langevinfts_b200.learned import conv3d_tcgen05, pack_conv
+    monkeypatch.setenv("LFTS_CONV_TZ", tz)
+    torch.manual_seed(cin * 17 + cout)
+    conv = torch.nn.Conv3d(cin, cout, 3).cuda()
+    x = torch.randn(batch, cin, *grid, device="cuda").to(torch.bfloat16).float()
+    layer = pack_conv(conv, list(range(cin)), cin_pad)
+    h = torch.nn.functional.pad(x.permute(0, 2, 3, 4, 1), (0, cin_pad - cin)).to(torch.bfloat16).contiguous()
+    got = conv3d_tcgen05(h, layer, True).float()
+    torch.cuda.synchronize()
+    ref = _reference(x, conv, True).permute(0, 2, 3, 4, 1)
+    assert float((got[..., :cout] - ref).abs().max()) <= 8e-3 * float(ref.abs().max()) + 1e-6
+
+
+@pytest.mark.parametrize("ws", ["2", "3", "4"])
+@pytest.mark.parametrize("cin,cout,k,grid,batch", [
+    (32, 32, 3, (16, 16, 16), 2), (48, 96, 3, (16, 16, 16), 1), (80, 32, 3, (6, 16, 16), 3), (32, 16, 1, (8, 8, 8), 1),
+    (32, 16, 3, (2, 8, 64), 2), (32, 32, 3, (2, 4, 96), 3), (16, 16, 3, (4, 8, 24), 2),  # row segments of 64, 32, 8
+    (16, 32, 3, (4, 6, 12), 2)])  # W % 8 != 0: per-tap gathers
+def test_wgrad_ring_depths(monkeypatch, ws, cin, cout, k, grid, batch):
+    """lfts_conv3d_wgrad_bf16 with every ring depth (the LFTS_CONV_WGRAD_RING
+    override) against torch's FP32 weight gradient of the same BF16 operands,
+    over several 2048-position chunks and a ragged last chunk, for x staged as
+    row segments of every length and as per-tap gathers."""
+    import torch
+    import torch.nn.functional as F
+    from langevinfts_b200.capi import check, lib
+    monkeypatch.setenv("LFTS_CONV_WGRAD_RING", ws)
+    torch.manual_seed(cin + cout + k)
+    x = torch.randn(batch, *grid, cin, device="cuda").to(torch.bfloat16)
+    gy = torch.randn(batch, *grid, cout, device="cuda").to(torch.bfloat16)
+    taps = k ** 3
+    dw = torch.zeros(taps, cout, cin, device="cuda")
+    check(lib().lfts_conv3d_wgrad_bf16(torch.cuda.current_stream().cuda_stream, x.data_ptr(), gy.data_ptr(), dw.data_ptr(),
+                                       batch, *grid, cin, cout, taps))
+    torch.cuda.synchronize()
+    xc = x.float().permute(0, 4, 1, 2, 3)
+    xp = F.pad(xc, (k // 2,) * 6, mode="circular") if k > 1 else xc
+    # dw[co][ci][kz][ky][kx] = sum_p gy[p][co] x[p + tap - 1][ci]
+    ref = torch.nn.grad.conv3d_weight(xp, (cout, cin, k, k, k), gy.float().permute(0, 4, 1, 2, 3))
+    ref = ref.permute(2, 3, 4, 0, 1).reshape(taps, cout, cin)
+    assert _rel(dw, ref) < 1e-4
+
+
 def test_tcgen05_unet_matches_torch_model():
     import torch
     from langevinfts_b200.learned import TcgenUNet, UNet3D
