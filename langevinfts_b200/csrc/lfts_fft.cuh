@@ -32,6 +32,28 @@ template <> struct CT<float> { using type = float2; };
 template <typename C> __device__ __forceinline__ C cmk(double re, double im) { C c; c.x = re; c.y = im; return c; }
 template <typename C> __device__ __forceinline__ C cadd(C a, C b) { a.x += b.x; a.y += b.y; return a; }
 template <typename C> __device__ __forceinline__ C csub(C a, C b) { a.x -= b.x; a.y -= b.y; return a; }
+// FP32 complex add and subtract as one packed instruction each (add / sub
+// .rn.f32x2 of sm_100: each lane rounded to nearest, as two scalar adds are)
+__device__ __forceinline__ unsigned long long pack2(float2 a) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long r) {
+    float2 a;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
+    return unpack2(r);
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
+    return unpack2(r);
+}
 template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
     C c;
     c.x = a.x * b.x - a.y * b.y;

@@ -3,9 +3,11 @@
 After the Langevin update of the real (exchange) fields w_-, the saddle-point
 search over the imaginary (pressure) fields w_+ normally starts from the
 previous step's saddle point.  Here a 3-level periodic 3D U-Net predicts the
-new saddle point from (new w_-, previous w_+) and the search starts there:
+new saddle point from the new w_-, the previous w_+ and the step's change of
+w_- (dw_- = w_- - w_-prev, which drives the shift of the saddle point), and
+the search starts there:
 
-    w_+start = w_+prev + s_out * UNet([w_- / s_in, w_+prev / s_out])
+    w_+start = w_+prev + s_out * UNet([w_- / s_in, w_+prev / s_out, dw_- / s_d])
 
 The network adds a residual to the warm start; its last layer starts at zero,
 so an untrained model reproduces the plain warm start exactly.  The search
@@ -24,8 +26,8 @@ Pieces:
                     on the tensor cores (_ConvFn: input gradient by the forward
                     kernel with mirrored taps, weight gradient by
                     lfts_conv3d_wgrad_bf16).
-  generate_pairs    training pairs from the plain solver: inputs (w_-, w_+prev)
-                    and target w_+ of every replica and step.
+  generate_pairs    training pairs from the plain solver: inputs (w_-, w_+prev,
+                    dw_-) and target w_+ of every replica and step.
   FlatAdamW         AdamW on this library's kernel (lfts_adamw_f32): the
                     parameters live in one flat FP32 buffer, one launch a step.
   train             AdamW on the mean-squared error of the residual; by default
@@ -33,10 +35,11 @@ Pieces:
                     cores and the update by FlatAdamW (tcgen05=False: torch's
                     convolutions under BF16 autocast and torch's AdamW, kept as
                     the comparison).
-  LearnedStart      the callable BatchedLFTS.step(start=...) uses: reads w_aux
-                    on the device (zero copy), writes the predicted w_+ in place
-                    on the engine's stream; inference on the tensor cores by
-                    default.
+  LearnedStart      the callable BatchedLFTS.step(start=...) uses: keeps a
+                    device copy of w_- before each Langevin update
+                    (before_update), reads w_aux on the device (zero copy),
+                    writes the predicted w_+ in place on the engine's stream;
+                    inference on the tensor cores by default.
 
 Pooling, upsampling and concatenation are torch tensor operations between the
 convolutions.  Grids must have extents divisible by 4.
@@ -89,9 +92,9 @@ class UNet3D(nn.Module):
 def generate_pairs(sim, nsteps):
     """Run nsteps plain Langevin steps of a started BatchedLFTS and collect, per
     replica and step that met the tolerance, the network inputs (w_- after the
-    update, w_+ before the search) and the target (w_+ at the saddle point).
-    Returns float32 arrays X [n, 2, nx, ny, nz], Y [n, 1, nx, ny, nz] and the
-    saddle iterations of the steps."""
+    update, w_+ before the search, and the update's change of w_-) and the
+    target (w_+ at the saddle point).  Returns float32 arrays X [n, 3, nx, ny,
+    nz], Y [n, 1, nx, ny, nz] and the saddle iterations of the steps."""
     shape = list(sim.cb.get_nx())
     ri, ii = sim.mpt.aux_fields_real_idx, sim.mpt.aux_fields_imag_idx
     if len(ri) != 1 or len(ii) != 1:
@@ -104,7 +107,8 @@ def generate_pairs(sim, nsteps):
         for r in range(sim.R):
             if st["failed"][r]:
                 continue
-            X.append(np.stack([w[r, ri[0]], w_prev[r, ii[0]]]).reshape([2] + shape).astype(np.float32))
+            X.append(np.stack([w[r, ri[0]], w_prev[r, ii[0]], w[r, ri[0]] - w_prev[r, ri[0]]]).reshape([3] + shape)
+                     .astype(np.float32))
             Y.append(w[r, ii[0]].reshape([1] + shape).astype(np.float32))
         iters += list(st["iterations"])
         w_prev = w
@@ -331,22 +335,41 @@ class LearnedStart:
     tcgen05=True (default): every convolution on this library's tensor-core
     kernel; False: torch's convolutions under BF16 autocast."""
 
-    def __init__(self, model, s_in, s_out, batch=8, tcgen05=True):
+    def __init__(self, model, s_in, s_out, s_d=None, batch=8, tcgen05=True):
         self.model, self.s_in, self.s_out, self.batch = model.eval(), float(s_in), float(s_out), batch
+        # s_d: scale of the third input channel, the update's change of w_- (None: a two-channel network)
+        self.s_d = None if s_d is None else float(s_d)
+        self._wm_prev = None
         # tcgen05=True: the convolutions run on this library's tensor-core kernel
         self.net = TcgenUNet(self.model) if tcgen05 else None
+
+    @torch.no_grad()
+    def before_update(self, sim):
+        """Device copy of every replica's w_- before the Langevin update, on the
+        engine's stream (BatchedLFTS.step calls it when the start has it)."""
+        if self.s_d is None:
+            return
+        ri = sim.mpt.aux_fields_real_idx[0]
+        with torch.cuda.stream(torch.cuda.ExternalStream(sim.engine.stream_ptr())):
+            w = torch.as_tensor(_DeviceArray(sim.engine.w_aux_ptr(), (sim.R, sim.S, sim.M)), device="cuda")
+            self._wm_prev = w[:, ri].clone()
 
     @torch.no_grad()
     def __call__(self, sim):
         shape = list(sim.cb.get_nx())
         R, S, M = sim.R, sim.S, sim.M
         ri, ii = sim.mpt.aux_fields_real_idx[0], sim.mpt.aux_fields_imag_idx[0]
+        if self.s_d is not None and (self._wm_prev is None or self._wm_prev.shape != (R, M)):
+            raise RuntimeError("LearnedStart: no copy of w_- from before this step's update (before_update)")
         stream = torch.cuda.ExternalStream(sim.engine.stream_ptr())
         with torch.cuda.stream(stream):
             w = torch.as_tensor(_DeviceArray(sim.engine.w_aux_ptr(), (R, S, M)), device="cuda")
             for r0 in range(0, R, self.batch):
                 wr = w[r0:r0 + self.batch]
-                x = torch.stack([wr[:, ri] / self.s_in, wr[:, ii] / self.s_out], 1).float().reshape([-1, 2] + shape)
+                ch = [wr[:, ri] / self.s_in, wr[:, ii] / self.s_out]
+                if self.s_d is not None:
+                    ch.append((wr[:, ri] - self._wm_prev[r0:r0 + self.batch]) / self.s_d)
+                x = torch.stack(ch, 1).float().reshape([-1, len(ch)] + shape)
                 if self.net is not None:
                     d = self.net(x)
                 else:
@@ -391,17 +414,19 @@ def ablation(sim, starts, nsteps):
 
 def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_decay=1e-4, seed=0, log=None, tcgen05=True):
     """AdamW on MSE of the scaled residual target (Y - w_+prev) / s_out until
-    `seconds` or `epochs` run out.  tcgen05=True (default): every convolution's
+    `seconds` or `epochs` run out.  X holds 2 input channels (w_-, w_+prev) or
+    3 (and dw_-), each scaled by its standard deviation.  tcgen05=True (default): every convolution's
     forward and backward on this library's tensor-core kernels and the update
     by FlatAdamW (lfts_adamw_f32); False: BF16 autocast over torch's
     convolutions and torch's AdamW.  Returns (LearnedStart, history of (epoch,
     mean loss))."""
     torch.manual_seed(seed)
-    s_in = float(np.std(X[:, 0])) or 1.0
-    s_out = float(np.std(X[:, 1])) or 1.0
-    xin = torch.from_numpy(np.concatenate([X[:, :1] / s_in, X[:, 1:] / s_out], 1)).cuda()
-    tgt = torch.from_numpy((Y - X[:, 1:]) / s_out).cuda()
-    model = UNet3D(cin=2, cout=1, base=base).cuda()
+    scales = [float(np.std(X[:, c])) or 1.0 for c in range(X.shape[1])]
+    s_in, s_out = scales[0], scales[1]
+    s_d = scales[2] if X.shape[1] > 2 else None
+    xin = torch.from_numpy(np.concatenate([X[:, c:c + 1] / scales[c] for c in range(X.shape[1])], 1)).cuda()
+    tgt = torch.from_numpy((Y - X[:, 1:2]) / s_out).cuda()
+    model = UNet3D(cin=X.shape[1], cout=1, base=base).cuda()
     fwd = TcgenUNetTrain(model) if tcgen05 else None
     if tcgen05:
         opt = FlatAdamW(model.parameters(), lr=lr, weight_decay=weight_decay)
@@ -428,4 +453,4 @@ def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_dec
             log(f"epoch {ep} loss {tot / n:.4e}")
         if time.time() - t0 > seconds:
             break
-    return LearnedStart(model, s_in, s_out, tcgen05=tcgen05), hist
+    return LearnedStart(model, s_in, s_out, s_d, tcgen05=tcgen05), hist

@@ -343,10 +343,13 @@ class BatchedLFTS:
         """One Langevin step of every replica.  start (optional): a callable
         (e.g. learned.LearnedStart) run after the Langevin update and before the
         saddle-point search; it may change the imaginary fields on the device,
-        which the search then starts from."""
+        which the search then starts from.  A start with a before_update method
+        gets it called before the update."""
         if start is not None:
             import torch
             keep = None
+            if hasattr(start, "before_update"):
+                start.before_update(self)
             if self.noise == "device" and noise is None:
                 self.engine.langevin_update_rng(self.sigma)
             else:
@@ -376,6 +379,8 @@ class BatchedLFTS:
         if start is None:
             stats = self.engine.step_device(noise_ptr)
         else:
+            if hasattr(start, "before_update"):
+                start.before_update(self)
             self.engine.langevin_update_device(noise_ptr)
             start(self)
             stats = self.engine.finish_step()

@@ -49,7 +49,7 @@ def test_generate_pairs_and_training_lowers_the_loss():
     sim.start([{"A": rng.normal(0, 1, sim.M), "B": rng.normal(0, 1, sim.M)} for _ in range(sim.R)])
     w_before = sim.fields()
     X, Y, iters = generate_pairs(sim, 3)
-    assert X.shape == (12, 2, 16, 16, 16) and Y.shape == (12, 1, 16, 16, 16) and len(iters) == 12
+    assert X.shape == (12, 3, 16, 16, 16) and Y.shape == (12, 1, 16, 16, 16) and len(iters) == 12
     w_after = sim.fields()
     ri, ii = sim.mpt.aux_fields_real_idx[0], sim.mpt.aux_fields_imag_idx[0]
     # the last step's pairs: inputs (w_- now, w_+ of the step before), target w_+ now
@@ -58,6 +58,10 @@ def test_generate_pairs_and_training_lowers_the_loss():
     np.testing.assert_allclose(last[1][:, 0].reshape(sim.R, -1), w_after[:, ii].astype(np.float32), rtol=0, atol=0)
     first = X[:sim.R]
     np.testing.assert_allclose(first[:, 1].reshape(sim.R, -1), w_before[:, ii].astype(np.float32), rtol=0, atol=0)
+    # third channel: the update's change of w_- (w_- now minus w_- before the step), in FP32
+    np.testing.assert_allclose((first[:, 0].astype(np.float64) - first[:, 2]).reshape(sim.R, -1), w_before[:, ri],
+                               rtol=0, atol=1e-5)
+    np.testing.assert_allclose(last[0][:, 2], last[0][:, 0] - X[-2 * sim.R:-sim.R, 0], rtol=0, atol=1e-5)
     # the network can fit a handful of pairs: 150 AdamW steps on 4 of them
     start, hist = train(X[:4], Y[:4], base=8, seconds=120, epochs=150, batch=4, lr=3e-3)
     assert hist[-1][1] < 0.6 * hist[0][1], hist[:: max(1, len(hist) // 6)]
