@@ -537,7 +537,7 @@ def run_ensemble(args):
     f32 = sims["cuda-fp32"]
     restore(f32)
     t0 = time.time()
-    X, Y, _ = generate_pairs(f32, LEARNED_PAIR_STEPS)
+    X, Y, _ = generate_pairs(f32, learned_pair_steps(f32.R))
     start, hist = train(X, Y, seconds=args.learned_train)
     t_train = time.time() - t0
     _, edges, idx = radial_bins(sim, args.sf_bins)
@@ -738,9 +738,14 @@ def run_scft(args):
 
 # timed steps of each variant (capped so the default run stays within minutes)
 VARIANT_STEPS_MAX = 8
-# plain Langevin steps whose fields train the learned start, and its time budget (s)
-LEARNED_PAIR_STEPS = 16
+# plain Langevin steps whose fields train the learned start (about LEARNED_PAIRS
+# pairs: 16 steps at 64 replicas, 64 at 16), and its time budget (s)
+LEARNED_PAIRS = 1024
 LEARNED_TRAIN_S = 120.0
+
+
+def learned_pair_steps(replicas):
+    return int(min(64, max(16, -(-LEARNED_PAIRS // replicas))))
 
 
 def time_batched(sim, K, start=None):
@@ -791,7 +796,7 @@ def run_variants(args, value_fp64):
       fp32              FP32 propagators and FFTs, FP64 reductions (cuda-fp32)
       fp32_learned      the same with the learned saddle-point start: a U-Net
                         trained in this run (tensor-core kernels, AdamW kernel)
-                        on pairs from LEARNED_PAIR_STEPS plain FP32 steps
+                        on about LEARNED_PAIRS pairs from plain FP32 steps
       fp64_one_replica  the unbatched plain FP64 form: one replica per engine
     Each carries value, e2e, mean saddle iterations, failed steps and its
     ratio to the plain FP64 value."""
@@ -822,12 +827,13 @@ def run_variants(args, value_fp64):
                                   "platform": "cuda-fp32: FP32 propagators and FFTs, compensated FP64 reductions"})
     sys.stderr.write(f"[bench] fp32 {r[0]:.3f} {UNIT} ({np.mean(r[2]):.2f} iterations)\n")
     t0 = time.time()
-    X, Y, _ = generate_pairs(sim, LEARNED_PAIR_STEPS)
+    pair_steps = learned_pair_steps(sim.R)
+    X, Y, _ = generate_pairs(sim, pair_steps)
     t_pairs = time.time() - t0
     start, hist = train(X, Y, seconds=LEARNED_TRAIN_S)
     r = time_batched(sim, K, start=start)
     out["fp32_learned"] = entry(*r, sim, {
-        "dtype": "f32", "training_pairs": int(len(X)), "pair_steps": LEARNED_PAIR_STEPS, "pair_seconds": t_pairs,
+        "dtype": "f32", "training_pairs": int(len(X)), "pair_steps": pair_steps, "pair_seconds": t_pairs,
         "train_seconds": LEARNED_TRAIN_S, "epochs": len(hist), "loss_first_last": [hist[0][1], hist[-1][1]],
         "network": "3-level periodic 3D U-Net, 24 base channels; convolutions forward and backward on lfts_conv3d_bf16 / "
                    "lfts_conv3d_wgrad_bf16 (tcgen05), AdamW on lfts_adamw_f32, inference on lfts_conv3d_bf16"})

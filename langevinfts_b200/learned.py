@@ -412,10 +412,13 @@ def ablation(sim, starts, nsteps):
     return out
 
 
-def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_decay=1e-4, seed=0, log=None, tcgen05=True):
+def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_decay=1e-4, seed=0, log=None, tcgen05=True,
+          schedule="cosine"):
     """AdamW on MSE of the scaled residual target (Y - w_+prev) / s_out until
     `seconds` or `epochs` run out.  X holds 2 input channels (w_-, w_+prev) or
-    3 (and dw_-), each scaled by its standard deviation.  tcgen05=True (default): every convolution's
+    3 (and dw_-), each scaled by its standard deviation.  schedule "cosine":
+    the learning rate falls from lr to 0 over the time budget (half a cosine
+    in elapsed time); "constant": lr throughout.  tcgen05=True (default): every convolution's
     forward and backward on this library's tensor-core kernels and the update
     by FlatAdamW (lfts_adamw_f32); False: BF16 autocast over torch's
     convolutions and torch's AdamW.  Returns (LearnedStart, history of (epoch,
@@ -432,12 +435,27 @@ def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_dec
         opt = FlatAdamW(model.parameters(), lr=lr, weight_decay=weight_decay)
     else:
         opt = torch.optim.AdamW(model.parameters(), lr=lr, weight_decay=weight_decay)
+    if schedule not in ("cosine", "constant"):
+        raise ValueError('schedule must be "cosine" or "constant"')
+
+    def set_lr(v):
+        if tcgen05:
+            opt.lr = v
+        else:
+            for g in opt.param_groups:
+                g["lr"] = v
     n = xin.shape[0]
-    hist, t0 = [], time.time()
+    hist, t0, out_of_time = [], time.time(), False
     for ep in range(epochs):
         perm = torch.randperm(n, device="cuda")
-        tot = 0.0
+        tot, seen = torch.zeros((), device="cuda"), 0  # summed on the device: no synchronisation per batch
         for k in range(0, n, batch):
+            elapsed = time.time() - t0
+            if elapsed > seconds:
+                out_of_time = True
+                break
+            if schedule == "cosine":
+                set_lr(lr * 0.5 * (1.0 + np.cos(np.pi * elapsed / seconds)))
             idx = perm[k:k + batch]
             if fwd is not None:
                 loss = F.mse_loss(fwd(xin[idx]), tgt[idx])
@@ -447,10 +465,12 @@ def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_dec
             opt.zero_grad(set_to_none=True)
             loss.backward()
             opt.step()
-            tot += float(loss.detach()) * len(idx)
-        hist.append((ep, tot / n))
-        if log:
-            log(f"epoch {ep} loss {tot / n:.4e}")
-        if time.time() - t0 > seconds:
+            tot += loss.detach() * len(idx)
+            seen += len(idx)
+        if seen:
+            hist.append((ep, float(tot) / seen))
+            if log:
+                log(f"epoch {ep} loss {hist[-1][1]:.4e}")
+        if out_of_time:
             break
     return LearnedStart(model, s_in, s_out, s_d, tcgen05=tcgen05), hist
