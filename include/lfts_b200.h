@@ -446,6 +446,14 @@ int lfts_conv3d_wgrad_bf16(void *stream, const void *x, const void *gy, float *d
 int lfts_adamw_f32(void *stream, float *p, const float *g, float *m, float *v, long long n, double lr, double b1, double b2,
                    double eps, double weight_decay, int step);
 
+/* Backward of the ReLU after a U-Net convolution (training): g = gy where
+ * y > 0, else 0, for every one of the cpad channels of npos positions (BF16,
+ * channels last, 16-byte aligned), and db[c] += sum over positions of g[p][c]
+ * for c < co (FP32, on the device; the caller zeroes it).  cpad a multiple of
+ * 8 up to 256.  The reference has no learned start; this replaces torch's
+ * autograd of the ReLU and of the bias sum in the U-Net's training. */
+int lfts_relu_grad_bf16(void *stream, const void *gy, const void *y, void *g, float *db, long long npos, int cpad, int co);
+
 /* Adam field update of the SCFT driver (examples/scft/scft.py:42-54), on n
  * doubles: m = b1 m + (1-b1) d; v = b2 v + (1-b2) d^2;
  * w_new = w + lr (m / (1 - b1^count)) / (sqrt(v / (1 - b2^count)) + eps).

@@ -113,6 +113,7 @@ _SIGS = {
     "lfts_pcg64_normal": [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_double, C.c_void_p],
     "lfts_conv3d_bf16": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                          C.c_int, C.c_int, C.c_int, C.c_int],
+    "lfts_relu_grad_bf16": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_int],
     "lfts_adamw_f32": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.c_double,
                        C.c_double, C.c_double, C.c_double, C.c_int],
     "lfts_conv3d_wgrad_bf16": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,

@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_halo_umma(const uint4 *__rest
 // positions of one channel chunk form a core matrix (16-byte rows), channel
 // chunks are a fixed stride apart (SBO).  gy (A): chunk c of position k at
 // (c * WG_K + k) * 16 bytes.  A CTA takes one (kz, ky) row of taps (kx = 0..2;
-// the single tap of a 1x1x1 kernel) over WG_CHUNK positions, keeps one
+// the single tap of a 1x1x1 kernel) over nst stages of WG_K positions, keeps one
 // accumulator per tap in tensor memory, and adds them to dw (FP32, zeroed by
 // the caller) with atomics.
 //
@@ -378,16 +378,16 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_halo_umma(const uint4 *__rest
 // apart (SEG = 8).  Gather form (other W): per tap, the shifted row of each
 // position, chunk c of position k at (c * WG_K + k) * 16 bytes.
 //
-// The stages go through a ring of WS slots: every thread copies its share of
-// stage v with cp.async (one commit group per stage; items run chunk-fastest so
-// a warp's copies are coalesced), and at stage u waits only for its own group
-// of stage u (WS - 2 newer groups may still be in flight), fences and arrives
-// on full[u % WS]; thread 0 issues the stage's MMAs once all 128 arrived and
-// commits them to empty[u % WS], which each thread waits for before it refills
-// the slot.
+// The stages go through a ring of WS slots.  Warps 0-3 load: every thread
+// copies its share of stage v with cp.async (one commit group per stage; items
+// run chunk-fastest so a warp's copies are coalesced), and at stage u waits
+// only for its own group of stage u (WS - 2 newer groups may still be in
+// flight), fences and arrives on full[u % WS].  Lane 0 of warp 4 does nothing
+// else than issue: it waits for full[u % WS] (all 128 arrivals), issues the
+// stage's MMAs and commits them to empty[u % WS], which each loading thread
+// waits for before it refills the slot.  Warps 0-3 then read the accumulators
+// (tensor-memory lanes 32 w .. 32 w + 31).
 constexpr int WG_K = 64;        // positions per stage (4 MMA K-steps)
-constexpr int WG_CHUNK = 2048;  // positions per CTA
-constexpr int WG_STAGES = WG_CHUNK / WG_K;
 
 template <int N>
 __device__ __forceinline__ void cp_async_wait_group() {
@@ -410,10 +410,12 @@ __host__ __device__ constexpr int wgrad_slot_units(int cin, int cout, int ntap, 
     return (cout / 8) * WG_K + (seg > 0 ? (cin / 8) * (WG_K / seg) * (seg + 2) : ntap * (cin / 8) * WG_K);
 }
 
+constexpr int WG_THREADS = CONV_M + 32;  // 4 loading warps and the MMA warp
+
 template <int WS, bool ROWS>
-__global__ void __launch_bounds__(CONV_M) k_conv3d_wgrad_umma(const uint4 *__restrict__ x, const uint4 *__restrict__ gy,
+__global__ void __launch_bounds__(WG_THREADS) k_conv3d_wgrad_umma(const uint4 *__restrict__ x, const uint4 *__restrict__ gy,
                                                               float *__restrict__ dw, int B, int D, int H, int W, int cin,
-                                                              int cout, int taps, uint32_t tmem_cols, int seg) {
+                                                              int cout, int taps, uint32_t tmem_cols, int seg, int nst) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int ntap = taps == 27 ? 3 : 1;
     const int xc = cin / 8, gc = cout / 8;             // 16-byte chunks per position
@@ -424,11 +426,12 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_wgrad_umma(const uint4 *__res
     uint64_t *full = (uint64_t *)(stage0 + wgrad_ring_units(WS, st_units)), *empty = full + WS;
     uint32_t *tmem_slot = (uint32_t *)(empty + WS);
     long long *seg_row = (long long *)(empty + WS + 1);  // ROWS: per (stage, segment) shifted row start, -1 past the end
-    int *seg_x0 = (int *)(seg_row + WG_STAGES * R);       // ROWS: x of the segment's first position
+    int *seg_x0 = (int *)(seg_row + nst * R);             // ROWS: x of the segment's first position
     const int tid = threadIdx.x, warp = tid >> 5;
     const long long npos = (long long)B * D * H * W;
-    const long long p0 = (long long)blockIdx.x * WG_CHUNK;
-    const int g = blockIdx.y;  // tap row: kz = g / 3, ky = g % 3
+    // the tap rows of a chunk are neighbours in the grid, so its x and gy come from DRAM once
+    const long long p0 = (long long)blockIdx.y * nst * WG_K;
+    const int g = blockIdx.x;  // tap row: kz = g / 3, ky = g % 3
     const int dz = taps == 27 ? g / 3 - 1 : 0, dy = taps == 27 ? g % 3 - 1 : 0;
     if (tid == 0) {
         for (int s = 0; s < WS; s++) {
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_wgrad_umma(const uint4 *__res
         }
     }
     if (ROWS) {
-        for (int e = tid; e < WG_STAGES * R; e += CONV_M) {
+        for (int e = tid; e < nst * R; e += WG_THREADS) {
             const long long ps = p0 + (long long)e * seg;  // stage e / R, segment e % R
             long long base = -1;
             int x0 = 0;
@@ -470,6 +473,9 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_wgrad_umma(const uint4 *__res
     // M = 128, N = cin, both operands MN-major, FP32 accumulate
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(cin >> 3) << 17) |
                            ((uint32_t)(CONV_M >> 4) << 24);
+    // gather form with ntap cin <= 256: all taps in one MMA (N = ntap cin, accumulator j at columns j cin as before)
+    const bool stack = !ROWS && ntap * cin <= 256;
+    const uint32_t idesc_stack = (idesc & ~(0x3Fu << 17)) | ((uint32_t)((ntap * cin) >> 3) << 17);
     const float rgc = 1.0f / (float)gc, rxc = 1.0f / (float)xc, rsw = 1.0f / (float)SW;
     // this thread's copies of stage v into its slot (zeros beyond the last position)
     auto load = [&](int v) {
@@ -525,25 +531,47 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_wgrad_umma(const uint4 *__res
             }
         }
     };
-    // one commit group per stage (empty past the last), so group u holds stage u
-    for (int v = 0; v < WS - 1; v++) {
-        if (v < WG_STAGES) load(v);
-        cp_async_commit();
-    }
     bool ok = true;
-    int u = 0;
-    for (; u < WG_STAGES; u++) {
-        const int st = u % WS;
-        cp_async_wait_group<WS - 2>();  // this thread's stage u has landed (WS - 2 newer groups may not)
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive(full + st);
-        if (tid == 0) {
+    int u = 0;  // the MMA thread: stages issued
+    if (warp < 4) {
+        // one commit group per stage (empty past the last), so group u holds stage u
+        for (int v = 0; v < WS - 1; v++) {
+            if (v < nst) load(v);
+            cp_async_commit();
+        }
+        for (int w = 0; w < nst; w++) {
+            cp_async_wait_group<WS - 2>();  // this thread's stage w has landed (WS - 2 newer groups may not)
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(full + w % WS);
+            // refill the slot of stage w - 1 with stage w + WS - 1 once its MMAs are done
+            const int v = w + WS - 1;
+            if (v < nst) {
+                if (v >= WS && !mbar_wait(empty + v % WS, (v / WS - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                load(v);
+            }
+            cp_async_commit();
+        }
+        cp_async_wait_all();
+    } else if (tid == CONV_M) {
+        for (; u < nst; u++) {
+            const int st = u % WS;
             if (!mbar_wait(full + st, (u / WS) & 1)) {
                 ok = false;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t a0 = smem_addr(stage0 + st * st_units), b0 = a0 + (uint32_t)a_units * 16;
+            if (!ROWS && stack) {
+                // gather form: the taps' copies are chunks j * xc + c at one stride, so one MMA of N = ntap cin
+                for (int s = 0; s < WG_K / 16; s++)
+                    umma_bf16(tmem, umma_desc(a0 + (uint32_t)(16 * s * 16), 128, WG_K * 16),
+                              umma_desc(b0 + (uint32_t)(16 * s * 16), 128, WG_K * 16), idesc_stack, (u > 0 || s > 0) ? 1u : 0u);
+                umma_commit(empty + st);
+                continue;
+            }
             for (int s = 0; s < WG_K / 16; s++) {
                 const uint64_t da = umma_desc(a0 + (uint32_t)(16 * s * 16), 128, WG_K * 16);
                 for (int j = 0; j < ntap; j++) {
@@ -560,27 +588,16 @@ __global__ void __launch_bounds__(CONV_M) k_conv3d_wgrad_umma(const uint4 *__res
             }
             umma_commit(empty + st);
         }
-        // refill the slot of stage u - 1 with stage u + WS - 1 once its MMAs are done
-        const int v = u + WS - 1;
-        if (v < WG_STAGES) {
-            if (v >= WS && !mbar_wait(empty + v % WS, (v / WS - 1) & 1)) {
-                ok = false;
-                break;
-            }
-            load(v);
-        }
-        cp_async_commit();
     }
-    cp_async_wait_all();
     {
         // the last stage's MMAs are the last to complete (one thread issues them in order)
-        const bool fin = __syncthreads_and(ok) ? mbar_wait(empty + (WG_STAGES - 1) % WS, ((WG_STAGES - 1) / WS) & 1) : false;
+        const bool fin = __syncthreads_and(ok) ? mbar_wait(empty + (nst - 1) % WS, ((nst - 1) / WS) & 1) : false;
         ok = __syncthreads_and(fin);
     }
     if (!ok) {
-        // a second bounded wait for MMAs still in flight: the last stage thread 0 committed
-        if (tid == 0 && u > 0) mbar_wait(empty + (u - 1) % WS, ((u - 1) / WS) & 1);
-    } else {
+        // a second bounded wait for MMAs still in flight: the last stage the MMA thread committed
+        if (tid == CONV_M && u > 0) mbar_wait(empty + (u - 1) % WS, ((u - 1) / WS) & 1);
+    } else if (warp < 4) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int co = 32 * warp + (tid & 31);  // accumulator row of this thread
         for (int j = 0; j < ntap; j++) {
@@ -614,44 +631,65 @@ extern "C" int lfts_conv3d_wgrad_bf16(void *stream, const void *x, const void *g
     if (taps != 1 && taps != 27) return fail("conv3d wgrad: taps must be 1 or 27");
     if (((uintptr_t)x | (uintptr_t)gy) & 15) return fail("conv3d wgrad: buffers must be 16-byte aligned");
     const long long npos = (long long)B * D * H * W;
-    const long long chunks = (npos + lfts::unet::WG_CHUNK - 1) / lfts::unet::WG_CHUNK;
-    if (chunks > 0x7fffffffLL) return fail("conv3d wgrad: too many positions");
     const int ntap = taps == 27 ? 3 : 1;
+    const long long rows = taps == 27 ? 9 : 1;
     uint32_t cols = 32;
     while ((int)cols < ntap * cin) cols <<= 1;
     if (cout > 128) return fail("conv3d wgrad: cout (the accumulator rows) must be <= 128");
     using namespace lfts::unet;
     // x staged as row segments with a halo when W % 8 == 0 (segment: the longest of 64, 32, 16, 8 dividing W)
-    const int seg = W % 64 == 0 ? 64 : W % 32 == 0 ? 32 : W % 16 == 0 ? 16 : W % 8 == 0 ? 8 : 0;
+    int seg = W % 64 == 0 ? 64 : W % 32 == 0 ? 32 : W % 16 == 0 ? 16 : W % 8 == 0 ? 8 : 0;
+    if (const char *env = std::getenv("LFTS_CONV_WGRAD_GATHER"))  // 1: per-tap gathers at every W
+        if (env[0] == '1') seg = 0;
     const int st_units = wgrad_slot_units(cin, cout, ntap, seg);
-    const size_t table = seg ? (size_t)WG_STAGES * (WG_K / seg) * (sizeof(long long) + sizeof(int)) : 0;
-    auto smem_of = [&](int ws) {
+    auto smem_of = [&](int ws, int nst) {
+        const size_t table = seg ? (size_t)nst * (WG_K / seg) * (sizeof(long long) + sizeof(int)) : 0;
         return (size_t)16 * wgrad_ring_units(ws, st_units) + (2 * (size_t)ws + 1) * sizeof(uint64_t) + table + 16;
     };
-    // ring depth: the most stages in flight per SM (CTAs per SM by shared memory
-    // and tensor-memory columns, times WS - 1); ties go to the deeper ring
+    // resident CTAs per SM: shared memory (228 KB per SM, 1 KB reserved per CTA) and tensor-memory columns
+    auto resident = [&](size_t smem) {
+        int c = (int)((228 * 1024) / (smem + 1024));
+        return c < (int)(512 / cols) ? c : (int)(512 / cols);
+    };
+    // ring depth: the most stages in flight per SM (resident CTAs times WS - 1); ties go to the deeper ring
     int WS = 0, best = 0;
     for (int ws = 2; ws <= 4; ws++) {
-        if (smem_of(ws) > 200 * 1024) continue;
-        int ctas = (int)((228 * 1024) / (smem_of(ws) + 1024));
-        if (ctas > (int)(512 / cols)) ctas = (int)(512 / cols);
-        if (ctas * (ws - 1) >= best) {
-            best = ctas * (ws - 1);
+        if (smem_of(ws, 64) > 200 * 1024) continue;
+        const int c = resident(smem_of(ws, 64));
+        if (c * (ws - 1) >= best) {
+            best = c * (ws - 1);
             WS = ws;
         }
     }
     if (const char *env = std::getenv("LFTS_CONV_WGRAD_RING")) {  // 2, 3 or 4 overrides the choice
         const int ws = env[0] - '0';
-        if (ws >= 2 && ws <= 4 && smem_of(ws) <= 200 * 1024) WS = ws;
+        if (ws >= 2 && ws <= 4 && smem_of(ws, 64) <= 200 * 1024) WS = ws;
     }
     if (WS == 0) return fail("conv3d wgrad: cin too large for the shared-memory stages");
-    using Kern = void (*)(const uint4 *, const uint4 *, float *, int, int, int, int, int, int, int, uint32_t, int);
+    // stages of WG_K positions per CTA (each CTA adds its partial sums to dw with
+    // atomics): 64 while that gives at least four waves of resident CTAs, else the
+    // most (32 .. 256) that still fill one wave
+    auto ctas = [&](int nst) { return (npos + (long long)nst * WG_K - 1) / ((long long)nst * WG_K) * rows; };
+    const long long wave = 148LL * resident(smem_of(WS, 64));
+    int nst = 64;
+    if (ctas(64) < 4 * wave) {
+        nst = 32;
+        while (nst < 256 && ctas(2 * nst) >= wave - wave / 16) nst *= 2;
+    }
+    if (const char *env = std::getenv("LFTS_CONV_WGRAD_STAGES")) {  // override: 32 .. 1024
+        const int v = std::atoi(env);
+        if (v >= 32 && v <= 1024) nst = v;
+    }
+    const long long chunks = (npos + (long long)nst * WG_K - 1) / ((long long)nst * WG_K);
+    if (chunks > 65535) return fail("conv3d wgrad: too many positions (more than 65535 chunks of nst x 64)");
+    if (smem_of(WS, nst) > 200 * 1024) return fail("conv3d wgrad: shared memory of the stages and the segment table");
+    using Kern = void (*)(const uint4 *, const uint4 *, float *, int, int, int, int, int, int, int, uint32_t, int, int);
     Kern kern = seg ? (WS == 2 ? k_conv3d_wgrad_umma<2, true> : WS == 3 ? k_conv3d_wgrad_umma<3, true> : k_conv3d_wgrad_umma<4, true>)
                     : (WS == 2 ? k_conv3d_wgrad_umma<2, false> : WS == 3 ? k_conv3d_wgrad_umma<3, false> : k_conv3d_wgrad_umma<4, false>);
     cudaError_t e = cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     if (e != cudaSuccess) return fail(std::string("conv3d wgrad: ") + cudaGetErrorString(e));
-    kern<<<dim3((unsigned)chunks, taps == 27 ? 9 : 1), CONV_M, smem_of(WS), (cudaStream_t)stream>>>(
-        (const uint4 *)x, (const uint4 *)gy, dw, B, D, H, W, cin, cout, taps, cols, seg);
+    kern<<<dim3(taps == 27 ? 9 : 1, (unsigned)chunks), WG_THREADS, smem_of(WS, nst), (cudaStream_t)stream>>>(
+        (const uint4 *)x, (const uint4 *)gy, dw, B, D, H, W, cin, cout, taps, cols, seg, nst);
     e = cudaPeekAtLastError();
     if (e != cudaSuccess) return fail(std::string("conv3d wgrad launch: ") + cudaGetErrorString(e));
     return 0;
@@ -759,5 +797,68 @@ extern "C" int lfts_adamw_f32(void *stream, float *p, const float *g, float *m, 
                                                                    (float)std::sqrt(bc2));
     cudaError_t e = cudaPeekAtLastError();
     if (e != cudaSuccess) return fail(std::string("adamw launch: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+namespace lfts {
+namespace unet {
+
+// ---------------------------------------------------------------- ReLU backward (training of the U-Net)
+// g = gy where y > 0, else +0 (BF16, [npos][cpad]), and db[c] += sum_p g[p][c]
+// for c < co (FP32).  Thread t of a block of cg * k threads (cg = cpad / 8
+// chunks of 8 channels) keeps chunk t % cg for the whole grid-stride loop, so
+// its 8 partial sums stay in registers; the block adds them up by chunk in
+// shared memory and issues one atomic per channel.
+__global__ void k_relu_grad_bf16(const uint4 *__restrict__ gy, const uint4 *__restrict__ y, uint4 *__restrict__ g,
+                                 float *__restrict__ db, long long units, int cg, int co) {
+    extern __shared__ float red[];  // [blockDim][8]
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < units; u += stride) {
+        const uint4 a = gy[u], m = y[u];
+        const uint32_t av[4] = {a.x, a.y, a.z, a.w}, mv[4] = {m.x, m.y, m.z, m.w};
+        uint32_t ov[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            // BF16 y > 0: sign bit clear, not zero, not NaN (as torch's y > 0)
+            const uint32_t lo = mv[i] & 0xFFFFu, hi = mv[i] >> 16;
+            const bool plo = !(lo & 0x8000u) && (lo & 0x7FFFu) && (lo & 0x7FFFu) <= 0x7F80u;
+            const bool phi = !(hi & 0x8000u) && (hi & 0x7FFFu) && (hi & 0x7FFFu) <= 0x7F80u;
+            const uint32_t o = (plo ? (av[i] & 0xFFFFu) : 0u) | (phi ? (av[i] & 0xFFFF0000u) : 0u);
+            ov[i] = o;
+            acc[2 * i] += __uint_as_float(o << 16);
+            acc[2 * i + 1] += __uint_as_float(o & 0xFFFF0000u);
+        }
+        g[u] = make_uint4(ov[0], ov[1], ov[2], ov[3]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) red[threadIdx.x * 8 + i] = acc[i];
+    __syncthreads();
+    // thread c8 < cg * 8 sums channel c8 over the block's threads of its chunk
+    for (int c8 = threadIdx.x; c8 < cg * 8; c8 += blockDim.x) {
+        const int chunk = c8 >> 3, i = c8 & 7;
+        float s = 0.f;
+        for (int t = chunk; t < (int)blockDim.x; t += cg) s += red[t * 8 + i];
+        if (c8 < co) atomicAdd(db + c8, s);
+    }
+}
+}  // namespace unet
+}  // namespace lfts
+
+extern "C" int lfts_relu_grad_bf16(void *stream, const void *gy, const void *y, void *g, float *db, long long npos, int cpad,
+                                   int co) {
+    if (!gy || !y || !g || !db) return fail("relu grad: null argument");
+    if (npos < 0 || cpad < 8 || cpad % 8 || cpad > 256 || co < 0 || co > cpad)
+        return fail("relu grad: cpad must be a multiple of 8 up to 256 and 0 <= co <= cpad");
+    if (((uintptr_t)gy | (uintptr_t)y | (uintptr_t)g) & 15) return fail("relu grad: buffers must be 16-byte aligned");
+    if (npos == 0) return 0;
+    const int cg = cpad / 8, threads = cg * (256 / cg);
+    const long long units = npos * cg;
+    long long blocks = (units + threads - 1) / threads;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    lfts::unet::k_relu_grad_bf16<<<(unsigned)blocks, threads, (size_t)threads * 8 * sizeof(float), (cudaStream_t)stream>>>(
+        (const uint4 *)gy, (const uint4 *)y, (uint4 *)g, db, units, cg, co);
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) return fail(std::string("relu grad launch: ") + cudaGetErrorString(e));
     return 0;
 }

@@ -184,8 +184,17 @@ class _ConvFn(torch.autograd.Function):
         from langevinfts_b200.capi import check, lib
         x, y, full = ctx.saved_tensors
         co, ci, k, in_map, cin_pad, cout_pad, taps, relu = ctx.meta
-        g = gy * (y > 0) if relu else gy
-        g = g.to(torch.bfloat16).contiguous()
+        gy = gy.to(torch.bfloat16).contiguous()
+        if relu:
+            # ReLU mask and bias gradient in one pass (lfts_relu_grad_bf16)
+            g = torch.empty_like(y)
+            dbp = torch.zeros(cout_pad, device=gy.device)
+            check(lib().lfts_relu_grad_bf16(torch.cuda.current_stream().cuda_stream, gy.data_ptr(), y.data_ptr(), g.data_ptr(),
+                                            dbp.data_ptr(), y.numel() // cout_pad, cout_pad, co))
+            db = dbp[:co]
+        else:
+            g = gy
+            db = g[..., :co].float().sum((0, 1, 2, 3))
         # input gradient: the same convolution of g, weights transposed, taps mirrored
         back = full.flip(0).transpose(1, 2).contiguous()  # [taps, cin_pad, cout_pad]
         dx = conv3d_tcgen05(g, (_pack_full(back), torch.zeros(cin_pad, device=g.device), cin_pad, taps), False)
@@ -194,7 +203,6 @@ class _ConvFn(torch.autograd.Function):
         check(lib().lfts_conv3d_wgrad_bf16(torch.cuda.current_stream().cuda_stream, x.data_ptr(), g.data_ptr(), dwp.data_ptr(),
                                            B, D, H, W, cin_pad, cout_pad, taps))
         dw = dwp[:, :co, torch.as_tensor(in_map, device=g.device)].reshape(k, k, k, co, ci).permute(3, 4, 0, 1, 2).contiguous()
-        db = g[..., :co].float().sum((0, 1, 2, 3))
         return dx, dw, db, None, None, None
 
 
@@ -211,12 +219,16 @@ class TcgenUNetTrain(torch.nn.Module):
         self.pb, self.p2, self.p4 = _pad16(b), _pad16(2 * b), _pad16(4 * b)
         self.cin = net.e1[0].in_channels
         self.cin_pad = _pad16(self.cin)
-        r = lambda n: list(range(n))
+        # channel maps as device tensors, made once (no host upload inside a step, so a step can be graph-captured)
+        dev = net.e1[0].weight.device
+        r = lambda n: torch.arange(n, device=dev)
+        cat = lambda a, off, n: torch.cat([a, torch.arange(off, off + n, device=dev)])
         pb, p2, p4 = self.pb, self.p2, self.p4
         self.maps = {"e1": (r(self.cin), self.cin_pad, r(b), pb), "e2": (r(b), pb, r(2 * b), p2),
                      "e3": (r(2 * b), p2, r(4 * b), p4),
-                     "d2": (r(4 * b) + [p4 + i for i in range(2 * b)], p4 + p2, r(2 * b), p2),
-                     "d1": (r(2 * b) + [p2 + i for i in range(b)], p2 + pb, r(b), pb)}
+                     "d2": (cat(r(4 * b), p4, 2 * b), p4 + p2, r(2 * b), p2),
+                     "d1": (cat(r(2 * b), p2, b), p2 + pb, r(b), pb)}
+        self.out_map = r(net.out.in_channels)
 
     def _block(self, h, name):
         blk = getattr(self.net, name)
@@ -241,8 +253,8 @@ class TcgenUNetTrain(torch.nn.Module):
         x3 = self._block(self._pool(x2), "e3")
         y2 = self._block(torch.cat([self._up(x3), x2], -1).contiguous(), "d2")
         y1 = self._block(torch.cat([self._up(y2), x1], -1).contiguous(), "d1")
-        o = _ConvFn.apply(y1, self.net.out.weight, self.net.out.bias, list(range(self.net.out.in_channels)),
-                          self.pb, False)[..., :self.net.out.out_channels]
+        o = _ConvFn.apply(y1, self.net.out.weight, self.net.out.bias, self.out_map, self.pb,
+                          False)[..., :self.net.out.out_channels]
         return o.permute(0, 4, 1, 2, 3).float()
 
 
@@ -413,12 +425,15 @@ def ablation(sim, starts, nsteps):
 
 
 def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_decay=1e-4, seed=0, log=None, tcgen05=True,
-          schedule="cosine"):
+          schedule="cosine", graph=True):
     """AdamW on MSE of the scaled residual target (Y - w_+prev) / s_out until
     `seconds` or `epochs` run out.  X holds 2 input channels (w_-, w_+prev) or
     3 (and dw_-), each scaled by its standard deviation.  schedule "cosine":
     the learning rate falls from lr to 0 over the time budget (half a cosine
-    in elapsed time); "constant": lr throughout.  tcgen05=True (default): every convolution's
+    in elapsed time); "constant": lr throughout.  graph (tensor-core path): the
+    forward and backward of a batch are captured once as a CUDA graph and
+    replayed on static batch buffers (full batches only); the AdamW step runs
+    after each replay.  tcgen05=True (default): every convolution's
     forward and backward on this library's tensor-core kernels and the update
     by FlatAdamW (lfts_adamw_f32); False: BF16 autocast over torch's
     convolutions and torch's AdamW.  Returns (LearnedStart, history of (epoch,
@@ -445,6 +460,21 @@ def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_dec
             for g in opt.param_groups:
                 g["lr"] = v
     n = xin.shape[0]
+    step_graph = None
+    if tcgen05 and graph and n >= batch:
+        xs, ts = xin[:batch].clone(), tgt[:batch].clone()
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):  # warm-up outside the capture (allocations, kernel attributes)
+            for _ in range(2):
+                model.zero_grad(set_to_none=True)
+                F.mse_loss(fwd(xs), ts).backward()
+        torch.cuda.current_stream().wait_stream(side)
+        model.zero_grad(set_to_none=True)
+        step_graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(step_graph):
+            static_loss = F.mse_loss(fwd(xs), ts)
+            static_loss.backward()
     hist, t0, out_of_time = [], time.time(), False
     for ep in range(epochs):
         perm = torch.randperm(n, device="cuda")
@@ -457,14 +487,23 @@ def train(X, Y, base=24, seconds=60.0, epochs=1000, batch=4, lr=1e-3, weight_dec
             if schedule == "cosine":
                 set_lr(lr * 0.5 * (1.0 + np.cos(np.pi * elapsed / seconds)))
             idx = perm[k:k + batch]
-            if fwd is not None:
-                loss = F.mse_loss(fwd(xin[idx]), tgt[idx])
+            if step_graph is not None:
+                if len(idx) < batch:
+                    break  # full batches only
+                torch.index_select(xin, 0, idx, out=xs)
+                torch.index_select(tgt, 0, idx, out=ts)
+                step_graph.replay()  # gradients into the parameters' captured .grad tensors
+                opt.step()
+                loss = static_loss
             else:
-                with torch.autocast("cuda", dtype=torch.bfloat16):
-                    loss = F.mse_loss(model(xin[idx]).float(), tgt[idx])
-            opt.zero_grad(set_to_none=True)
-            loss.backward()
-            opt.step()
+                if fwd is not None:
+                    loss = F.mse_loss(fwd(xin[idx]), tgt[idx])
+                else:
+                    with torch.autocast("cuda", dtype=torch.bfloat16):
+                        loss = F.mse_loss(model(xin[idx]).float(), tgt[idx])
+                opt.zero_grad(set_to_none=True)
+                loss.backward()
+                opt.step()
             tot += loss.detach() * len(idx)
             seen += len(idx)
         if seen:

@@ -102,6 +102,53 @@ def test_wgrad_ring_depths(monkeypatch, ws, cin, cout, k, grid, batch):
     assert _rel(dw, ref) < 1e-4
 
 
+@pytest.mark.parametrize("stages", ["64", "100", "256"])
+def test_wgrad_stage_counts(monkeypatch, stages):
+    """lfts_conv3d_wgrad_bf16 with more stages of 64 positions per CTA (the
+    LFTS_CONV_WGRAD_STAGES override), ragged last chunk, against torch."""
+    import torch
+    import torch.nn.functional as F
+    from langevinfts_b200.capi import check, lib
+    monkeypatch.setenv("LFTS_CONV_WGRAD_STAGES", stages)
+    torch.manual_seed(int(stages))
+    cin, cout, grid, batch = 32, 16, (6, 16, 32), 5
+    x = torch.randn(batch, *grid, cin, device="cuda").to(torch.bfloat16)
+    gy = torch.randn(batch, *grid, cout, device="cuda").to(torch.bfloat16)
+    dw = torch.zeros(27, cout, cin, device="cuda")
+    check(lib().lfts_conv3d_wgrad_bf16(torch.cuda.current_stream().cuda_stream, x.data_ptr(), gy.data_ptr(), dw.data_ptr(),
+                                       batch, *grid, cin, cout, 27))
+    torch.cuda.synchronize()
+    xp = F.pad(x.float().permute(0, 4, 1, 2, 3), (1,) * 6, mode="circular")
+    ref = torch.nn.grad.conv3d_weight(xp, (cout, cin, 3, 3, 3), gy.float().permute(0, 4, 1, 2, 3))
+    assert _rel(dw, ref.permute(2, 3, 4, 0, 1).reshape(27, cout, cin)) < 1e-4
+
+
+@pytest.mark.parametrize("cpad,co", [(32, 24), (48, 48), (16, 1), (144, 144), (256, 200)])
+def test_relu_grad_kernel(cpad, co):
+    """lfts_relu_grad_bf16 against torch: g = gy * (y > 0) value for value
+    (zeros, negative zeros, infinities and NaN in y included; the kernel writes
+    +0 where torch's product gives -0) and the bias gradient against a float64
+    sum."""
+    import torch
+    from langevinfts_b200.capi import check, lib
+    torch.manual_seed(cpad + co)
+    npos = 3 * 17 * 19 + 5
+    gy = torch.randn(npos, cpad, device="cuda").to(torch.bfloat16)
+    y = torch.randn(npos, cpad, device="cuda").to(torch.bfloat16)
+    special = torch.tensor([0.0, -0.0, float("inf"), float("-inf"), float("nan"), 1e-40], device="cuda").to(torch.bfloat16)
+    y.view(-1)[:special.numel() * 7:7] = special.repeat(1)
+    g = torch.empty_like(gy)
+    db = torch.zeros(cpad, device="cuda")
+    check(lib().lfts_relu_grad_bf16(torch.cuda.current_stream().cuda_stream, gy.data_ptr(), y.data_ptr(), g.data_ptr(),
+                                    db.data_ptr(), npos, cpad, co))
+    torch.cuda.synchronize()
+    ref = gy * (y > 0)
+    assert torch.equal(g.float(), ref.float())
+    want = ref[:, :co].double().sum(0)
+    assert float((db[:co].double() - want).abs().max()) <= 1e-5 * float(want.abs().max()) + 1e-6
+    assert float(db[co:].abs().max() if co < cpad else 0) == 0.0
+
+
 def test_tcgen05_unet_matches_torch_model():
     import torch
     from langevinfts_b200.learned import TcgenUNet, UNet3D
