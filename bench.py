@@ -638,6 +638,10 @@ def run_conv(args):
               ("d2b", 2 * b, 48, 2 * b, 3, 1), ("d1a", 3 * b, 80, b, 3, 0), ("d1b", b, 32, b, 3, 0), ("out", b, 32, 1, 1, 0)]
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     rows, tot_us, tot_us_ref, tot_flop = [], 0.0, 0.0, 0.0
+    if args.conv_layer:
+        layers = [l for l in layers if l[0] == args.conv_layer]
+        if not layers:
+            raise SystemExit(f"--conv-layer: no layer {args.conv_layer}")
     for name, ci, cip, co, k, lev in layers:
         n = N >> lev
         conv = torch.nn.Conv3d(ci, co, k).cuda()
@@ -1096,6 +1100,7 @@ def main():
     ap.add_argument("--ref-scft", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--scft", action="store_true", help="SCFT of the 64^3 asymmetric diblock (device loop, FP64 and FP32)")
     ap.add_argument("--conv", action="store_true", help="time the tensor-core U-Net convolutions against cuDNN")
+    ap.add_argument("--conv-layer", default=None, help="with --conv: time only this layer (e1a ... d1b, out; for profiling)")
     ap.add_argument("--ensemble", action="store_true",
                     help="ensemble <H>, dH/dchiN and S(k) of the FP32 and learned forms against plain FP64 (same noise)")
     ap.add_argument("--sf-period", type=int, default=5, help=argparse.SUPPRESS)
