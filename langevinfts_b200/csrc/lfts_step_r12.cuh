@@ -504,7 +504,10 @@ constexpr int XW = 32;  // columns per item (512-byte rows in FP64, 256 in FP32)
 constexpr int XTILES = PLANE / XW;
 static_assert(PLANE % XW == 0, "x-pass tiles cover the plane exactly");
 template <typename C> constexpr size_t xpipe_smem() { return 2 * sizeof(C) * (size_t)N * XW + 16; }
-template <typename T> __host__ __device__ constexpr int minb_xpass() { return sizeof(T) == 4 ? 3 : 2; }
+// resident CTAs per SM: FP32 four (64 registers, a few spills; the pass waits at
+// its barriers, so more CTAs hide more of it: 0.765 against 0.777 ms a 32-job
+// step at three), FP64 two
+template <typename T> __host__ __device__ constexpr int minb_xpass() { return sizeof(T) == 4 ? 4 : 2; }
 
 template <typename T, int NBR>
 __global__ void __launch_bounds__(NTHR, minb_xpass<T>()) kq_xpass(GridPlan g, const lfts_step_job *__restrict__ jobs, int nj,
