@@ -617,6 +617,166 @@ __global__ void __launch_bounds__(WG_THREADS) k_conv3d_wgrad_umma(const uint4 *_
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
 }
+// ------------------------------------------------------------------------
+// 3x3x3 convolution by slices of 16 input channels: for the tile of TZ x 16 x 8
+// output positions (TZ = 1, 2 or 4 planes, one accumulator of COUT columns per
+// plane) each stage of a ring of NS slots holds one slice: the halo of its two
+// 16-byte channel chunks, (TZ + 2) x 18 x 10 positions as two planes of odd
+// length HPLP (the layout of k_conv3d_halo_umma restricted to two chunks), and
+// the 27 taps' weights of those channels, tap t at t * 2 * COUT units (two
+// chunks of COUT rows).  A slice feeds 27 x TZ MMAs of K = 16.  Warps 0-3 load
+// (the halo with cp.async, chunk-fastest; thread 0 also issues one bulk copy
+// per tap for the weights, counted in transaction bytes on the slot's full
+// barrier), wait for their own copies with a lag of NS - 2 groups, fence and
+// arrive; lane 0 of warp 4 issues the MMAs of a full slot and commits them to
+// its empty barrier; warps 0-3 then read the accumulators.  Against the halo
+// kernel the loads overlap the MMAs inside a CTA and each weight byte staged
+// serves TZ x 128 positions.  Needs H % 16 == 0, W % 8 == 0, D % TZ == 0.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+constexpr int KS_THREADS = CONV_M + 32;  // 4 loading warps and the MMA warp
+
+template <int TZ> __host__ __device__ constexpr int kslice_hplp() { return (TZ + 2) * HROW + 1; }
+__host__ __device__ constexpr int kslice_slot_units(int hplp, int cout) { return 2 * hplp + 27 * 2 * cout; }
+
+template <int TZ, int NS>
+__global__ void __launch_bounds__(KS_THREADS) k_conv3d_kslice_umma(const uint4 *__restrict__ in, const uint4 *__restrict__ wpk,
+                                                                 const float *__restrict__ bias, uint16_t *__restrict__ out,
+                                                                 int B, int D, int H, int W, int cin, int cout, int relu,
+                                                                 uint32_t tmem_cols) {
+    constexpr int HPLP = kslice_hplp<TZ>();
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int kc_n = cin / 8, nsl = kc_n / 2, b_units = kc_n * cout;
+    const int slot_units = kslice_slot_units(HPLP, cout);
+    const uint32_t w_bytes = 27u * 2u * (uint32_t)cout * 16u;
+    uint4 *ring = (uint4 *)smem_raw;
+    uint64_t *full = (uint64_t *)(ring + (size_t)NS * slot_units), *empty = full + NS, *done = empty + NS;
+    uint32_t *tmem_slot = (uint32_t *)(done + 1);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int ztiles = D / TZ;
+    const int x0 = blockIdx.x * HT_X, y0 = blockIdx.y * HT_Y, z0 = (blockIdx.z % ztiles) * TZ, n = blockIdx.z / ztiles;
+    if (tid == 0) {
+        for (int i = 0; i < NS; i++) {
+            mbar_init(full + i, CONV_M);
+            mbar_init(empty + i, 1);
+        }
+        mbar_init(done, 1);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    // loading thread's copies of slice v into its slot
+    auto load = [&](int v) {
+        uint4 *slot = ring + (size_t)(v % NS) * slot_units;
+        if (tid == 0) {
+            mbar_expect_tx(full + v % NS, w_bytes);
+            uint4 *wd = slot + 2 * HPLP;
+            for (int t = 0; t < 27; t++)
+                bulk_load(wd + t * 2 * cout, wpk + (long long)t * b_units + 2 * v * cout, 2u * (uint32_t)cout * 16u,
+                          full + v % NS);
+        }
+        // halo items (position, chunk), chunk fastest: two consecutive threads read a position's 32 bytes
+        for (int i = tid; i < 2 * (TZ + 2) * HROW; i += CONV_M) {
+            const int r = i >> 1, c = i & 1;
+            const int zh = r / HROW, rem = r - zh * HROW, yh = rem / HX, xh = rem - yh * HX;
+            int xx = x0 + xh - 1, yy = y0 + yh - 1, zz = z0 + zh - 1;
+            xx += xx < 0 ? W : 0;
+            xx -= xx >= W ? W : 0;
+            yy += yy < 0 ? H : 0;
+            yy -= yy >= H ? H : 0;
+            zz += zz < 0 ? D : 0;
+            zz -= zz >= D ? D : 0;
+            cp_async16(slot + c * HPLP + r, in + ((((long long)n * D + zz) * H + yy) * W + xx) * kc_n + 2 * v + c);
+        }
+    };
+    bool ok = true;
+    int u = 0;  // the MMA thread: slices issued
+    if (warp < 4) {
+        for (int v = 0; v < NS - 1; v++) {
+            if (v < nsl) load(v);
+            cp_async_commit();
+        }
+        for (int w = 0; w < nsl; w++) {
+            cp_async_wait_group<NS - 2>();  // this thread's halo copies of slice w have landed
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(full + w % NS);
+            const int v = w + NS - 1;
+            if (v < nsl) {
+                if (v >= NS && !mbar_wait(empty + v % NS, (v / NS - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                load(v);
+            }
+            cp_async_commit();
+        }
+        cp_async_wait_all();
+    } else if (tid == CONV_M) {
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(cout >> 3) << 17) | ((uint32_t)(CONV_M >> 4) << 24);
+        for (; u < nsl; u++) {
+            const int st = u % NS;
+            if (!mbar_wait(full + st, (u / NS) & 1)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t h0 = smem_addr(ring + (size_t)st * slot_units), w0 = h0 + (uint32_t)(2 * HPLP) * 16u;
+            for (int t = 0; t < 27; t++) {
+                const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+                const uint64_t db = umma_desc(w0 + (uint32_t)(t * 2 * cout) * 16u, (uint32_t)cout * 16, 128);
+#pragma unroll
+                for (int j = 0; j < TZ; j++) {
+                    const uint32_t a = h0 + (uint32_t)((((j + dz) * HY + dy) * HX + dx) * 16);
+                    umma_bf16(tmem + (uint32_t)(j * cout), umma_desc(a, HPLP * 16, HX * 16), db, idesc,
+                              (u > 0 || t > 0) ? 1u : 0u);
+                }
+            }
+            umma_commit(empty + st);
+        }
+        if (ok) umma_commit(done);
+    }
+    {
+        const bool fin = __syncthreads_and(ok) ? mbar_wait(done, 0) : false;
+        ok = __syncthreads_and(fin);
+    }
+    if (!ok) {
+        // a wait gave up after its bound (the weight copies issued have long landed by
+        // then): a second bounded wait for the MMAs the MMA thread committed
+        if (tid == CONV_M && u > 0) mbar_wait(empty + (u - 1) % NS, ((u - 1) / NS) & 1);
+    } else if (warp < 4) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int m = tid;  // accumulator row = 8 j + l: position (y0 + j, x0 + l)
+#pragma unroll
+        for (int j = 0; j < TZ; j++) {
+            const long long p = (((long long)n * D + z0 + j) * H + (y0 + m / 8)) * W + (x0 + m % 8);
+            for (int c0 = 0; c0 < cout; c0 += 16) {
+                uint32_t v[16];
+                tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(j * cout + c0), v);
+                uint16_t h[16];
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    float f = __uint_as_float(v[i]) + bias[c0 + i];
+                    if (relu && f < 0.f) f = 0.f;
+                    h[i] = to_bf16(f);
+                }
+                uint4 *o = (uint4 *)(out + p * cout + c0);
+                o[0] = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
+                o[1] = make_uint4(h[8] | (h[9] << 16), h[10] | (h[11] << 16), h[12] | (h[13] << 16), h[14] | (h[15] << 16));
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+}
 }  // namespace unet
 }  // namespace lfts
 
@@ -710,6 +870,47 @@ extern "C" int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, c
     if (blocks > 0x7fffffffLL) return fail("conv3d: too many positions");
     uint32_t cols = 32;
     while ((int)cols < cout) cols <<= 1;
+    if (taps == 27 && H % lfts::unet::HT_Y == 0 && W % lfts::unet::HT_X == 0 && cin >= 32) {
+        // slices of 16 input channels, by default from three slices on (at two the
+        // halo kernel is faster: 323 against 498 us for 32 -> 32 channels at 64^3 x 8;
+        // d1a 80 -> 32: 890 against 1161 us, d2a 144 -> 48: 210 against 378 us):
+        // the most output planes (4, 2, 1) whose ring of 3 (else 2) slots fits 200 KB;
+        // LFTS_CONV_KSLICE=0|1 (1: from two slices on) and LFTS_CONV_KSLICE_TZ=1|2|4 override
+        using namespace lfts::unet;
+        bool use = cin >= 48;
+        int want_tz = 0;
+        if (const char *env = std::getenv("LFTS_CONV_KSLICE")) use = env[0] != '0';
+        if (const char *env = std::getenv("LFTS_CONV_KSLICE_TZ")) want_tz = std::atoi(env);
+        auto smem_of = [&](int tz, int ns) {
+            const int hplp = (tz + 2) * HROW + 1;
+            return (size_t)16 * ns * kslice_slot_units(hplp, cout) + (2 * (size_t)ns + 1) * sizeof(uint64_t) + 16;
+        };
+        int tz = 0, ns = 0;
+        for (int t : {4, 2, 1}) {
+            if (tz || (want_tz && t != want_tz) || D % t || t * cout > 256) continue;
+            for (int q : {3, 2})
+                if (!tz && smem_of(t, q) <= 200 * 1024) {
+                    tz = t;
+                    ns = q;
+                }
+        }
+        if (use && tz && (long long)B * D / tz <= 65535) {
+            uint32_t kcols = 32;
+            while ((int)kcols < tz * cout) kcols <<= 1;
+            using Kern = void (*)(const uint4 *, const uint4 *, const float *, uint16_t *, int, int, int, int, int, int, int, uint32_t);
+            Kern kern = tz == 4 ? (ns == 3 ? k_conv3d_kslice_umma<4, 3> : k_conv3d_kslice_umma<4, 2>)
+                      : tz == 2 ? (ns == 3 ? k_conv3d_kslice_umma<2, 3> : k_conv3d_kslice_umma<2, 2>)
+                                : (ns == 3 ? k_conv3d_kslice_umma<1, 3> : k_conv3d_kslice_umma<1, 2>);
+            cudaError_t e = cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            if (e != cudaSuccess) return fail(std::string("conv3d: ") + cudaGetErrorString(e));
+            kern<<<dim3((unsigned)(W / HT_X), (unsigned)(H / HT_Y), (unsigned)(B * D / tz)), KS_THREADS, smem_of(tz, ns),
+                   (cudaStream_t)stream>>>((const uint4 *)in, (const uint4 *)wpk, bias, (uint16_t *)out, B, D, H, W, cin, cout,
+                                           relu, kcols);
+            e = cudaPeekAtLastError();
+            if (e != cudaSuccess) return fail(std::string("conv3d launch: ") + cudaGetErrorString(e));
+            return 0;
+        }
+    }
     if (taps == 27 && H % lfts::unet::HT_Y == 0 && W % lfts::unet::HT_X == 0) {
         // halo-staged kernel: TZ output planes per CTA, a ring of NS weight stages
         using namespace lfts::unet;

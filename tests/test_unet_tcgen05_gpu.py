@@ -60,6 +60,7 @@ def test_conv_halo_tiles(monkeypatch, tz, cin, cin_pad, cout, grid, batch):
     LFTS_CONV_TZ override), each with the ring depth its shared memory allows."""
     import torch
     from langevinfts_b200.learned import conv3d_tcgen05, pack_conv
+    monkeypatch.setenv("LFTS_CONV_KSLICE", "0")
     monkeypatch.setenv("LFTS_CONV_TZ", tz)
     torch.manual_seed(cin * 17 + cout)
     conv = torch.nn.Conv3d(cin, cout, 3).cuda()
@@ -70,6 +71,30 @@ def test_conv_halo_tiles(monkeypatch, tz, cin, cin_pad, cout, grid, batch):
     torch.cuda.synchronize()
     ref = _reference(x, conv, True).permute(0, 2, 3, 4, 1)
     assert float((got[..., :cout] - ref).abs().max()) <= 8e-3 * float(ref.abs().max()) + 1e-6
+
+
+@pytest.mark.parametrize("tz", ["1", "2", "4"])
+@pytest.mark.parametrize("cin,cin_pad,cout,grid,batch,relu", [
+    (24, 32, 24, (8, 16, 16), 2, True), (72, 80, 24, (4, 32, 8), 2, False), (48, 48, 48, (4, 16, 24), 1, True),
+    (144, 144, 48, (8, 16, 8), 1, True), (96, 96, 48, (4, 16, 8), 3, False)])
+def test_conv_kslice(monkeypatch, tz, cin, cin_pad, cout, grid, batch, relu):
+    """The kernel that stages the halo and all 27 taps' weights by slices of 16
+    input channels, with 1, 2 and 4 output planes per CTA (the
+    LFTS_CONV_KSLICE_TZ override), against torch."""
+    import torch
+    from langevinfts_b200.learned import conv3d_tcgen05, pack_conv
+    monkeypatch.setenv("LFTS_CONV_KSLICE", "1")
+    monkeypatch.setenv("LFTS_CONV_KSLICE_TZ", tz)
+    torch.manual_seed(cin * 13 + cout + int(tz))
+    conv = torch.nn.Conv3d(cin, cout, 3).cuda()
+    x = torch.randn(batch, cin, *grid, device="cuda").to(torch.bfloat16).float()
+    layer = pack_conv(conv, list(range(cin)), cin_pad)
+    h = torch.nn.functional.pad(x.permute(0, 2, 3, 4, 1), (0, cin_pad - cin)).to(torch.bfloat16).contiguous()
+    got = conv3d_tcgen05(h, layer, relu).float()
+    torch.cuda.synchronize()
+    ref = _reference(x, conv, relu).permute(0, 2, 3, 4, 1)
+    assert float((got[..., :cout] - ref).abs().max()) <= 8e-3 * float(ref.abs().max()) + 1e-6
+    assert float(got[..., cout:].abs().max() if got.shape[-1] > cout else 0) == 0.0
 
 
 @pytest.mark.parametrize("ws", ["2", "3", "4"])
