@@ -872,27 +872,40 @@ extern "C" int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, c
     while ((int)cols < cout) cols <<= 1;
     if (taps == 27 && H % lfts::unet::HT_Y == 0 && W % lfts::unet::HT_X == 0 && cin >= 32) {
         // slices of 16 input channels, by default from three slices on (at two the
-        // halo kernel is faster: 323 against 498 us for 32 -> 32 channels at 64^3 x 8;
-        // d1a 80 -> 32: 890 against 1161 us, d2a 144 -> 48: 210 against 378 us):
-        // the most output planes (4, 2, 1) whose ring of 3 (else 2) slots fits 200 KB;
-        // LFTS_CONV_KSLICE=0|1 (1: from two slices on) and LFTS_CONV_KSLICE_TZ=1|2|4 override
+        // halo kernel is faster: 323 against 498 us for 32 -> 32 channels at 64^3 x 8).
+        // Of the (output planes 4, 2, 1; ring of 3 or 2 slots) within 200 KB, the one
+        // with the most resident CTAs per SM, then the most planes, then slots
+        // (d1a 80 -> 32: 2 planes, 2 slots, two CTAs per SM 625 us against 859-891 us
+        // for 4 planes at one CTA per SM and 1161 us for the halo kernel; d2a 144 -> 48:
+        // 4 planes, 2 slots 210 against 378 us).  LFTS_CONV_KSLICE=0|1 (1: from two
+        // slices on), LFTS_CONV_KSLICE_TZ=1|2|4 and LFTS_CONV_KSLICE_NS=2|3 override
         using namespace lfts::unet;
         bool use = cin >= 48;
         int want_tz = 0;
         if (const char *env = std::getenv("LFTS_CONV_KSLICE")) use = env[0] != '0';
+        int want_ns = 0;
         if (const char *env = std::getenv("LFTS_CONV_KSLICE_TZ")) want_tz = std::atoi(env);
+        if (const char *env = std::getenv("LFTS_CONV_KSLICE_NS")) want_ns = std::atoi(env);
         auto smem_of = [&](int tz, int ns) {
             const int hplp = (tz + 2) * HROW + 1;
             return (size_t)16 * ns * kslice_slot_units(hplp, cout) + (2 * (size_t)ns + 1) * sizeof(uint64_t) + 16;
         };
-        int tz = 0, ns = 0;
+        int tz = 0, ns = 0, best = 0;
         for (int t : {4, 2, 1}) {
-            if (tz || (want_tz && t != want_tz) || D % t || t * cout > 256) continue;
-            for (int q : {3, 2})
-                if (!tz && smem_of(t, q) <= 200 * 1024) {
+            if ((want_tz && t != want_tz) || D % t || t * cout > 256) continue;
+            for (int q : {3, 2}) {
+                if ((want_ns && q != want_ns) || smem_of(t, q) > 200 * 1024) continue;
+                int res = (int)((228 * 1024) / (smem_of(t, q) + 1024));  // resident CTAs: shared memory ...
+                int cols = 32;
+                while (cols < t * cout) cols <<= 1;
+                if (res > 512 / cols) res = 512 / cols;                  // ... and tensor-memory columns
+                const int score = res * 100 + t * 10 + q;
+                if (score > best) {
+                    best = score;
                     tz = t;
                     ns = q;
                 }
+            }
         }
         if (use && tz && (long long)B * D / tz <= 65535) {
             uint32_t kcols = 32;
