@@ -425,6 +425,13 @@ int lfts_pcg64_normal(lfts_ctx ctx, unsigned long long *states, int nstreams, lo
  * FP32 (device).  cin, cout: multiples of 16, cin <= LFTS_CONV_MAX_CIN,
  * cout <= LFTS_CONV_MAX_COUT, and the two shared stages, 32 cin (128 + cout)
  * bytes, within 200 KB; act = ReLU when relu != 0.  stream: cudaStream_t.
+ * Kernel choice: 3x3x3 with H % 16 == 0 and W % 8 == 0 stages each tile's halo
+ * in shared memory (from 48 input channels by slices of 16 channels with all
+ * taps' weights, else once with a ring of per-tap weights); other grids and
+ * 1x1x1 gather the shifted rows per tap.  The results agree to FP32
+ * accumulation order.  LFTS_CONV_KSLICE, LFTS_CONV_KSLICE_TZ,
+ * LFTS_CONV_KSLICE_NS and LFTS_CONV_TZ (environment) override the choice, for
+ * tests and measurement.
  * No counterpart in the reference (it has no learned component). */
 #define LFTS_CONV_MAX_CIN 160
 #define LFTS_CONV_MAX_COUT 256
@@ -433,8 +440,12 @@ int lfts_conv3d_bf16(void *stream, const void *in, const void *wpk, const float 
 /* Its weight gradient, also on the tensor cores:
  *   dw[tap][co][ci] += sum_p gy[p][co] x[(p + tap) mod box][ci]
  * x: [B][D][H][W][cin], gy: [B][D][H][W][cout] BF16 channels-last; dw: FP32
- * [taps][cout][ci], accumulated (zero it first); cout <= 128.  The input gradient is
- * lfts_conv3d_bf16 of gy with the weights transposed and the taps mirrored. */
+ * [taps][cout][ci], accumulated (zero it first); cout <= 128, at most 65535
+ * chunks of 32-256 stages of 64 positions.  The input gradient is
+ * lfts_conv3d_bf16 of gy with the weights transposed and the taps mirrored.
+ * LFTS_CONV_WGRAD_RING, LFTS_CONV_WGRAD_STAGES and LFTS_CONV_WGRAD_GATHER
+ * (environment) override the ring depth, the stages per CTA and the x staging,
+ * for tests and measurement. */
 int lfts_conv3d_wgrad_bf16(void *stream, const void *x, const void *gy, float *dw, int B, int D, int H, int W, int cin,
                            int cout, int taps);
 
