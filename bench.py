@@ -350,7 +350,7 @@ def scft_params(platform_tol=1e-8, max_iter=2000):
     epsilon = b_A / b_B = 1.2, box 3.6 per side relaxing with stress, Anderson
     mixing with 20 histories, tolerance 1e-8.  N = 100 contour steps: with
     f = 0.36 the A block of an N = 90 chain would have 32.4 segments, which the
-    reference (like this build) rejects."""
+    reference (and this module) rejects."""
     eps, f = 1.2, 0.36
     den = eps * eps * f + (1 - f)
     return {"nx": [64, 64, 64], "lx": [3.6, 3.6, 3.6], "chain_model": "continuous", "ds": 1 / 100,

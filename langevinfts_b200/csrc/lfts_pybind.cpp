@@ -280,12 +280,12 @@ PYBIND11_MODULE(langevinfts, m) {
 
     py::class_<Factory>(m, "AbstractFactory")
         .def("create_array", [](Factory &, unsigned int) -> py::object {
-            throw std::runtime_error("Array is not part of this build (the solver API works on numpy arrays)");
+            throw std::runtime_error("Array is not part of this module (the solver API works on numpy arrays)");
         })
         .def("create_computation_box", [](Factory &, std::vector<int> nx, std::vector<double> lx, py::object bc, py::object mask) {
             std::vector<std::string> bcv;
             if (!bc.is_none()) bcv = bc.cast<std::vector<std::string>>();
-            if (!mask.is_none()) throw std::runtime_error("mask (impenetrable regions) is not supported by this build");
+            if (!mask.is_none()) throw std::runtime_error("mask (impenetrable regions) is not supported by this module");
             return new ComputationBox(nx, lx, bcv);
         }, py::arg("nx"), py::arg("lx"), py::arg("bc") = py::none(), py::arg("mask") = py::none())
         .def("create_molecules_information", [](Factory &, std::string model, double ds, std::map<std::string, double> bonds) {
