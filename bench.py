@@ -39,15 +39,15 @@ METRIC_FP32 = "Langevin steps/s @ saddle err 1e-4 (batched L-FTS, FP32 propagato
 UNIT = "replica-steps/s"
 
 
-# The batched L-FTS workloads: config4 is the headline (64^3, 64 replicas);
-# config5 is the system of the learned-start study run with the plain solver.
+# The batched L-FTS workloads: diblock64 is the headline (64^3, 64 replicas);
+# diblock96 is the system of the learned-start study run with the plain solver.
 WORKLOADS = {
-    "config4": {"nx": 64, "lx": 7.3, "f": 0.5, "chin": 17.0, "nbar": 100, "replicas": 64, "seed": 1000},
-    "config5": {"nx": 96, "lx": 8.0, "f": 0.4, "chin": 18.0, "nbar": 200, "replicas": 16, "seed": 2000},
+    "diblock64": {"nx": 64, "lx": 7.3, "f": 0.5, "chin": 17.0, "nbar": 100, "replicas": 64, "seed": 1000},
+    "diblock96": {"nx": 96, "lx": 8.0, "f": 0.4, "chin": 18.0, "nbar": 200, "replicas": 16, "seed": 2000},
 }
 
 
-def workload_config(R, nx, name="config4"):
+def workload_config(R, nx, name="diblock64"):
     """The benchmark workload as both arms report it."""
     w = WORKLOADS[name]
     return {"workload": f"batched L-FTS: {R} replicas/GPU of AB diblock f={w['f']} chiN={w['chin']:g} nbar={w['nbar']} "
@@ -133,7 +133,7 @@ def load_reference():
     return mod
 
 
-def reference_sample(n_iter, threads, timeout=900, workload="config4"):
+def reference_sample(n_iter, threads, timeout=900, workload="diblock64"):
     """Time n_iter saddle-point iterations of one replica on the reference CPU
     platform through the same driver; returns (seconds per iteration, threads).
     Runs in a child process: the reference keeps two grids of reals and two of
@@ -154,7 +154,7 @@ def reference_sample(n_iter, threads, timeout=900, workload="config4"):
     return tuple(json.loads(r.stdout.strip().splitlines()[-1]))
 
 
-def _reference_sample_child(n_iter, threads, workload="config4"):
+def _reference_sample_child(n_iter, threads, workload="diblock64"):
     ref = load_reference()
     if ref is None:
         return None
@@ -183,7 +183,7 @@ def _reference_sample_child(n_iter, threads, workload="config4"):
     return 0
 
 
-def _reference_steps_child(k_max, budget_s, workload="config4"):
+def _reference_steps_child(k_max, budget_s, workload="diblock64"):
     """The reference CPU platform through the driver: the initial saddle-point
     search of one replica (untimed, its warm-up), then Langevin steps until
     k_max are done or the next one would pass budget_s of timed work (at
@@ -277,10 +277,10 @@ def step_traffic_per_job(s_bytes):
 # compute_statistics of one system through the langevinfts API: configs 1 (32^3
 # diblock) and 3 (48^3 discrete branched mixture), seeded normal fields.
 STAT_CONFIGS = {
-    "config1_32cubed_diblock": {
+    "diblock32_continuous": {
         "nx": [32, 32, 32], "lx": [4.0, 4.0, 4.0], "model": "continuous", "ds": 0.01, "bonds": {"A": 1.0, "B": 1.0},
         "polymers": [(1.0, [["A", 0.5, 0, 1], ["B", 0.5, 1, 2]])], "seed": 1, "sigma": 1.0},
-    "config3_48cubed_branched_discrete": {
+    "branched48_discrete": {
         "nx": [48, 48, 48], "lx": [5.0, 5.0, 5.0], "model": "discrete", "ds": 1 / 60,
         "bonds": {"A": 1.0, "B": 1.0, "C": 1.0},
         "polymers": [(0.5, [["A", 20 / 60, 0, 1], ["B", 20 / 60, 0, 2], ["C", 20 / 60, 0, 3]]),
@@ -1082,8 +1082,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config4", choices=sorted(WORKLOADS),
-                    help="config4: 64^3, 64 replicas (the headline); config5: 96^3, 16 replicas")
+    ap.add_argument("--workload", default="diblock64", choices=sorted(WORKLOADS),
+                    help="diblock64: 64^3, 64 replicas (the headline); diblock96: 96^3, 16 replicas")
     ap.add_argument("--replicas", type=int, default=None)
     ap.add_argument("--nx", type=int, default=None)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
